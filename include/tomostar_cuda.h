@@ -1,0 +1,153 @@
+/*
+ * tomostar_cuda.h — C ABI of libtomostar_cuda.so, the B200 (sm_100a) forward engine of TomoSTAR.
+ *
+ * The C# host binds it with [DllImport("tomostar_cuda")] (the native-library convention of
+ * src/TomoStar.Core/Compute/MpiSession.cs:158-168) behind the interfaces the OpenCL backend
+ * implements today:
+ *   - src/TomoStar.Core/Forward/EikonalOpenCl.cs (TryCreate, SuggestBatch, TrySolve, SelfTest),
+ *   - the per-arrival body of src/TomoStar.Core/Tomography/RayKernels.cs:67-107
+ *     (RayTracing.Backtrack + RayTracing.Kernel), which has no device interface in the reference.
+ *
+ * Conventions: nothing throws or aborts across the boundary. Every entry point returns TS_OK (0)
+ * or a TS_E_* code, and ts_last_error() gives the text (the `reason` of TrySolve). Arrays are
+ * caller-owned host memory passed by pointer; device memory is owned by the context. Calls on one
+ * context are serialised internally (as EikonalOpenCl's lock(_gate), EikonalOpenCl.cs:64,165).
+ * There is no CPU fallback inside any entry point: a device failure is returned as an error.
+ */
+#ifndef TOMOSTAR_CUDA_H
+#define TOMOSTAR_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TS_OK 0
+#define TS_E_ARG 1        /* invalid argument (sizes, pointers, grid) */
+#define TS_E_CUDA 2       /* a CUDA call failed; text in ts_last_error */
+#define TS_E_NOMEM 3      /* device memory exhausted */
+#define TS_E_UNSETTLED 4  /* "sweeping not settled after N rounds" (EikonalOpenCl.cs:269) */
+#define TS_E_CANCELLED 5  /* the cancel flag was raised (CancellationToken, EikonalOpenCl.cs:243,262) */
+#define TS_E_TIMEOUT 6    /* a bounded device-side wait ran out; the context stays usable */
+#define TS_E_CAPACITY 7   /* an output buffer is too small; the needed size is reported */
+#define TS_E_NOSEEDS 8    /* "no seed nodes" (EikonalOpenCl.cs:164) */
+#define TS_E_SELFTEST 9   /* the device disagreed with the host solver beyond the gate */
+#define TS_E_NODEVICE 10  /* no CUDA device */
+
+#define TS_PRECISION_F64 64
+#define TS_PRECISION_F32 32
+
+/* Solve modes of ts_eik_solve. */
+#define TS_MODE_ENGINE 0  /* batched tiled engine: tile-wavefront sweeps, one cooperative launch */
+#define TS_MODE_PLAIN 1   /* the reference scheme as-is: one launch per diagonal plane, one field at a time */
+
+/* Output element types. */
+#define TS_OUT_F64 0
+#define TS_OUT_F32 1
+
+typedef struct ts_ctx ts_ctx;
+
+/* GridDefinition (src/TomoStar.Core/Geo/SphericalGrid.cs:13-31). depth_km (extension, not in the
+ * reference): nz increasing depths for a variable vertical spacing, or NULL for the uniform grid. */
+typedef struct ts_grid {
+    double min_lon, max_lon, min_lat, max_lat, min_depth_km, max_depth_km;
+    int32_t nx, ny, nz, reserved;
+    const double* depth_km;
+} ts_grid;
+
+typedef struct ts_eik_stats {
+    int32_t rounds[2];      /* rounds of eight sweeps per phase, largest over the batch (LastStats) */
+    int32_t launches;       /* kernel launches made by the solve */
+    int32_t reserved;
+    int64_t node_updates;   /* node evaluations performed (one per node per tile or plane visit) */
+    int64_t tile_visits;    /* tiles processed (engine) or planes launched (plain) */
+    double device_ms;       /* CUDA-event time of the solve on the device */
+} ts_eik_stats;
+
+/* ---- context (EikonalOpenCl.TryCreate / Dispose / Device) ----------------------------------- */
+
+/* Creates a context on a CUDA device (EikonalOpenCl.TryCreate, EikonalOpenCl.cs:88-118, without
+ * the self-test: call ts_cuda_selftest, as TryCreate does at :109-115, before trusting it). */
+int ts_cuda_create(int32_t device, ts_ctx** out);
+void ts_cuda_destroy(ts_ctx* ctx);                       /* EikonalOpenCl.Dispose (:376-384) */
+const char* ts_last_error(ts_ctx* ctx);                  /* the `reason` strings of TrySolve */
+int ts_device_name(ts_ctx* ctx, char* buf, int32_t cap); /* EikonalOpenCl.Device (:83) */
+const char* ts_last_stats(ts_ctx* ctx);                  /* EikonalOpenCl.LastStats (:86) */
+/* Raises or clears the cancel flag polled between rounds (CancellationToken of TrySolve). */
+void ts_set_cancel(ts_ctx* ctx, int32_t cancel);
+
+/* Fields of `nodes` nodes per batch that fit this device (EikonalOpenCl.SuggestBatch, :121-132);
+ * the engine caps it at 1024 instead of 32 because it has no per-plane launch cost to amortise. */
+int32_t ts_eik_suggest_batch(ts_ctx* ctx, int64_t nodes, int32_t precision);
+
+/* ---- eikonal ----------------------------------------------------------------------------------- */
+
+/* SphericalEikonal.PointSource (Forward/SphericalEikonal.cs:68-100) on the host: the seed nodes
+ * of a point source. Returns the seed count; when it exceeds cap, nothing is written past cap and
+ * the count needed is returned. radius_cells is the reference's default 3. */
+int32_t ts_point_source(const ts_grid* grid, const double* slowness, double lon, double lat, double depth_km,
+                        double origin_time, double radius_cells, int32_t* idx_out, double* t_out, int32_t cap);
+
+/* EikonalOpenCl.TrySolve (EikonalOpenCl.cs:138-166): one field per seed set, all on one grid and
+ * one slowness (double[n], grid order, x fastest). Seed set f is seed_index/seed_time
+ * [seed_offsets[f], seed_offsets[f+1]); out-of-range indices are ignored and duplicates take the
+ * smallest time. precision: TS_PRECISION_F64 (result equals SphericalEikonal.Relax to the bit) or
+ * TS_PRECISION_F32. mode: TS_MODE_ENGINE or TS_MODE_PLAIN. tol: settle tolerance of a round, s
+ * (the reference's 1e-7; 0 runs to the exact fixed point). max_rounds <= 0 uses the reference cap
+ * max(32, (nx+ny+nz)/4) per phase. out: n_fields*n values, field-major, of out_type; unreached
+ * nodes are +inf. Returns TS_E_UNSETTLED, like TrySolve's refusal, if any field did not settle. */
+int ts_eik_solve(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32_t n_fields,
+                 const int32_t* seed_offsets, const int32_t* seed_index, const double* seed_time, int32_t precision,
+                 int32_t mode, double tol, int32_t max_rounds, void* out, int32_t out_type, ts_eik_stats* stats);
+
+/* EikonalOpenCl.SelfTest (EikonalOpenCl.cs:346-374): the reference's 22x20x16 heterogeneous case
+ * solved on the device and by the host sweeping solver; *rel_err = max |dt| / field range. The
+ * gate passes when *rel_err <= 1e-6 (SelfTestTolerance, :45); otherwise TS_E_SELFTEST. */
+int ts_cuda_selftest(ts_ctx* ctx, int32_t precision, double* rel_err, char* msg, int32_t cap);
+
+/* Engine tile shapes compiled into the library: writes up to cap (id, bx, by, bz) quadruples to
+ * shapes and returns how many exist. No reference counterpart (the OpenCL kernel is untiled). */
+int32_t ts_engine_shapes(int32_t* shapes, int32_t cap);
+/* Selects the engine's tile shape for one precision on this context (the autotuner's knob). */
+int ts_engine_set_tile(ts_ctx* ctx, int32_t precision, int32_t shape_id);
+
+/* ---- rays and Jacobian rows (RayKernels.Compute's per-arrival body) ---------------------------- */
+
+typedef struct ts_rows ts_rows;
+
+/* Traces rays on travel-time tables and integrates them on the inversion grid
+ * (RayTracing.Backtrack, Forward/RayTracing.cs:73-111; RayTracing.Kernel, :118-159; row
+ * finalisation, Tomography/RayKernels.cs:79-97). tables: n_tables float32 fields on fwd (the
+ * .qttb values, TravelTimeTable.cs:73); table_station: 3 doubles (lon, lat, depth) per table (the
+ * table header's station). Ray a starts at events[3a..3a+2] on table table_of[a]. step_km: the
+ * RayKernels step 0.5·min(forward, inversion MinSpacingKm). Produces one CSR row per ray (nodes
+ * ascending, float32 lengths), TCalc and the source gradient; a ray the reference drops has ok=0
+ * and an empty row. The result stays on the device until ts_rows_copy. */
+int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float* tables, const double* table_station,
+                  const ts_grid* inv, int32_t n_rays, const int32_t* table_of, const double* events, double step_km,
+                  ts_rows** out);
+
+/* RayKernels.Compute for travel times (Tomography/RayKernels.cs:30-115) with the tables built on
+ * the device: one field per (station, phase) used, by the engine (precision as ts_eik_solve), each
+ * seeded by PointSource at the station and rounded to float32 as TravelTimeTable.Write does, then
+ * every arrival traced on its table. slowness: n_phases fields on fwd (ForwardModel, phase p at
+ * p*n). stations/events: 3 doubles each. Arrival a: (arr_event[a], arr_station[a], arr_phase[a]).
+ * step_km <= 0 uses the RayKernels step. */
+int ts_forward(ts_ctx* ctx, const ts_grid* fwd, const double* slowness, int32_t n_phases, const ts_grid* inv,
+               int32_t n_stations, const double* stations, int32_t n_events, const double* events,
+               int32_t n_arrivals, const int32_t* arr_event, const int32_t* arr_station, const int32_t* arr_phase,
+               int32_t precision, double step_km, ts_rows** out, ts_eik_stats* stats);
+
+/* Sizes of a result: rows (= rays or arrivals) and total non-zeros. */
+int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz);
+/* Copies a result to the host: row_ptr[n_rows+1], col[nnz] (int32 node), len[nnz] (float32 km),
+ * tcalc_grad[4*n_rows] (TCalc s, Ge, Gn, Gz s/km), ok[n_rows]. Any pointer may be NULL. */
+int ts_rows_copy(ts_rows* rows, int32_t* row_ptr, int32_t* col, float* len, double* tcalc_grad, uint8_t* ok);
+void ts_rows_free(ts_rows* rows);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOMOSTAR_CUDA_H */

@@ -1,0 +1,880 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement of TomoSTAR's forward path, used by the tests, by the smoke check and by
+// bench.py's CPU-baseline leg as the checker and baseline. The product (tomostar_b200/) never
+// links, loads or calls this file.
+//
+// Parity status: the reference is C# (.NET 10) and cannot be built or run here, so no bitwise
+// reference output exists. This restatement is pinned by the reference's own known-answer tests
+// (tests/TomoStar.Tests/NumericsTests.cs:88-123) and by the analytic cases of its validation
+// exporter (validation/TomoStar.Validation/Program.cs:107-143); tests/test_oracle.py runs them.
+//
+// Every function cites the reference lines it follows. Arithmetic is kept in the reference's
+// expression order and the file is compiled with -ffp-contract=off, so a double result is the
+// one .NET computes on the same libm (glibc on Linux).
+//
+// Extension not in the reference: a grid may carry an explicit depth array (variable, e.g.
+// geometric, vertical spacing). The z-axis spacing of the upwind update is then the distance
+// to the neighbour actually used, and the second-order term uses the non-uniform one-sided
+// three-point derivative. With a uniform grid the reference arithmetic is used unchanged.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <atomic>
+#include <vector>
+
+namespace {
+
+constexpr double kEarthRadiusKm = 6371.0;            // Geo/GeoMath.cs:43
+constexpr double kDeg2Rad = M_PI / 180.0;            // Geo/GeoMath.cs:45
+constexpr double kRad2Deg = 180.0 / M_PI;            // Geo/GeoMath.cs:46
+constexpr double kInf = std::numeric_limits<double>::infinity();
+
+struct V3 {
+    double x, y, z;
+};
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double norm(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }  // GeoMath.cs:18
+
+// GeoMath.ToCartesian (Geo/GeoMath.cs:49-56).
+inline V3 to_cartesian(double lon_deg, double lat_deg, double depth_km) {
+    double r = kEarthRadiusKm - depth_km;
+    double lat = lat_deg * kDeg2Rad;
+    double lon = lon_deg * kDeg2Rad;
+    double cl = std::cos(lat);
+    return {r * cl * std::cos(lon), r * cl * std::sin(lon), r * std::sin(lat)};
+}
+
+struct Geo {
+    double lon, lat, depth;
+};
+
+// GeoMath.FromCartesian (Geo/GeoMath.cs:61-68).
+inline Geo from_cartesian(V3 v) {
+    double r = norm(v);
+    if (r <= 0) return {0, 0, kEarthRadiusKm};
+    double lat = std::asin(std::clamp(v.z / r, -1.0, 1.0)) * kRad2Deg;
+    double lon = std::atan2(v.y, v.x) * kRad2Deg;
+    return {lon, lat, kEarthRadiusKm - r};
+}
+
+// GeoMath.LocalFrame (Geo/GeoMath.cs:71-80).
+inline void local_frame(double lon_deg, double lat_deg, V3& east, V3& north, V3& up) {
+    double lat = lat_deg * kDeg2Rad;
+    double lon = lon_deg * kDeg2Rad;
+    double sl = std::sin(lat), cl = std::cos(lat), so = std::sin(lon), co = std::cos(lon);
+    east = {-so, co, 0};
+    north = {-sl * co, -sl * so, cl};
+    up = {cl * co, cl * so, sl};
+}
+
+// GeoMath.UnwrapLon (Geo/GeoMath.cs:146-151).
+inline double unwrap_lon(double lon, double ref) {
+    if (lon < ref - 180) lon += 360 * std::ceil((ref - 180 - lon) / 360);
+    else if (lon > ref + 180) lon -= 360 * std::ceil((lon - ref - 180) / 360);
+    return lon;
+}
+
+}  // namespace
+
+extern "C" {
+
+// GridDefinition (Geo/SphericalGrid.cs:13-31) plus the optional depth array of the extension.
+struct or_grid_def {
+    double min_lon, max_lon, min_lat, max_lat, min_depth_km, max_depth_km;
+    int32_t nx, ny, nz, _pad;
+    const double* depth_km;  // nz depths (variable vertical spacing) or null (uniform)
+};
+
+}  // extern "C"
+
+namespace {
+
+// SphericalGrid (Geo/SphericalGrid.cs:84-116).
+struct Grid {
+    int nx, ny, nz;
+    double min_lon, min_lat, min_dep;
+    double dlon, dlat, ddep;  // GridDefinition.DLon/DLat/DDepth (SphericalGrid.cs:28-30)
+    double centre_lon, dlon_rad, dlat_rad, ddep_km;
+    bool variable;
+    std::vector<double> lon, lat, coslat, dep, rad;
+
+    explicit Grid(const or_grid_def& d) {
+        nx = d.nx; ny = d.ny; nz = d.nz;
+        min_lon = d.min_lon; min_lat = d.min_lat; min_dep = d.min_depth_km;
+        dlon = (d.max_lon - d.min_lon) / std::max(1, nx - 1);
+        dlat = (d.max_lat - d.min_lat) / std::max(1, ny - 1);
+        ddep = (d.max_depth_km - d.min_depth_km) / std::max(1, nz - 1);
+        variable = d.depth_km != nullptr;
+        lon.resize(nx); lat.resize(ny); coslat.resize(ny); dep.resize(nz); rad.resize(nz);
+        for (int i = 0; i < nx; i++) lon[i] = d.min_lon + i * dlon;
+        for (int j = 0; j < ny; j++) {
+            lat[j] = d.min_lat + j * dlat;
+            coslat[j] = std::cos(lat[j] * kDeg2Rad);
+        }
+        for (int k = 0; k < nz; k++) {
+            dep[k] = variable ? d.depth_km[k] : d.min_depth_km + k * ddep;
+            rad[k] = kEarthRadiusKm - dep[k];
+        }
+        centre_lon = 0.5 * (d.min_lon + d.max_lon);
+        dlon_rad = dlon * kDeg2Rad;
+        dlat_rad = dlat * kDeg2Rad;
+        ddep_km = ddep;
+    }
+    int count() const { return nx * ny * nz; }
+    int index(int i, int j, int k) const { return (k * ny + j) * nx + i; }  // SphericalGrid.cs:135
+    V3 cartesian(int i, int j, int k) const { return to_cartesian(lon[i], lat[j], dep[k]); }
+
+    // Fractional depth index; the extension inverts the depth array piecewise linearly.
+    double frac_z(double depth_km) const {
+        if (!variable) return (depth_km - min_dep) / ddep;
+        if (depth_km <= dep[0]) return (depth_km - dep[0]) / (dep[1] - dep[0]);
+        if (depth_km >= dep[nz - 1]) return (nz - 1) + (depth_km - dep[nz - 1]) / (dep[nz - 1] - dep[nz - 2]);
+        int k = int(std::upper_bound(dep.begin(), dep.end(), depth_km) - dep.begin()) - 1;
+        return k + (depth_km - dep[k]) / (dep[k + 1] - dep[k]);
+    }
+    // SphericalGrid.Fractional (SphericalGrid.cs:179-184).
+    void fractional(double lon_deg, double lat_deg, double depth_km, double& fx, double& fy, double& fz) const {
+        if (lon_deg < centre_lon - 180 || lon_deg > centre_lon + 180) lon_deg = unwrap_lon(lon_deg, centre_lon);
+        fx = (lon_deg - min_lon) / dlon;
+        fy = (lat_deg - min_lat) / dlat;
+        fz = frac_z(depth_km);
+    }
+    // SphericalGrid.TrilinearWeightsFractional (SphericalGrid.cs:205-224).
+    void weights_fractional(double fx, double fy, double fz, int* nodes, double* w) const {
+        fx = std::clamp(fx, 0.0, double(nx - 1));
+        fy = std::clamp(fy, 0.0, double(ny - 1));
+        fz = std::clamp(fz, 0.0, double(nz - 1));
+        int i0 = std::min(int(fx), nx - 2), j0 = std::min(int(fy), ny - 2), k0 = std::min(int(fz), nz - 2);
+        double tx = fx - i0, ty = fy - j0, tz = fz - k0;
+        int n = 0;
+        for (int dk = 0; dk < 2; dk++)
+            for (int dj = 0; dj < 2; dj++)
+                for (int di = 0; di < 2; di++) {
+                    nodes[n] = index(i0 + di, j0 + dj, k0 + dk);
+                    w[n] = (di == 0 ? 1 - tx : tx) * (dj == 0 ? 1 - ty : ty) * (dk == 0 ? 1 - tz : tz);
+                    n++;
+                }
+    }
+    void weights(double lon_deg, double lat_deg, double depth_km, int* nodes, double* w) const {
+        double fx, fy, fz;
+        fractional(lon_deg, lat_deg, depth_km, fx, fy, fz);
+        weights_fractional(fx, fy, fz, nodes, w);
+    }
+    // SphericalGrid.Interpolate (SphericalGrid.cs:227-235).
+    double interpolate(const double* field, double lon_deg, double lat_deg, double depth_km) const {
+        int nodes[8];
+        double w[8];
+        weights(lon_deg, lat_deg, depth_km, nodes, w);
+        double sum = 0;
+        for (int n = 0; n < 8; n++) sum += field[nodes[n]] * w[n];
+        return sum;
+    }
+    // SphericalGrid.MinSpacingKm (SphericalGrid.cs:159-164).
+    double min_spacing_km() const {
+        double r_min = rad[nz - 1];
+        double cos_min = *std::min_element(coslat.begin(), coslat.end());
+        double dz = ddep_km;
+        if (variable) {
+            dz = kInf;
+            for (int k = 0; k + 1 < nz; k++) dz = std::min(dz, dep[k + 1] - dep[k]);
+        }
+        return std::min(dz, std::min(r_min * dlat_rad, r_min * cos_min * dlon_rad));
+    }
+};
+
+// GridMetric (Forward/SphericalEikonal.cs:15-35), with the z spacing per interval for the extension.
+struct Metric {
+    const Grid& g;
+    std::vector<double> hlon, hlat, dz;  // dz[k] = depth[k+1] - depth[k] (extension only)
+    double hr;
+    explicit Metric(const Grid& grid) : g(grid) {
+        hlon.resize(size_t(g.ny) * g.nz);
+        hlat.resize(g.nz);
+        for (int k = 0; k < g.nz; k++) {
+            hlat[k] = g.rad[k] * g.dlat_rad;
+            for (int j = 0; j < g.ny; j++) hlon[size_t(k) * g.ny + j] = std::max(1e-9, g.rad[k] * g.coslat[j] * g.dlon_rad);
+        }
+        hr = g.ddep_km;
+        if (g.variable) {
+            dz.resize(g.nz - 1);
+            for (int k = 0; k + 1 < g.nz; k++) dz[k] = g.dep[k + 1] - g.dep[k];
+        }
+    }
+};
+
+// One upwind term: effective time, effective spacing, the neighbour's own time.
+struct Term {
+    double t, h, n;
+};
+
+// Stable insertion sort by effective time (SphericalEikonal.cs:262-275).
+inline void sort_terms(Term* q, int used) {
+    for (int a = 1; a < used; a++) {
+        Term x = q[a];
+        int b = a - 1;
+        while (b >= 0 && q[b].t > x.t) { q[b + 1] = q[b]; b--; }
+        q[b + 1] = x;
+    }
+}
+
+// The Godunov root over the used terms, largest subset first (SphericalEikonal.cs:179-199, 364-379).
+inline double godunov(const Term* q, int used, double s) {
+    for (int terms = used; terms >= 1; terms--) {
+        double sw = 0, swt = 0, swt2 = 0;
+        for (int r = 0; r < terms; r++) {
+            double w = 1.0 / (q[r].h * q[r].h);
+            sw += w;
+            swt += w * q[r].t;
+            swt2 += w * q[r].t * q[r].t;
+        }
+        double disc = swt * swt - sw * (swt2 - s * s);
+        if (disc < 0) continue;
+        double root = (swt + std::sqrt(disc)) / sw;
+        bool ok = true;
+        for (int r = 0; r < terms; r++)
+            if (root < q[r].n) { ok = false; break; }
+        if (ok) return root;
+    }
+    return kInf;
+}
+
+// Uniform-axis term (SphericalEikonal.cs:381-395 / EikonalOpenCl.cs:432-450): pick the smaller
+// neighbour, promote to second order when its partner beyond is finite and not larger.
+inline void axis_term(double minus, double plus, double minus2, double plus2, double h, bool second_order, Term* q,
+                      int& used) {
+    double first, t2;
+    if (minus <= plus) { first = minus; t2 = minus2; }
+    else { first = plus; t2 = plus2; }
+    if (!std::isfinite(first)) return;
+    if (!second_order) t2 = kInf;
+    if (std::isfinite(t2) && t2 <= first) q[used] = {(4 * first - t2) / 3, 2 * h / 3, first};
+    else q[used] = {first, h, first};
+    used++;
+}
+
+// Extension: z-axis term on a non-uniform axis. h1 = spacing to the first neighbour, h2 = from
+// there to the second. The one-sided derivative a·T0 + b·T1 + c·T2 with a = (2h1+h2)/(h1(h1+h2)),
+// b = −(h1+h2)/(h1 h2), c = h1/(h2(h1+h2)) is written as (T0 − te)/he: he = 1/a, te = −(b T1 + c T2)/a.
+inline void axis_term_var(double minus, double plus, double minus2, double plus2, double hm, double hp, double hm2,
+                          double hp2, bool second_order, Term* q, int& used) {
+    double first, t2, h1, h2;
+    if (minus <= plus) { first = minus; t2 = minus2; h1 = hm; h2 = hm2; }
+    else { first = plus; t2 = plus2; h1 = hp; h2 = hp2; }
+    if (!std::isfinite(first)) return;
+    if (!second_order) t2 = kInf;
+    if (std::isfinite(t2) && t2 <= first) {
+        double a = (2 * h1 + h2) / (h1 * (h1 + h2));
+        double b = (h1 + h2) / (h1 * h2);
+        double c = h1 / (h2 * (h1 + h2));
+        q[used] = {(b * first - c * t2) / a, 1 / a, first};
+    } else {
+        q[used] = {first, h1, first};
+    }
+    used++;
+}
+
+// RelaxNode (SphericalEikonal.cs:349-396): the upwind update of one node from the field values.
+inline double relax_node(const Metric& m, const double* s_arr, const double* f, int idx, int i, int j, int k,
+                         bool second_order) {
+    const Grid& g = m.g;
+    double s = s_arr[idx];
+    if (!(s > 0)) return kInf;
+    int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+    Term q[3];
+    int used = 0;
+    auto at = [&](bool ok, int off) { return ok ? f[idx + off] : kInf; };
+    axis_term(at(i > 0, -1), at(i + 1 < nx, 1), at(i > 1, -2), at(i + 2 < nx, 2), m.hlon[size_t(k) * ny + j],
+              second_order, q, used);
+    axis_term(at(j > 0, -nx), at(j + 1 < ny, nx), at(j > 1, -2 * nx), at(j + 2 < ny, 2 * nx), m.hlat[k], second_order,
+              q, used);
+    if (!g.variable) {
+        axis_term(at(k > 0, -nxy), at(k + 1 < nz, nxy), at(k > 1, -2 * nxy), at(k + 2 < nz, 2 * nxy), m.hr,
+                  second_order, q, used);
+    } else {
+        double hm = k > 0 ? m.dz[k - 1] : 1, hp = k + 1 < nz ? m.dz[k] : 1;
+        double hm2 = k > 1 ? m.dz[k - 2] : 1, hp2 = k + 2 < nz ? m.dz[k + 1] : 1;
+        axis_term_var(at(k > 0, -nxy), at(k + 1 < nz, nxy), at(k > 1, -2 * nxy), at(k + 2 < nz, 2 * nxy), hm, hp, hm2,
+                      hp2, second_order, q, used);
+    }
+    if (used == 0) return kInf;
+    sort_terms(q, used);
+    return godunov(q, used, s);
+}
+
+// SphericalEikonal.PlaneBounds (SphericalEikonal.cs:341-347).
+inline void plane_bounds(int nx, int ny, int nz, int p, int& i0, int& i1, int& k0, int& k1) {
+    i0 = std::max(0, p - (ny - 1) - (nz - 1));
+    i1 = std::min(nx - 1, p);
+    k0 = std::max(0, p - (nx - 1) - (ny - 1));
+    k1 = std::min(nz - 1, p);
+}
+
+// SphericalEikonal.SweepRoundCap (SphericalEikonal.cs:335).
+inline int sweep_round_cap(const Grid& g) { return std::max(32, (g.nx + g.ny + g.nz) / 4); }
+
+// FrontHeap (SphericalEikonal.cs:404-475): 4-ary min-heap, one entry per node, decrease-key in place.
+struct FrontHeap {
+    struct Entry {
+        double key;
+        int node;
+    };
+    std::vector<Entry> e;
+    std::vector<int> at;  // slot + 1; 0 = absent
+    int count = 0;
+    FrontHeap(int nodes, int capacity) : e(capacity), at(nodes, 0) {}
+    void set(int node, double key) {
+        int i = at[node] - 1;
+        if (i < 0) {
+            if (count == int(e.size())) e.resize(size_t(count) * 2);
+            i = count++;
+        }
+        while (i > 0) {
+            int p = (i - 1) >> 2;
+            if (e[p].key <= key) break;
+            e[i] = e[p];
+            at[e[i].node] = i + 1;
+            i = p;
+        }
+        e[i] = {key, node};
+        at[node] = i + 1;
+    }
+    bool pop(int& node) {
+        if (count == 0) { node = -1; return false; }
+        node = e[0].node;
+        at[node] = 0;
+        Entry last = e[--count];
+        if (count == 0) return true;
+        int i = 0;
+        for (;;) {
+            int c = 4 * i + 1;
+            if (c >= count) break;
+            int best = c;
+            double best_key = e[c].key;
+            int end = std::min(c + 4, count);
+            for (int q = c + 1; q < end; q++)
+                if (e[q].key < best_key) { best = q; best_key = e[q].key; }
+            if (best_key >= last.key) break;
+            e[i] = e[best];
+            at[e[i].node] = i + 1;
+            i = best;
+        }
+        e[i] = last;
+        at[last.node] = i + 1;
+        return true;
+    }
+};
+
+// TravelTimeTable float32 storage (Forward/TravelTimeTable.cs:73) and trilinear time (:122-136).
+struct Table {
+    const Grid& g;
+    const float* v;
+    double src_lon, src_lat, src_dep;
+    double time_fractional(double fx, double fy, double fz) const {
+        int nodes[8];
+        double w[8];
+        g.weights_fractional(fx, fy, fz, nodes, w);
+        double t = 0;
+        for (int n = 0; n < 8; n++) {
+            if (w[n] == 0) continue;
+            float x = v[nodes[n]];
+            if (!std::isfinite(x)) return kInf;
+            t += x * w[n];
+        }
+        return t;
+    }
+    double time(double lon, double lat, double dep) const {
+        double fx, fy, fz;
+        g.fractional(lon, lat, dep, fx, fy, fz);
+        return time_fractional(fx, fy, fz);
+    }
+    // TravelTimeTable.Gradient (TravelTimeTable.cs:143-157): central differences of the interpolant,
+    // half a node each side, in (east, north, down) s/km.
+    void gradient(double lon, double lat, double dep, double& ge, double& gn, double& gz) const {
+        double fx, fy, fz;
+        g.fractional(lon, lat, dep, fx, fy, fz);
+        const double d = 0.5;
+        double tx = (time_fractional(fx + d, fy, fz) - time_fractional(fx - d, fy, fz)) / (2 * d);
+        double ty = (time_fractional(fx, fy + d, fz) - time_fractional(fx, fy - d, fz)) / (2 * d);
+        double tz = (time_fractional(fx, fy, fz + d) - time_fractional(fx, fy, fz - d)) / (2 * d);
+        double r = kEarthRadiusKm - dep;
+        double hx = r * std::cos(lat * kDeg2Rad) * g.dlon_rad;
+        double hy = r * g.dlat_rad;
+        double hz = g.ddep_km;
+        ge = tx / hx; gn = ty / hy; gz = tz / hz;
+    }
+};
+
+// RayTracing.Backtrack (Forward/RayTracing.cs:73-111). Returns false where the reference returns null.
+bool backtrack(const Table& tb, double lon, double lat, double dep, double step_km, std::vector<Geo>& path) {
+    const Grid& g = tb.g;
+    double st_dep = std::clamp(tb.src_dep, g.dep[0], g.dep[g.nz - 1]);
+    V3 station = to_cartesian(tb.src_lon, tb.src_lat, st_dep);
+    V3 p = to_cartesian(lon, lat, dep);
+    path.clear();
+    path.push_back({lon, lat, dep});
+    double t0 = tb.time(lon, lat, dep);
+    if (!std::isfinite(t0)) return false;
+    int max_steps = 20 * int(std::ceil(norm(sub(p, station)) / step_km + 10));
+    double last_t = t0;
+    int stalls = 0;
+    for (int step = 0; step < max_steps; step++) {
+        if (norm(sub(p, station)) <= 1.5 * step_km) break;
+        Geo gp = from_cartesian(p);
+        double ge, gn, gz;
+        tb.gradient(gp.lon, gp.lat, gp.depth, ge, gn, gz);
+        if (!std::isfinite(ge) || !std::isfinite(gn) || !std::isfinite(gz)) return false;
+        V3 e, nn, up;
+        local_frame(gp.lon, gp.lat, e, nn, up);
+        V3 grad = add(add(scale(e, ge), scale(nn, gn)), scale(up, -gz));
+        double nrm = norm(grad);
+        if (nrm < 1e-12) return false;
+        p = sub(p, scale(grad, step_km / nrm));
+        Geo q = from_cartesian(p);
+        q = {std::clamp(unwrap_lon(q.lon, g.centre_lon), g.lon[0], g.lon[g.nx - 1]),
+             std::clamp(q.lat, g.lat[0], g.lat[g.ny - 1]), std::clamp(q.depth, g.dep[0], g.dep[g.nz - 1])};
+        p = to_cartesian(q.lon, q.lat, q.depth);
+        path.push_back(q);
+        double t = tb.time(q.lon, q.lat, q.depth);
+        if (!(t < last_t)) {
+            if (++stalls > 20) return false;
+        } else {
+            stalls = 0;
+        }
+        last_t = std::min(last_t, t);
+    }
+    path.push_back({tb.src_lon, tb.src_lat, st_dep});
+    return true;
+}
+
+// RayTracing.Kernel without an outside domain (RayTracing.cs:126-159): (node, length) in first-visit
+// order, each length summed in visit order like the reference's dictionary.
+void ray_kernel(const Grid& inv, const std::vector<Geo>& ray, std::vector<int>& keys, std::vector<double>& vals) {
+    keys.clear();
+    vals.clear();
+    // node -> slot of keys/vals: open addressing with linear probing, kept under half full
+    size_t cap = 1024;
+    std::vector<int> hk(cap, -1), hv(cap, -1);
+    auto find = [&](int node) -> int {
+        size_t m = cap - 1, h = (uint32_t(node) * 2654435761u) & m;
+        while (hk[h] != -1 && hk[h] != node) h = (h + 1) & m;
+        if (hk[h] == node) return hv[h];
+        return -1 - int(h);
+    };
+    auto insert_new = [&](int node, double v) {
+        if (keys.size() * 2 >= cap) {
+            cap *= 2;
+            hk.assign(cap, -1); hv.assign(cap, -1);
+            for (size_t s = 0; s < keys.size(); s++) {
+                size_t m = cap - 1, h = (uint32_t(keys[s]) * 2654435761u) & m;
+                while (hk[h] != -1) h = (h + 1) & m;
+                hk[h] = keys[s]; hv[h] = int(s);
+            }
+        }
+        size_t m = cap - 1, h = (uint32_t(node) * 2654435761u) & m;
+        while (hk[h] != -1) h = (h + 1) & m;
+        hk[h] = node; hv[h] = int(keys.size());
+        keys.push_back(node);
+        vals.push_back(v);
+    };
+    double h = 0.5 * inv.min_spacing_km();
+    int nodes[8];
+    double w[8];
+    for (size_t i = 1; i < ray.size(); i++) {
+        V3 a = to_cartesian(ray[i - 1].lon, ray[i - 1].lat, ray[i - 1].depth);
+        V3 b = to_cartesian(ray[i].lon, ray[i].lat, ray[i].depth);
+        double len = norm(sub(b, a));
+        if (len <= 0) continue;
+        int pieces = std::max(1, int(std::ceil(len / h)));
+        double dl = len / pieces;
+        for (int q = 0; q < pieces; q++) {
+            Geo mid = from_cartesian(add(a, scale(sub(b, a), (q + 0.5) / pieces)));
+            inv.weights(mid.lon, mid.lat, mid.depth, nodes, w);
+            for (int n = 0; n < 8; n++) {
+                if (w[n] == 0) continue;
+                double v = dl * w[n] * 1.0;
+                int s = find(nodes[n]);
+                if (s >= 0) vals[s] = vals[s] + v;
+                else insert_new(nodes[n], v);
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- geometry --------------------------------------------------------------------------------
+
+// GridMetric arrays (SphericalEikonal.cs:17-29): hlon[ny*nz], hlat[nz], *hr; dz[nz-1] when variable.
+void or_metric(const or_grid_def* d, double* hlon, double* hlat, double* hr, double* dz) {
+    Grid g(*d);
+    Metric m(g);
+    std::copy(m.hlon.begin(), m.hlon.end(), hlon);
+    std::copy(m.hlat.begin(), m.hlat.end(), hlat);
+    *hr = m.hr;
+    if (dz && g.variable) std::copy(m.dz.begin(), m.dz.end(), dz);
+}
+
+// Node coordinates: lon[nx], lat[ny], coslat[ny], depth[nz] (SphericalGrid.cs:96-111).
+void or_grid_coords(const or_grid_def* d, double* lon, double* lat, double* coslat, double* depth) {
+    Grid g(*d);
+    std::copy(g.lon.begin(), g.lon.end(), lon);
+    std::copy(g.lat.begin(), g.lat.end(), lat);
+    std::copy(g.coslat.begin(), g.coslat.end(), coslat);
+    std::copy(g.dep.begin(), g.dep.end(), depth);
+}
+
+double or_min_spacing_km(const or_grid_def* d) { return Grid(*d).min_spacing_km(); }
+
+void or_to_cartesian(double lon, double lat, double dep, double* xyz) {
+    V3 v = to_cartesian(lon, lat, dep);
+    xyz[0] = v.x; xyz[1] = v.y; xyz[2] = v.z;
+}
+
+void or_from_cartesian(const double* xyz, double* geo) {
+    Geo g = from_cartesian({xyz[0], xyz[1], xyz[2]});
+    geo[0] = g.lon; geo[1] = g.lat; geo[2] = g.depth;
+}
+
+// SphericalGrid.TrilinearWeights (SphericalGrid.cs:199-224).
+void or_trilinear(const or_grid_def* d, double lon, double lat, double dep, int32_t* nodes, double* w) {
+    Grid g(*d);
+    int n[8];
+    g.weights(lon, lat, dep, n, w);
+    for (int q = 0; q < 8; q++) nodes[q] = n[q];
+}
+
+double or_interpolate(const or_grid_def* d, const double* field, double lon, double lat, double dep) {
+    return Grid(*d).interpolate(field, lon, lat, dep);
+}
+
+// ---- seeds -----------------------------------------------------------------------------------
+
+// SphericalEikonal.PointSource (SphericalEikonal.cs:68-100). Returns the seed count (or, when it
+// exceeds cap, the count needed, with nothing written past cap).
+int32_t or_point_source(const or_grid_def* d, const double* slowness, double lon, double lat, double depth_km,
+                        double origin_time, double radius_cells, int32_t* idx_out, double* t_out, int32_t cap) {
+    Grid g(*d);
+    double dep = std::clamp(depth_km, g.dep[0], g.dep[g.nz - 1]);
+    double fx, fy, fz;
+    g.fractional(lon, lat, dep, fx, fy, fz);
+    fx = std::clamp(fx, 0.0, double(g.nx - 1));
+    fy = std::clamp(fy, 0.0, double(g.ny - 1));
+    fz = std::clamp(fz, 0.0, double(g.nz - 1));
+    V3 src = to_cartesian(lon, lat, dep);
+    double s_src = g.interpolate(slowness, lon, lat, dep);
+    double r = kEarthRadiusKm - dep;
+    double h_lon = std::max(1e-9, r * std::cos(lat * kDeg2Rad) * g.dlon_rad);
+    double h_lat = r * g.dlat_rad;
+    double h_r = g.ddep_km;
+    if (g.variable) {  // extension: the local vertical spacing at the source
+        int kk = std::min(int(fz), g.nz - 2);
+        h_r = g.dep[kk + 1] - g.dep[kk];
+    }
+    double radius_km = radius_cells * std::max(h_lon, std::max(h_lat, h_r));
+    int ri = int(std::ceil(radius_km / h_lon)), rj = int(std::ceil(radius_km / h_lat)), rk = int(std::ceil(radius_km / h_r));
+    int i0 = int(std::nearbyint(fx)), j0 = int(std::nearbyint(fy)), k0 = int(std::nearbyint(fz));  // Math.Round: half to even
+    if (g.variable) rk += 2;  // extension: vertical spacing varies; the distance test below decides
+    int n = 0;
+    for (int k = std::max(0, k0 - rk); k <= std::min(g.nz - 1, k0 + rk); k++)
+        for (int j = std::max(0, j0 - rj); j <= std::min(g.ny - 1, j0 + rj); j++)
+            for (int i = std::max(0, i0 - ri); i <= std::min(g.nx - 1, i0 + ri); i++) {
+                int idx = g.index(i, j, k);
+                double dd = norm(sub(g.cartesian(i, j, k), src));
+                bool inside = std::fabs(i - fx) <= 1 && std::fabs(j - fy) <= 1 && std::fabs(k - fz) <= 1;
+                if (dd > radius_km && !inside) continue;
+                if (n < cap) {
+                    idx_out[n] = idx;
+                    t_out[n] = origin_time + dd * 0.5 * (s_src + slowness[idx]);
+                }
+                n++;
+            }
+    return n;
+}
+
+// ---- solvers ---------------------------------------------------------------------------------
+
+// SphericalEikonal.Relax (SphericalEikonal.cs:284-325), plane-ordered fast sweeping: phase 0 first
+// order, phase 1 with second-order promotion; a round is eight sweeps; a phase ends at a round in
+// which no node dropped by more than tol (reference: SettleTolerance = 1e-7, :332); tol = 0 runs
+// to the exact fixed point. max_rounds <= 0 uses SweepRoundCap (:335). rounds_out[2] receives the
+// rounds of each phase. Returns 1 when both phases settled within the cap, else 0.
+int32_t or_relax(const or_grid_def* d, const double* slowness, int32_t n_seeds, const int32_t* seed_idx,
+                 const double* seed_t, int32_t max_rounds, double tol, double* out, int32_t* rounds_out) {
+    Grid g(*d);
+    Metric m(g);
+    int n = g.count();
+    std::fill(out, out + n, kInf);
+    std::vector<uint8_t> fixed(n, 0);
+    for (int q = 0; q < n_seeds; q++) {
+        int s = seed_idx[q];
+        if (unsigned(s) >= unsigned(n)) continue;
+        out[s] = std::min(out[s], seed_t[q]);
+        fixed[s] = 1;
+    }
+    int nx = g.nx, ny = g.ny, nz = g.nz;
+    int cap = max_rounds > 0 ? max_rounds : sweep_round_cap(g);
+    int settled_all = 1;
+    for (int phase = 0; phase < 2; phase++) {
+        int settled = 0, round = 0;
+        for (round = 0; round < cap; round++) {
+            bool changed = false;
+            for (int dir = 0; dir < 8; dir++)
+                for (int p = 0; p < nx + ny + nz - 2; p++) {
+                    int i0, i1, k0, k1;
+                    plane_bounds(nx, ny, nz, p, i0, i1, k0, k1);
+                    for (int kp = k0; kp <= k1; kp++)
+                        for (int ip = i0; ip <= i1; ip++) {
+                            int jp = p - ip - kp;
+                            if (jp < 0 || jp >= ny) continue;
+                            int i = (dir & 1) ? nx - 1 - ip : ip;
+                            int j = (dir & 2) ? ny - 1 - jp : jp;
+                            int k = (dir & 4) ? nz - 1 - kp : kp;
+                            int idx = g.index(i, j, k);
+                            if (fixed[idx]) continue;
+                            double cur = out[idx];
+                            double cand = relax_node(m, slowness, out, idx, i, j, k, phase == 1);
+                            if (!(cand < cur)) continue;
+                            out[idx] = cand;
+                            if (!std::isfinite(cur) || cur - cand > tol) changed = true;
+                        }
+                }
+            if (!changed) { settled = 1; round++; break; }
+        }
+        if (rounds_out) rounds_out[phase] = round;
+        if (!settled) settled_all = 0;
+    }
+    return settled_all;
+}
+
+// SphericalEikonal.Solve (SphericalEikonal.cs:102-152): fast marching, the reference's production CPU
+// solver (and the timed CPU baseline). Seeds are imposed; neighbours are updated from Alive nodes only.
+int32_t or_fmm(const or_grid_def* d, const double* slowness, int32_t n_seeds, const int32_t* seed_idx,
+               const double* seed_t, double* out) {
+    Grid g(*d);
+    Metric m(g);
+    int n = g.count();
+    if (n_seeds == 0) return 0;
+    enum : uint8_t { Far = 0, Trial = 1, Alive = 2, Seed = 3 };
+    std::fill(out, out + n, kInf);
+    std::vector<uint8_t> status(n, Far);
+    FrontHeap heap(n, std::max(1024, n / 64));
+    for (int q = 0; q < n_seeds; q++) {
+        int s = seed_idx[q];
+        if (unsigned(s) >= unsigned(n) || !(seed_t[q] < out[s])) continue;
+        out[s] = seed_t[q];
+        status[s] = Seed;
+        heap.set(s, seed_t[q]);
+    }
+    int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+    auto alive = [&](int node) { return status[node] == Alive; };
+    // March.Axis (SphericalEikonal.cs:202-222): the term of one axis from Alive neighbours.
+    auto axis = [&](int index, int pos, int nn, int stride, double h, Term* q, int& used, bool zvar, int k) {
+        double minus = pos > 0 && alive(index - stride) ? out[index - stride] : kInf;
+        double plus = pos + 1 < nn && alive(index + stride) ? out[index + stride] : kInf;
+        double first;
+        int second;
+        bool minus_side = minus <= plus;
+        if (minus_side) { first = minus; second = pos > 1 ? index - 2 * stride : -1; }
+        else { first = plus; second = pos + 2 < nn ? index + 2 * stride : -1; }
+        if (!std::isfinite(first)) return;
+        double t2 = second >= 0 && alive(second) ? out[second] : kInf;
+        if (!zvar) {
+            if (std::isfinite(t2) && t2 <= first) q[used] = {(4 * first - t2) / 3, 2 * h / 3, first};
+            else q[used] = {first, h, first};
+        } else {
+            double h1 = minus_side ? m.dz[k - 1] : m.dz[k];
+            if (std::isfinite(t2) && t2 <= first) {
+                double h2 = minus_side ? m.dz[k - 2] : m.dz[k + 1];
+                double a = (2 * h1 + h2) / (h1 * (h1 + h2));
+                double b = (h1 + h2) / (h1 * h2);
+                double c = h1 / (h2 * (h1 + h2));
+                q[used] = {(b * first - c * t2) / a, 1 / a, first};
+            } else {
+                q[used] = {first, h1, first};
+            }
+        }
+        used++;
+    };
+    // March.SolveNode (SphericalEikonal.cs:167-200).
+    auto solve_node = [&](int index, int i, int j, int k) -> double {
+        double s = slowness[index];
+        if (!(s > 0) || !std::isfinite(s)) return kInf;
+        Term q[3];
+        int used = 0;
+        axis(index, i, nx, 1, m.hlon[size_t(k) * ny + j], q, used, false, k);
+        axis(index, j, ny, nx, m.hlat[k], q, used, false, k);
+        axis(index, k, nz, nxy, m.hr, q, used, g.variable, k);
+        if (used == 0) return kInf;
+        sort_terms(q, used);
+        return godunov(q, used, s);
+    };
+    auto update = [&](int nidx, int i, int j, int k) {
+        if (status[nidx] >= Alive) return;
+        double t = solve_node(nidx, i, j, k);
+        if (!(t < out[nidx])) return;
+        out[nidx] = t;
+        status[nidx] = Trial;
+        heap.set(nidx, t);
+    };
+    int idx;
+    while (heap.pop(idx)) {
+        status[idx] = Alive;
+        int k = idx / nxy, rest = idx - k * nxy, j = rest / nx, i = rest - j * nx;
+        if (i > 0) update(idx - 1, i - 1, j, k);
+        if (i + 1 < nx) update(idx + 1, i + 1, j, k);
+        if (j > 0) update(idx - nx, i, j - 1, k);
+        if (j + 1 < ny) update(idx + nx, i, j + 1, k);
+        if (k > 0) update(idx - nxy, i, j, k - 1);
+        if (k + 1 < nz) update(idx + nxy, i, j, k + 1);
+    }
+    return 1;
+}
+
+// Many fast-marching solves at once, one field per thread (TravelTimeTable.cs:332-354, 396-400):
+// fields f uses seeds [seed_off[f], seed_off[f+1]) and slowness slowness + sl_of[f]*n.
+void or_fmm_many(const or_grid_def* d, const double* slowness, const int32_t* sl_of, int32_t n_fields,
+                 const int32_t* seed_off, const int32_t* seed_idx, const double* seed_t, double* out,
+                 int32_t threads) {
+    int n = d->nx * d->ny * d->nz;
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (;;) {
+            int f = next.fetch_add(1);
+            if (f >= n_fields) return;
+            or_fmm(d, slowness + size_t(sl_of[f]) * n, seed_off[f + 1] - seed_off[f], seed_idx + seed_off[f],
+                   seed_t + seed_off[f], out + size_t(f) * n);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); t++) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+}
+
+// ---- tables and rays -------------------------------------------------------------------------
+
+// TravelTimeTable.Write's float32 rounding (TravelTimeTable.cs:73).
+void or_to_table(const double* t, int64_t n, float* out) {
+    for (int64_t q = 0; q < n; q++) out[q] = std::isfinite(t[q]) ? float(t[q]) : std::numeric_limits<float>::infinity();
+}
+
+double or_table_time(const or_grid_def* d, const float* table, double lon, double lat, double dep) {
+    Grid g(*d);
+    Table tb{g, table, 0, 0, 0};
+    return tb.time(lon, lat, dep);
+}
+
+void or_table_gradient(const or_grid_def* d, const float* table, double lon, double lat, double dep, double* g3) {
+    Grid g(*d);
+    Table tb{g, table, 0, 0, 0};
+    tb.gradient(lon, lat, dep, g3[0], g3[1], g3[2]);
+}
+
+// RayTracing.Backtrack: writes up to cap points (lon, lat, depth interleaved); returns the point
+// count, 0 when the reference returns null, or -needed when cap is too small.
+int32_t or_backtrack(const or_grid_def* d, const float* table, double st_lon, double st_lat, double st_dep,
+                     double lon, double lat, double dep, double step_km, double* pts, int32_t cap) {
+    Grid g(*d);
+    Table tb{g, table, st_lon, st_lat, st_dep};
+    std::vector<Geo> path;
+    if (!backtrack(tb, lon, lat, dep, step_km, path)) return 0;
+    if (int(path.size()) > cap) return -int(path.size());
+    for (size_t q = 0; q < path.size(); q++) {
+        pts[3 * q] = path[q].lon; pts[3 * q + 1] = path[q].lat; pts[3 * q + 2] = path[q].depth;
+    }
+    return int(path.size());
+}
+
+// RayTracing.Kernel over a given polyline on the inversion grid; nodes in first-visit order.
+int32_t or_kernel(const or_grid_def* inv, const double* pts, int32_t n_pts, int32_t* nodes, double* lens, int32_t cap) {
+    Grid g(*inv);
+    std::vector<Geo> ray(n_pts);
+    for (int q = 0; q < n_pts; q++) ray[q] = {pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]};
+    std::vector<int> keys;
+    std::vector<double> vals;
+    ray_kernel(g, ray, keys, vals);
+    if (int(keys.size()) > cap) return -int(keys.size());
+    for (size_t q = 0; q < keys.size(); q++) { nodes[q] = keys[q]; lens[q] = vals[q]; }
+    return int(keys.size());
+}
+
+// One arrival of RayKernels.Compute (Tomography/RayKernels.cs:77-97): backtrack on the station's
+// table, TCalc and the source gradient, the kernel on the inversion grid, nodes ascending, lengths
+// cast to float32. Returns nnz, 0 for a dropped arrival, or -needed when cap is too small.
+int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, double st_lat, double st_dep,
+                   const or_grid_def* inv, double ev_lon, double ev_lat, double ev_dep, double step_km,
+                   int32_t* nodes, float* lens, int32_t cap, double* tcalc_grad4) {
+    Grid g(*fwd);
+    Grid ig(*inv);
+    Table tb{g, table, st_lon, st_lat, st_dep};
+    std::vector<Geo> path;
+    if (!backtrack(tb, ev_lon, ev_lat, ev_dep, step_km, path)) return 0;
+    double tcalc = tb.time(ev_lon, ev_lat, ev_dep);
+    double ge, gn, gz;
+    tb.gradient(ev_lon, ev_lat, ev_dep, ge, gn, gz);
+    if (!std::isfinite(tcalc)) return 0;
+    std::vector<int> keys;
+    std::vector<double> vals;
+    ray_kernel(ig, path, keys, vals);
+    if (int(keys.size()) > cap) return -int(keys.size());
+    std::vector<int> order(keys.size());
+    for (size_t q = 0; q < order.size(); q++) order[q] = int(q);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+    for (size_t q = 0; q < order.size(); q++) {
+        nodes[q] = keys[order[q]];
+        lens[q] = float(vals[order[q]]);
+    }
+    tcalc_grad4[0] = tcalc; tcalc_grad4[1] = ge; tcalc_grad4[2] = gn; tcalc_grad4[3] = gz;
+    return int(keys.size());
+}
+
+// Many arrivals on a thread pool (RayKernels.cs:67): arrival a traces on table tables + tab_of[a]*n
+// with station st[3*a..]; writes row a's nnz into nnz[a] and its entries at [a*cap_per_row, ...).
+void or_ray_rows_many(const or_grid_def* fwd, const float* tables, const int32_t* tab_of, const double* st,
+                      const or_grid_def* inv, const double* ev, int32_t n_rays, double step_km, int32_t cap_per_row,
+                      int32_t* nnz, int32_t* nodes, float* lens, double* tcalc_grad4, int32_t threads) {
+    int64_t n = int64_t(fwd->nx) * fwd->ny * fwd->nz;
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (;;) {
+            int a = next.fetch_add(1);
+            if (a >= n_rays) return;
+            nnz[a] = or_ray_row(fwd, tables + size_t(tab_of[a]) * n, st[3 * a], st[3 * a + 1], st[3 * a + 2], inv,
+                                ev[3 * a], ev[3 * a + 1], ev[3 * a + 2], step_km, nodes + size_t(a) * cap_per_row,
+                                lens + size_t(a) * cap_per_row, cap_per_row, tcalc_grad4 + 4 * size_t(a));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); t++) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+}
+
+// Many Relax solves on a thread pool (parity checks of batches).
+void or_relax_many(const or_grid_def* d, const double* slowness, const int32_t* sl_of, int32_t n_fields,
+                   const int32_t* seed_off, const int32_t* seed_idx, const double* seed_t, double tol, double* out,
+                   int32_t* rounds, int32_t* settled, int32_t threads) {
+    int n = d->nx * d->ny * d->nz;
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (;;) {
+            int f = next.fetch_add(1);
+            if (f >= n_fields) return;
+            settled[f] = or_relax(d, slowness + size_t(sl_of[f]) * n, seed_off[f + 1] - seed_off[f],
+                                  seed_idx + seed_off[f], seed_t + seed_off[f], 0, tol, out + size_t(f) * n,
+                                  rounds + 2 * f);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); t++) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+}
+
+}  // extern "C"

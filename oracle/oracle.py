@@ -1,0 +1,296 @@
+"""ctypes front end of the C++ oracle (oracle.cpp) — TEST INFRASTRUCTURE ONLY.
+
+The oracle restates the reference's CPU solvers (Forward/SphericalEikonal.cs, Forward/RayTracing.cs,
+Forward/TravelTimeTable.cs, Tomography/RayKernels.cs). Parity status: pinned by the reference's own
+known-answer tests, not by bitwise reference output (the reference is C#/.NET and cannot run here).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+class GridDef(C.Structure):
+    """GridDefinition (Geo/SphericalGrid.cs:13-31) plus an optional depth array."""
+
+    _fields_ = [
+        ("min_lon", C.c_double), ("max_lon", C.c_double),
+        ("min_lat", C.c_double), ("max_lat", C.c_double),
+        ("min_depth_km", C.c_double), ("max_depth_km", C.c_double),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("_pad", C.c_int32),
+        ("depth_km", C.POINTER(C.c_double)),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (g++ -O2 -ffp-contract=off)."""
+    src = os.path.join(HERE, "oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        d, i32, i64, dp, fp, ip = C.c_double, C.c_int32, C.c_int64, P(C.c_double), P(C.c_float), P(C.c_int32)
+        g = P(GridDef)
+        sig = {
+            "or_metric": (None, [g, dp, dp, dp, dp]),
+            "or_grid_coords": (None, [g, dp, dp, dp, dp]),
+            "or_min_spacing_km": (d, [g]),
+            "or_to_cartesian": (None, [d, d, d, dp]),
+            "or_from_cartesian": (None, [dp, dp]),
+            "or_trilinear": (None, [g, d, d, d, ip, dp]),
+            "or_interpolate": (d, [g, dp, d, d, d]),
+            "or_point_source": (i32, [g, dp, d, d, d, d, d, ip, dp, i32]),
+            "or_relax": (i32, [g, dp, i32, ip, dp, i32, d, dp, ip]),
+            "or_fmm": (i32, [g, dp, i32, ip, dp, dp]),
+            "or_fmm_many": (None, [g, dp, ip, i32, ip, ip, dp, dp, i32]),
+            "or_relax_many": (None, [g, dp, ip, i32, ip, ip, dp, d, dp, ip, ip, i32]),
+            "or_to_table": (None, [dp, i64, fp]),
+            "or_table_time": (d, [g, fp, d, d, d]),
+            "or_table_gradient": (None, [g, fp, d, d, d, dp]),
+            "or_backtrack": (i32, [g, fp, d, d, d, d, d, d, d, dp, i32]),
+            "or_kernel": (i32, [g, dp, i32, ip, dp, i32]),
+            "or_ray_row": (i32, [g, fp, d, d, d, g, d, d, d, d, ip, fp, i32, dp]),
+            "or_ray_rows_many": (None, [g, fp, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class Grid:
+    """A grid definition with the ctypes struct kept alive (and its depth array, if variable)."""
+
+    def __init__(self, min_lon, max_lon, min_lat, max_lat, min_depth_km, max_depth_km, nx, ny, nz, depth_km=None):
+        self.depth = None if depth_km is None else np.ascontiguousarray(depth_km, dtype=np.float64)
+        self.struct = GridDef(min_lon, max_lon, min_lat, max_lat, min_depth_km, max_depth_km, nx, ny, nz, 0,
+                              None if self.depth is None else _p(self.depth, C.c_double))
+        self.nx, self.ny, self.nz = nx, ny, nz
+
+    @classmethod
+    def of(cls, g):
+        """From any object with the GridDefinition fields (e.g. tomostar_b200.grid.GridDef)."""
+        return cls(g.min_lon, g.max_lon, g.min_lat, g.max_lat, g.min_depth_km, g.max_depth_km, g.nx, g.ny, g.nz,
+                   getattr(g, "depth_km", None))
+
+    @property
+    def count(self):
+        return self.nx * self.ny * self.nz
+
+    @property
+    def ref(self):
+        return C.byref(self.struct)
+
+
+def metric(g: Grid):
+    hlon = np.empty(g.ny * g.nz)
+    hlat = np.empty(g.nz)
+    hr = C.c_double()
+    dz = np.empty(max(1, g.nz - 1))
+    lib().or_metric(g.ref, _p(hlon, C.c_double), _p(hlat, C.c_double), C.byref(hr), _p(dz, C.c_double))
+    return hlon, hlat, hr.value, (dz if g.depth is not None else None)
+
+
+def coords(g: Grid):
+    lon, lat, cl, dep = np.empty(g.nx), np.empty(g.ny), np.empty(g.ny), np.empty(g.nz)
+    lib().or_grid_coords(g.ref, *(_p(a, C.c_double) for a in (lon, lat, cl, dep)))
+    return lon, lat, cl, dep
+
+
+def min_spacing_km(g: Grid) -> float:
+    return lib().or_min_spacing_km(g.ref)
+
+
+def to_cartesian(lon, lat, dep):
+    out = np.empty(3)
+    lib().or_to_cartesian(lon, lat, dep, _p(out, C.c_double))
+    return out
+
+
+def trilinear(g: Grid, lon, lat, dep):
+    nodes = np.empty(8, np.int32)
+    w = np.empty(8)
+    lib().or_trilinear(g.ref, lon, lat, dep, _p(nodes, C.c_int32), _p(w, C.c_double))
+    return nodes, w
+
+
+def interpolate(g: Grid, field, lon, lat, dep):
+    f = np.ascontiguousarray(field, np.float64)
+    return lib().or_interpolate(g.ref, _p(f, C.c_double), lon, lat, dep)
+
+
+def point_source(g: Grid, slowness, lon, lat, dep, origin_time=0.0, radius_cells=3.0):
+    """SphericalEikonal.PointSource: (node indices int32, times float64)."""
+    s = np.ascontiguousarray(slowness, np.float64)
+    cap = 4096
+    while True:
+        idx = np.empty(cap, np.int32)
+        t = np.empty(cap)
+        n = lib().or_point_source(g.ref, _p(s, C.c_double), lon, lat, dep, origin_time, radius_cells,
+                                  _p(idx, C.c_int32), _p(t, C.c_double), cap)
+        if n <= cap:
+            return idx[:n].copy(), t[:n].copy()
+        cap = n
+
+
+def relax(g: Grid, slowness, seed_idx, seed_t, tol=1e-7, max_rounds=0):
+    """SphericalEikonal.Relax; returns (field, settled, rounds[2])."""
+    s = np.ascontiguousarray(slowness, np.float64)
+    si = np.ascontiguousarray(seed_idx, np.int32)
+    st = np.ascontiguousarray(seed_t, np.float64)
+    out = np.empty(g.count)
+    rounds = np.zeros(2, np.int32)
+    ok = lib().or_relax(g.ref, _p(s, C.c_double), len(si), _p(si, C.c_int32), _p(st, C.c_double), max_rounds, tol,
+                        _p(out, C.c_double), _p(rounds, C.c_int32))
+    return out, bool(ok), rounds
+
+
+def fmm(g: Grid, slowness, seed_idx, seed_t):
+    """SphericalEikonal.Solve (fast marching)."""
+    s = np.ascontiguousarray(slowness, np.float64)
+    si = np.ascontiguousarray(seed_idx, np.int32)
+    st = np.ascontiguousarray(seed_t, np.float64)
+    out = np.empty(g.count)
+    lib().or_fmm(g.ref, _p(s, C.c_double), len(si), _p(si, C.c_int32), _p(st, C.c_double), _p(out, C.c_double))
+    return out
+
+
+def _seed_arrays(seed_sets):
+    off = np.zeros(len(seed_sets) + 1, np.int32)
+    for f, (si, _) in enumerate(seed_sets):
+        off[f + 1] = off[f] + len(si)
+    idx = np.concatenate([np.asarray(si, np.int32) for si, _ in seed_sets]) if seed_sets else np.zeros(0, np.int32)
+    t = np.concatenate([np.asarray(st, np.float64) for _, st in seed_sets]) if seed_sets else np.zeros(0)
+    return off, np.ascontiguousarray(idx), np.ascontiguousarray(t)
+
+
+def fmm_many(g: Grid, slownesses, sl_of, seed_sets, threads=None):
+    """Fast marching of many fields on a thread pool; slownesses is (n_models, n)."""
+    s = np.ascontiguousarray(slownesses, np.float64)
+    so = np.ascontiguousarray(sl_of, np.int32)
+    off, idx, t = _seed_arrays(seed_sets)
+    out = np.empty((len(seed_sets), g.count))
+    lib().or_fmm_many(g.ref, _p(s, C.c_double), _p(so, C.c_int32), len(seed_sets), _p(off, C.c_int32),
+                      _p(idx, C.c_int32), _p(t, C.c_double), _p(out, C.c_double), threads or os.cpu_count())
+    return out
+
+
+def relax_many(g: Grid, slownesses, sl_of, seed_sets, tol=1e-7, threads=None):
+    s = np.ascontiguousarray(slownesses, np.float64)
+    so = np.ascontiguousarray(sl_of, np.int32)
+    off, idx, t = _seed_arrays(seed_sets)
+    nf = len(seed_sets)
+    out = np.empty((nf, g.count))
+    rounds = np.zeros((nf, 2), np.int32)
+    settled = np.zeros(nf, np.int32)
+    lib().or_relax_many(g.ref, _p(s, C.c_double), _p(so, C.c_int32), nf, _p(off, C.c_int32), _p(idx, C.c_int32),
+                        _p(t, C.c_double), tol, _p(out, C.c_double), _p(rounds, C.c_int32),
+                        _p(settled, C.c_int32), threads or os.cpu_count())
+    return out, settled.astype(bool), rounds
+
+
+def to_table(t):
+    """TravelTimeTable.Write's float32 rounding (non-finite → +inf)."""
+    t = np.ascontiguousarray(t, np.float64)
+    out = np.empty(t.shape, np.float32)
+    lib().or_to_table(_p(t, C.c_double), t.size, _p(out, C.c_float))
+    return out
+
+
+def table_time(g: Grid, table, lon, lat, dep):
+    tb = np.ascontiguousarray(table, np.float32)
+    return lib().or_table_time(g.ref, _p(tb, C.c_float), lon, lat, dep)
+
+
+def table_gradient(g: Grid, table, lon, lat, dep):
+    tb = np.ascontiguousarray(table, np.float32)
+    out = np.empty(3)
+    lib().or_table_gradient(g.ref, _p(tb, C.c_float), lon, lat, dep, _p(out, C.c_double))
+    return out
+
+
+def backtrack(g: Grid, table, station, lon, lat, dep, step_km):
+    """RayTracing.Backtrack: (n, 3) array of (lon, lat, depth) points, or None."""
+    tb = np.ascontiguousarray(table, np.float32)
+    cap = 4096
+    while True:
+        pts = np.empty(3 * cap)
+        n = lib().or_backtrack(g.ref, _p(tb, C.c_float), station[0], station[1], station[2], lon, lat, dep, step_km,
+                               _p(pts, C.c_double), cap)
+        if n == 0:
+            return None
+        if n > 0:
+            return pts[: 3 * n].reshape(n, 3).copy()
+        cap = -n
+
+
+def kernel(inv: Grid, pts):
+    """RayTracing.Kernel: (nodes in first-visit order, double lengths)."""
+    p = np.ascontiguousarray(pts, np.float64).reshape(-1)
+    cap = 8192
+    while True:
+        nodes = np.empty(cap, np.int32)
+        lens = np.empty(cap)
+        n = lib().or_kernel(inv.ref, _p(p, C.c_double), len(p) // 3, _p(nodes, C.c_int32), _p(lens, C.c_double), cap)
+        if n >= 0:
+            return nodes[:n].copy(), lens[:n].copy()
+        cap = -n
+
+
+def ray_row(fwd: Grid, table, station, inv: Grid, event, step_km):
+    """One RayKernels arrival: (nodes asc int32, lengths float32, tcalc, (ge, gn, gz)) or None."""
+    tb = np.ascontiguousarray(table, np.float32)
+    cap = 8192
+    while True:
+        nodes = np.empty(cap, np.int32)
+        lens = np.empty(cap, np.float32)
+        tg = np.empty(4)
+        n = lib().or_ray_row(fwd.ref, _p(tb, C.c_float), station[0], station[1], station[2], inv.ref, event[0],
+                             event[1], event[2], step_km, _p(nodes, C.c_int32), _p(lens, C.c_float), cap,
+                             _p(tg, C.c_double))
+        if n == 0:
+            return None
+        if n > 0:
+            return nodes[:n].copy(), lens[:n].copy(), tg[0], tg[1:].copy()
+        cap = -n
+
+
+def ray_rows_many(fwd: Grid, tables, tab_of, stations, inv: Grid, events, step_km, cap_per_row=4096, threads=None):
+    """Many arrivals on a thread pool. tables (n_tables, n) float32; stations/events (n_rays, 3)."""
+    tb = np.ascontiguousarray(tables, np.float32)
+    to = np.ascontiguousarray(tab_of, np.int32)
+    st = np.ascontiguousarray(stations, np.float64)
+    ev = np.ascontiguousarray(events, np.float64)
+    nr = len(to)
+    nnz = np.zeros(nr, np.int32)
+    nodes = np.empty(nr * cap_per_row, np.int32)
+    lens = np.empty(nr * cap_per_row, np.float32)
+    tg = np.empty((nr, 4))
+    lib().or_ray_rows_many(fwd.ref, _p(tb, C.c_float), _p(to, C.c_int32), _p(st, C.c_double), inv.ref,
+                           _p(ev, C.c_double), nr, step_km, cap_per_row, _p(nnz, C.c_int32), _p(nodes, C.c_int32),
+                           _p(lens, C.c_float), _p(tg, C.c_double), threads or os.cpu_count())
+    return nnz, nodes.reshape(nr, cap_per_row), lens.reshape(nr, cap_per_row), tg

@@ -1,0 +1,94 @@
+"""Loads libtomostar_cuda.so (built in-tree) and declares the C ABI of include/tomostar_cuda.h.
+
+There is no fallback: if the library is missing the import of the solver fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtomostar_cuda.so")
+
+TS_OK, TS_E_ARG, TS_E_CUDA, TS_E_NOMEM, TS_E_UNSETTLED, TS_E_CANCELLED = 0, 1, 2, 3, 4, 5
+TS_E_TIMEOUT, TS_E_CAPACITY, TS_E_NOSEEDS, TS_E_SELFTEST, TS_E_NODEVICE = 6, 7, 8, 9, 10
+F64, F32 = 64, 32
+MODE_ENGINE, MODE_PLAIN = 0, 1
+OUT_F64, OUT_F32 = 0, 1
+
+ERROR_NAMES = {
+    TS_E_ARG: "invalid argument", TS_E_CUDA: "CUDA error", TS_E_NOMEM: "out of device memory",
+    TS_E_UNSETTLED: "not settled", TS_E_CANCELLED: "cancelled", TS_E_TIMEOUT: "device wait timed out",
+    TS_E_CAPACITY: "capacity", TS_E_NOSEEDS: "no seed nodes", TS_E_SELFTEST: "self-test failed",
+    TS_E_NODEVICE: "no CUDA device",
+}
+
+
+class TsError(RuntimeError):
+    def __init__(self, code: int, reason: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {reason}")
+        self.code = code
+        self.reason = reason
+
+
+class GridStruct(C.Structure):
+    """ts_grid = GridDefinition (Geo/SphericalGrid.cs:13-31) + optional depth array."""
+
+    _fields_ = [
+        ("min_lon", C.c_double), ("max_lon", C.c_double),
+        ("min_lat", C.c_double), ("max_lat", C.c_double),
+        ("min_depth_km", C.c_double), ("max_depth_km", C.c_double),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("reserved", C.c_int32),
+        ("depth_km", C.POINTER(C.c_double)),
+    ]
+
+
+class EikStats(C.Structure):
+    _fields_ = [
+        ("rounds", C.c_int32 * 2), ("launches", C.c_int32), ("reserved", C.c_int32),
+        ("node_updates", C.c_int64), ("tile_visits", C.c_int64), ("device_ms", C.c_double),
+    ]
+
+
+# Every symbol the header declares, with its ctypes signature.
+_P = C.POINTER
+_vp, _i32, _i64, _d = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+_ip, _dp, _fp, _u8p = _P(C.c_int32), _P(C.c_double), _P(C.c_float), _P(C.c_uint8)
+_gp = _P(GridStruct)
+SIGNATURES = {
+    "ts_cuda_create": (C.c_int, [_i32, _P(_vp)]),
+    "ts_cuda_destroy": (None, [_vp]),
+    "ts_last_error": (C.c_char_p, [_vp]),
+    "ts_device_name": (C.c_int, [_vp, C.c_char_p, _i32]),
+    "ts_last_stats": (C.c_char_p, [_vp]),
+    "ts_set_cancel": (None, [_vp, _i32]),
+    "ts_eik_suggest_batch": (_i32, [_vp, _i64, _i32]),
+    "ts_engine_shapes": (_i32, [_ip, _i32]),
+    "ts_engine_set_tile": (C.c_int, [_vp, _i32, _i32]),
+    "ts_point_source": (_i32, [_gp, _dp, _d, _d, _d, _d, _d, _ip, _dp, _i32]),
+    "ts_eik_solve": (C.c_int, [_vp, _gp, _dp, _i32, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32, _P(EikStats)]),
+    "ts_cuda_selftest": (C.c_int, [_vp, _i32, _dp, C.c_char_p, _i32]),
+    "ts_rays_trace": (C.c_int, [_vp, _gp, _i32, _fp, _dp, _gp, _i32, _ip, _dp, _d, _P(_vp)]),
+    "ts_forward": (C.c_int, [_vp, _gp, _dp, _i32, _gp, _i32, _dp, _i32, _dp, _i32, _ip, _ip, _ip, _i32, _d, _P(_vp),
+                             _P(EikStats)]),
+    "ts_rows_info": (C.c_int, [_vp, _ip, _P(C.c_int64)]),
+    "ts_rows_copy": (C.c_int, [_vp, _ip, _ip, _fp, _dp, _u8p]),
+    "ts_rows_free": (None, [_vp]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """The library with every entry point typed; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run tomostar_b200.build.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib

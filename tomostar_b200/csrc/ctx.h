@@ -1,0 +1,96 @@
+// The context behind ts_ctx*: one CUDA device, one stream, cached device buffers, the last error.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "../../include/tomostar_cuda.h"
+
+struct ts_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;  // calls on one context are serialised (EikonalOpenCl.cs:64,165)
+    std::string err;
+    std::string stats;
+    std::string name;
+    int sm_count = 0;
+    size_t total_mem = 0;
+    volatile int* cancel_host = nullptr;  // host-mapped, read by kernels between rounds
+    int* cancel_dev = nullptr;
+    int tile_f64 = 0, tile_f32 = 0;       // engine tile shape per precision
+
+    struct Buf {
+        void* p = nullptr;
+        size_t n = 0;
+    };
+    std::map<std::string, Buf> bufs;
+
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+    // A grow-only named device buffer; nullptr (with err set) when the device is out of memory.
+    void* buf(const std::string& key, size_t bytes) {
+        Buf& b = bufs[key];
+        if (b.n >= bytes && b.p) return b.p;
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        if (cudaMalloc(&b.p, want) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            err = "device buffer '" + key + "' of " + std::to_string(want) + " bytes (too large for the device?)";
+            return nullptr;
+        }
+        b.n = want;
+        return b.p;
+    }
+    void release(const std::string& key) {
+        auto it = bufs.find(key);
+        if (it == bufs.end()) return;
+        if (it->second.p) cudaFree(it->second.p);
+        bufs.erase(it);
+    }
+};
+
+#define TS_CUDA_TRY(ctx, call)                                                                        \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) {                                                                      \
+            char b_[512];                                                                             \
+            snprintf(b_, sizeof b_, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return (ctx)->fail(e_ == cudaErrorMemoryAllocation ? TS_E_NOMEM : TS_E_CUDA, b_);        \
+        }                                                                                             \
+    } while (0)
+
+#define TS_BUF(ctx, var, type, key, count)                                  \
+    type* var = static_cast<type*>((ctx)->buf((key), sizeof(type) * size_t(count))); \
+    if (!var) return TS_E_NOMEM
+
+namespace ts {
+namespace eik {
+
+// Host-side entry points of the eikonal solvers (eik_host.cu).
+struct SolveIn {
+    const ts_grid* grid;
+    const double* slowness;
+    int n_fields;
+    const int32_t* seed_offsets;
+    const int32_t* seed_index;
+    const double* seed_time;
+    int precision;
+    int mode;
+    double tol;
+    int max_rounds;
+};
+
+int solve_to_device(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_stats* stats);
+int copy_fields_out(ts_ctx* ctx, const void* fields_dev, int precision, int64_t count, void* out, int out_type);
+
+}  // namespace eik
+}  // namespace ts

@@ -1,0 +1,323 @@
+// The tiled engine's host side: lays out the job's descriptors in one device arena, seeds the
+// fields, and makes the cooperative persistent launch.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "eik_engine.h"
+#include "eik_kernels.cuh"
+
+namespace ts {
+namespace eik {
+
+const std::vector<TileShapeInfo>& tile_shapes() {
+    static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}};
+    return shapes;
+}
+
+namespace {
+
+// A host image of device memory: aligned sub-allocations, uploaded in one copy.
+struct Arena {
+    std::vector<uint8_t> h;
+    size_t add(size_t bytes, size_t align = 16) {
+        size_t off = (h.size() + align - 1) / align * align;
+        h.resize(off + std::max<size_t>(bytes, 1), 0);
+        return off;
+    }
+    template <typename T>
+    T* at(size_t off) { return reinterpret_cast<T*>(h.data() + off); }
+};
+
+template <typename Real>
+__global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const GridDesc* __restrict__ grids,
+                                   uint8_t* __restrict__ dirty_base, const int64_t* __restrict__ dirty_off) {
+    const FieldDesc<Real>& fd = fields[blockIdx.y];
+    const GridDesc& g = grids[fd.grid];
+    int64_t n = int64_t(g.nx) * g.ny * g.nz;
+    const Real inf = real_inf<Real>();
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < n; q += int64_t(gridDim.x) * blockDim.x)
+        fd.T[q] = inf;
+    int64_t nt = int64_t(g.tx) * g.ty * g.tz;
+    uint8_t* d = dirty_base + dirty_off[blockIdx.y];
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nt; q += int64_t(gridDim.x) * blockDim.x)
+        d[q] = 1;
+}
+
+template <typename Real>
+__global__ void seed_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const int* __restrict__ field_of,
+                                   const int32_t* __restrict__ node, const double* __restrict__ t, int count) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) fields[field_of[q]].T[node[q]] = Real(t[q]);
+}
+
+template <typename Real, int BX, int BY, int BZ, int WARPS>
+int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
+    using S = Shape<BX, BY, BZ>;
+    const int nf = int(job.fields.size());
+    const int ng = int(job.grids.size());
+    bool any_var = false;
+    for (auto* g : job.grids) any_var |= g->variable;
+
+    Arena A;
+    // Grids.
+    std::vector<size_t> o_diag_off(ng), o_diag_tiles(ng), o_hlon(ng), o_hlat(ng), o_zc(ng);
+    std::vector<int> tx(ng), ty(ng), tz(ng), ndiag(ng);
+    size_t o_grids = A.add(sizeof(GridDesc) * ng);
+    for (int gi = 0; gi < ng; gi++) {
+        const host::Grid& g = *job.grids[gi];
+        const host::Metric& m = *job.metrics[gi];
+        tx[gi] = (g.nx + BX - 1) / BX;
+        ty[gi] = (g.ny + BY - 1) / BY;
+        tz[gi] = (g.nz + BZ - 1) / BZ;
+        if (tx[gi] > 1024 || ty[gi] > 1024 || tz[gi] > 1024) return ctx->fail(TS_E_ARG, "grid too large for the tile table");
+        ndiag[gi] = tx[gi] + ty[gi] + tz[gi] - 2;
+        int nt = tx[gi] * ty[gi] * tz[gi];
+        o_diag_off[gi] = A.add(sizeof(int) * (ndiag[gi] + 1));
+        o_diag_tiles[gi] = A.add(sizeof(uint32_t) * nt);
+        // Canonical tiles ordered by diagonal (counting sort).
+        std::vector<int> cnt(ndiag[gi] + 1, 0);
+        for (int c = 0; c < tz[gi]; c++)
+            for (int b = 0; b < ty[gi]; b++)
+                for (int a = 0; a < tx[gi]; a++) cnt[a + b + c + 1]++;
+        for (int q = 0; q < ndiag[gi]; q++) cnt[q + 1] += cnt[q];
+        int* doff = A.at<int>(o_diag_off[gi]);
+        for (int q = 0; q <= ndiag[gi]; q++) doff[q] = cnt[q];
+        std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+        uint32_t* dt = A.at<uint32_t>(o_diag_tiles[gi]);
+        for (int c = 0; c < tz[gi]; c++)
+            for (int b = 0; b < ty[gi]; b++)
+                for (int a = 0; a < tx[gi]; a++) dt[pos[a + b + c]++] = uint32_t(a) | (uint32_t(b) << 10) | (uint32_t(c) << 20);
+        o_hlon[gi] = A.add(sizeof(Real) * m.hlon.size());
+        for (size_t q = 0; q < m.hlon.size(); q++) A.at<Real>(o_hlon[gi])[q] = Real(m.hlon[q]);
+        o_hlat[gi] = A.add(sizeof(Real) * m.hlat.size());
+        for (size_t q = 0; q < m.hlat.size(); q++) A.at<Real>(o_hlat[gi])[q] = Real(m.hlat[q]);
+        o_zc[gi] = A.add(sizeof(Real) * std::max<size_t>(1, m.zc.size()));
+        for (size_t q = 0; q < m.zc.size(); q++) A.at<Real>(o_zc[gi])[q] = Real(m.zc[q]);
+    }
+    // Seed tiles of each field (sorted by tile id) with their fixed-node masks.
+    std::vector<int> seed_begin(nf), seed_count(nf);
+    std::vector<int> st_tile;
+    std::vector<uint32_t> st_mask;
+    std::vector<int> sc_field;
+    std::vector<int32_t> sc_node;
+    std::vector<double> sc_t;
+    for (int f = 0; f < nf; f++) {
+        const EngineField& ef = job.fields[f];
+        const host::Grid& g = *job.grids[ef.grid];
+        const int gi = ef.grid;
+        std::vector<std::pair<int, int>> tl;  // (tile, local)
+        for (size_t q = 0; q < ef.seed_idx->size(); q++) {
+            int node = (*ef.seed_idx)[q];
+            int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+            int tid = ((k / BZ) * ty[gi] + j / BY) * tx[gi] + i / BX;
+            int loc = ((k % BZ) * BY + j % BY) * BX + i % BX;
+            tl.push_back({tid, loc});
+            sc_field.push_back(f);
+            sc_node.push_back(node);
+            sc_t.push_back((*ef.seed_t)[q]);
+        }
+        std::sort(tl.begin(), tl.end());
+        seed_begin[f] = int(st_tile.size());
+        for (size_t q = 0; q < tl.size(); q++) {
+            if (q == 0 || tl[q].first != tl[q - 1].first) {
+                st_tile.push_back(tl[q].first);
+                st_mask.resize(st_mask.size() + S::MW, 0u);
+            }
+            st_mask[(st_tile.size() - 1) * S::MW + tl[q].second / 32] |= 1u << (tl[q].second % 32);
+        }
+        seed_count[f] = int(st_tile.size()) - seed_begin[f];
+    }
+    size_t o_seed_tile = A.add(sizeof(int) * std::max<size_t>(1, st_tile.size()));
+    std::copy(st_tile.begin(), st_tile.end(), A.at<int>(o_seed_tile));
+    size_t o_seed_mask = A.add(sizeof(uint32_t) * std::max<size_t>(1, st_mask.size()));
+    std::copy(st_mask.begin(), st_mask.end(), A.at<uint32_t>(o_seed_mask));
+    size_t o_sc_field = A.add(sizeof(int) * sc_field.size());
+    std::copy(sc_field.begin(), sc_field.end(), A.at<int>(o_sc_field));
+    size_t o_sc_node = A.add(sizeof(int32_t) * sc_node.size());
+    std::copy(sc_node.begin(), sc_node.end(), A.at<int32_t>(o_sc_node));
+    size_t o_sc_t = A.add(sizeof(double) * sc_t.size(), 8);
+    std::copy(sc_t.begin(), sc_t.end(), A.at<double>(o_sc_t));
+    // Node planes of the canonical tile.
+    size_t o_ptab = A.add(sizeof(uint16_t) * S::N);
+    size_t o_poff = A.add(sizeof(int) * (S::NPLANES + 1));
+    {
+        std::vector<int> cnt(S::NPLANES + 1, 0);
+        for (int k = 0; k < BZ; k++)
+            for (int j = 0; j < BY; j++)
+                for (int i = 0; i < BX; i++) cnt[i + j + k + 1]++;
+        for (int p = 0; p < S::NPLANES; p++) cnt[p + 1] += cnt[p];
+        std::copy(cnt.begin(), cnt.end(), A.at<int>(o_poff));
+        std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+        uint16_t* pt = A.at<uint16_t>(o_ptab);
+        for (int k = 0; k < BZ; k++)
+            for (int j = 0; j < BY; j++)
+                for (int i = 0; i < BX; i++) pt[pos[i + j + k]++] = uint16_t(i | (j << 5) | (k << 10));
+    }
+    // Plan: one group per grid that has fields, fields ordered by group.
+    std::vector<int> group_grid, group_first, field_list;
+    std::vector<int> group_nf;
+    for (int gi = 0; gi < ng; gi++) {
+        int first = int(field_list.size());
+        for (int f = 0; f < nf; f++)
+            if (job.fields[f].grid == gi) field_list.push_back(f);
+        if (int(field_list.size()) > first) {
+            group_grid.push_back(gi);
+            group_first.push_back(first);
+            group_nf.push_back(int(field_list.size()) - first);
+        }
+    }
+    const int G = int(group_grid.size());
+    int maxdiag = 0;
+    for (int gg = 0; gg < G; gg++) maxdiag = std::max(maxdiag, ndiag[group_grid[gg]]);
+    size_t o_group_grid = A.add(sizeof(int) * G);
+    std::copy(group_grid.begin(), group_grid.end(), A.at<int>(o_group_grid));
+    size_t o_group_first = A.add(sizeof(int) * G);
+    std::copy(group_first.begin(), group_first.end(), A.at<int>(o_group_first));
+    size_t o_field_list = A.add(sizeof(int) * field_list.size());
+    std::copy(field_list.begin(), field_list.end(), A.at<int>(o_field_list));
+    size_t o_pre = A.add(sizeof(int) * size_t(maxdiag) * (G + 1));
+    for (int q = 0; q < maxdiag; q++) {
+        int* pre = A.at<int>(o_pre) + size_t(q) * (G + 1);
+        int64_t acc = 0;
+        for (int gg = 0; gg < G; gg++) {
+            pre[gg] = int(acc);
+            int gi = group_grid[gg];
+            int cnt = 0;
+            if (q < ndiag[gi]) cnt = A.at<int>(o_diag_off[gi])[q + 1] - A.at<int>(o_diag_off[gi])[q];
+            acc += int64_t(group_nf[gg]) * cnt;
+        }
+        if (acc > INT32_MAX) return ctx->fail(TS_E_ARG, "too many tiles in one diagonal step");
+        pre[G] = int(acc);
+    }
+    // Fields, states, control.
+    size_t o_fields = A.add(sizeof(FieldDesc<Real>) * nf);
+    size_t o_state = A.add(sizeof(FieldState) * nf);
+    size_t o_ctl = A.add(sizeof(Control));
+    size_t o_dirty_off = A.add(sizeof(int64_t) * nf, 8);
+    int64_t dirty_total = 0;
+    for (int f = 0; f < nf; f++) {
+        A.at<int64_t>(o_dirty_off)[f] = dirty_total;
+        int gi = job.fields[f].grid;
+        dirty_total += int64_t(tx[gi]) * ty[gi] * tz[gi];
+    }
+
+    uint8_t* D = static_cast<uint8_t*>(ctx->buf("eng.arena", A.h.size()));
+    if (!D) return TS_E_NOMEM;
+    uint8_t* dirty = static_cast<uint8_t*>(ctx->buf("eng.dirty", size_t(dirty_total)));
+    if (!dirty) return TS_E_NOMEM;
+    for (int gi = 0; gi < ng; gi++) {
+        GridDesc gd{};
+        const host::Grid& g = *job.grids[gi];
+        gd.nx = g.nx; gd.ny = g.ny; gd.nz = g.nz;
+        gd.tx = tx[gi]; gd.ty = ty[gi]; gd.tz = tz[gi];
+        gd.ndiag = ndiag[gi];
+        gd.varz = g.variable ? 1 : 0;
+        gd.diag_off = reinterpret_cast<const int*>(D + o_diag_off[gi]);
+        gd.diag_tiles = reinterpret_cast<const uint32_t*>(D + o_diag_tiles[gi]);
+        gd.hlon = D + o_hlon[gi];
+        gd.hlat = D + o_hlat[gi];
+        gd.zc = D + o_zc[gi];
+        gd.hr = job.metrics[gi]->hr;
+        A.at<GridDesc>(o_grids)[gi] = gd;
+    }
+    for (int f = 0; f < nf; f++) {
+        const EngineField& ef = job.fields[f];
+        FieldDesc<Real> fd{};
+        fd.T = static_cast<Real*>(ef.T);
+        fd.s = static_cast<const Real*>(ef.slowness);
+        fd.dirty = dirty + A.at<int64_t>(o_dirty_off)[f];
+        fd.grid = ef.grid;
+        fd.seed_begin = seed_begin[f];
+        fd.seed_count = seed_count[f];
+        fd.cap = ef.cap;
+        A.at<FieldDesc<Real>>(o_fields)[f] = fd;
+    }
+    A.at<Control>(o_ctl)->running = nf;
+
+    cudaStream_t s = ctx->stream;
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(D, A.h.data(), A.h.size(), cudaMemcpyHostToDevice, s));
+    {
+        int64_t maxn = 0;
+        for (auto* g : job.grids) maxn = std::max(maxn, g->count());
+        dim3 grid(unsigned(std::min<int64_t>((maxn + 255) / 256, 512)), unsigned(nf));
+        fill_fields_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
+                                                      reinterpret_cast<const GridDesc*>(D + o_grids), dirty,
+                                                      reinterpret_cast<const int64_t*>(D + o_dirty_off));
+        int cnt = int(sc_node.size());
+        if (cnt > 0)
+            seed_fields_kernel<Real><<<(cnt + 255) / 256, 256, 0, s>>>(
+                reinterpret_cast<const FieldDesc<Real>*>(D + o_fields), reinterpret_cast<const int*>(D + o_sc_field),
+                reinterpret_cast<const int32_t*>(D + o_sc_node), reinterpret_cast<const double*>(D + o_sc_t), cnt);
+        TS_CUDA_TRY(ctx, cudaGetLastError());
+    }
+
+    Args<Real> args{};
+    args.grids = reinterpret_cast<const GridDesc*>(D + o_grids);
+    args.fields = reinterpret_cast<const FieldDesc<Real>*>(D + o_fields);
+    args.state = reinterpret_cast<FieldState*>(D + o_state);
+    args.seed_tile = reinterpret_cast<const int*>(D + o_seed_tile);
+    args.seed_mask = reinterpret_cast<const uint32_t*>(D + o_seed_mask);
+    args.plane_tab = reinterpret_cast<const uint16_t*>(D + o_ptab);
+    args.plane_off = reinterpret_cast<const int*>(D + o_poff);
+    args.ctl = reinterpret_cast<Control*>(D + o_ctl);
+    args.cancel = ctx->cancel_dev;
+    args.plan.ngroups = G;
+    args.plan.maxdiag = maxdiag;
+    args.plan.group_grid = reinterpret_cast<const int*>(D + o_group_grid);
+    args.plan.group_first = reinterpret_cast<const int*>(D + o_group_first);
+    args.plan.field_list = reinterpret_cast<const int*>(D + o_field_list);
+    args.plan.pre = reinterpret_cast<const int*>(D + o_pre);
+    args.n_active = int(field_list.size());
+    args.max_rounds_per_launch = 0;
+    args.barrier_timeout_ns = 5000000000LL;
+    args.tol = Real(job.tol);
+
+    const int smem = engine_smem_bytes<S>(WARPS, int(sizeof(Real)));
+    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, true>
+                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, false>;
+    TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
+    if (per_sm < 1) return ctx->fail(TS_E_CUDA, "engine kernel does not fit on an SM");
+    int blocks = per_sm * ctx->sm_count;
+    void* params[] = {&args};
+    TS_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s));
+    Control ctl{};
+    std::vector<FieldState> st(nf);
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(&ctl, D + o_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(st.data(), D + o_state, sizeof(FieldState) * nf, cudaMemcpyDeviceToHost, s));
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    for (int f = 0; f < nf; f++) {
+        job.fields[f].status = st[f].status;
+        job.fields[f].rounds[0] = st[f].rounds0;
+        job.fields[f].rounds[1] = st[f].rounds1;
+    }
+    if (stats) {
+        stats->node_updates += int64_t(ctl.updates);
+        stats->tile_visits += int64_t(ctl.visits);
+        stats->launches += 1;
+    }
+    if (ctl.error == TS_E_CANCELLED) return ctx->fail(TS_E_CANCELLED, "cancelled");
+    if (ctl.error) return ctx->fail(ctl.error, "engine: a device-side wait ran out (barrier timeout)");
+    return TS_OK;
+}
+
+}  // namespace
+
+template <typename Real>
+int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
+    if (job.fields.empty()) return TS_OK;
+    constexpr int W = sizeof(Real) == 8 ? 4 : 8;
+    switch (job.tile) {
+        case 1: return launch_shape<Real, 16, 8, 4, W>(ctx, job, stats);
+        default: return launch_shape<Real, 8, 8, 8, W>(ctx, job, stats);
+    }
+}
+
+template int engine_run<float>(ts_ctx*, EngineJob&, ts_eik_stats*);
+template int engine_run<double>(ts_ctx*, EngineJob&, ts_eik_stats*);
+
+}  // namespace eik
+}  // namespace ts

@@ -1,0 +1,128 @@
+"""Seeded synthetic forward problems of the named workloads (no network: no real data sets).
+
+Every "regular grid at h km" is a spherical GridDefinition anchored at 13.0°E, 43.0°N, depth 0,
+as in the reference's known-answer test (tests/TomoStar.Tests/NumericsTests.cs:91): ΔLat = h / (R·π/180),
+ΔLon = ΔLat / cos(centre latitude), depth spacing h. Positions given in km from the south-west top
+corner map to lon/lat through the grid's own spacing. Checkerboards are the reference's smooth
+sine-product pattern (Tomography/ResolutionTests.cs:62-82). Random numbers come from
+numpy.random.default_rng with the named seeds.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .grid import DEG2RAD, EARTH_RADIUS_KM, GridDef
+
+ANCHOR_LON, ANCHOR_LAT = 13.0, 43.0
+
+
+def regular_grid(nx: int, ny: int, nz: int, h_km: float, depth_km: np.ndarray | None = None) -> GridDef:
+    """A grid of nx×ny×nz nodes at about h km spacing anchored at (13.0°E, 43.0°N, 0 km)."""
+    dlat = h_km / (EARTH_RADIUS_KM * DEG2RAD)
+    centre_lat = ANCHOR_LAT + 0.5 * (ny - 1) * dlat
+    dlon = dlat / math.cos(centre_lat * DEG2RAD)
+    max_depth = (nz - 1) * h_km if depth_km is None else float(depth_km[-1])
+    min_depth = 0.0 if depth_km is None else float(depth_km[0])
+    return GridDef(ANCHOR_LON, ANCHOR_LON + (nx - 1) * dlon, ANCHOR_LAT, ANCHOR_LAT + (ny - 1) * dlat,
+                   min_depth, max_depth, nx, ny, nz, depth_km)
+
+
+def km_to_geo(grid: GridDef, x_km, y_km, h_km: float):
+    """(x, y) km from the grid's south-west corner → (lon, lat) through the node spacing."""
+    return grid.min_lon + np.asarray(x_km) / h_km * grid.dlon, grid.min_lat + np.asarray(y_km) / h_km * grid.dlat
+
+
+def surface_distance_km(lon1, lat1, lon2, lat2):
+    """GeoMath.SurfaceDistanceKm (Geo/GeoMath.cs:83-95), haversine."""
+    p1, p2 = np.asarray(lat1) * DEG2RAD, np.asarray(lat2) * DEG2RAD
+    dp = p2 - p1
+    dl = (np.asarray(lon2) - np.asarray(lon1)) * DEG2RAD
+    a = np.sin(dp / 2) ** 2 + np.cos(p1) * np.cos(p2) * np.sin(dl / 2) ** 2
+    return 2 * np.arcsin(np.minimum(1, np.sqrt(a))) * EARTH_RADIUS_KM
+
+
+def checkerboard(grid: GridDef, cell_h_km: float, cell_v_km: float, amplitude_percent: float) -> np.ndarray:
+    """ResolutionPattern.Evaluate, checkerboard branch (ResolutionTests.cs:62-75): fractional
+    perturbation at every node, grid order."""
+    lon, lat, dep = grid.lon(), grid.lat(), grid.depth()
+    L, A = np.meshgrid(lon, lat, indexing="xy")  # (ny, nx)
+    x = surface_distance_km(grid.min_lon, A, L, A)
+    y = surface_distance_km(L, grid.min_lat, L, A)
+    z = dep - grid.min_depth_km
+    horiz = np.sin(np.pi * x / cell_h_km) * np.sin(np.pi * y / cell_h_km)
+    vert = np.sin(np.pi * (z + 0.5 * cell_v_km) / cell_v_km)
+    return (amplitude_percent / 100 * vert[:, None, None] * horiz[None, :, :]).reshape(-1)
+
+
+@dataclass
+class Problem:
+    """A forward problem: grid, slowness per phase, stations (field origins) and events."""
+
+    name: str
+    grid: GridDef                      # forward grid
+    inv: GridDef                       # inversion grid (forward coarsened ×2)
+    slowness: np.ndarray               # (n_phases, n) s/km
+    stations: np.ndarray               # (n_stations, 3) lon, lat, depth
+    events: np.ndarray                 # (n_events, 3)
+    arrivals: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))  # (event, station, phase)
+    h_km: float = 1.0
+
+    @property
+    def step_km(self) -> float:
+        """RayKernels step (Tomography/RayKernels.cs:62)."""
+        return 0.5 * min(self.grid.min_spacing_km(), self.inv.min_spacing_km())
+
+
+def vp_linear(grid: GridDef, v0: float = 5.0, grad: float = 0.03) -> np.ndarray:
+    dep = grid.depth()
+    return np.broadcast_to((v0 + grad * dep)[:, None, None], grid.shape).reshape(-1).copy()
+
+
+def config0() -> Problem:
+    """61×61×31 at 1 km; Vp = (5 + 0.03 z)·(1 ± 5 % checkerboard of 10 km); source (30, 30, 10) km;
+    25 receivers uniformly at random on the surface (seed 0). FP64, compared with the CPU solver."""
+    h = 1.0
+    g = regular_grid(61, 61, 31, h)
+    vp = vp_linear(g) * (1 + checkerboard(g, 10, 10, 5))
+    slon, slat = km_to_geo(g, 30.0, 30.0, h)
+    rng = np.random.default_rng(0)
+    xy = rng.uniform(0, 60, size=(25, 2))
+    rlon, rlat = km_to_geo(g, xy[:, 0], xy[:, 1], h)
+    events = np.stack([rlon, rlat, np.zeros(25)], axis=1)
+    arrivals = np.stack([np.arange(25), np.zeros(25, int), np.zeros(25, int)], axis=1).astype(np.int32)
+    return Problem("config0", g, g.coarsened(2), (1 / vp)[None, :], np.array([[slon, slat, 10.0]]), events,
+                   arrivals, h)
+
+
+def config1() -> Problem:
+    """121×121×61 at 0.5 km; Vp as config 0; Vp/Vs = 1.73·(1 ± 3 % checkerboard of 10 km); 25 surface
+    stations (seed 1), 150 events in the box at 2–20 km depth (seed 2); P and S: 50 fields, 7,500 rays."""
+    h = 0.5
+    g = regular_grid(121, 121, 61, h)
+    vp = vp_linear(g) * (1 + checkerboard(g, 10, 10, 5))
+    vs = vp / (1.73 * (1 + checkerboard(g, 10, 10, 3)))
+    span = 120 * h
+    r1 = np.random.default_rng(1)
+    sxy = r1.uniform(0, span, size=(25, 2))
+    slon, slat = km_to_geo(g, sxy[:, 0], sxy[:, 1], h)
+    stations = np.stack([slon, slat, np.zeros(25)], axis=1)
+    r2 = np.random.default_rng(2)
+    exyz = np.column_stack([r2.uniform(0, span, 150), r2.uniform(0, span, 150), r2.uniform(2, 20, 150)])
+    elon, elat = km_to_geo(g, exyz[:, 0], exyz[:, 1], h)
+    events = np.stack([elon, elat, exyz[:, 2]], axis=1)
+    ev, st, ph = np.meshgrid(np.arange(150), np.arange(25), np.arange(2), indexing="ij")
+    arrivals = np.stack([ev.ravel(), st.ravel(), ph.ravel()], axis=1).astype(np.int32)
+    return Problem("config1", g, g.coarsened(2), np.stack([1 / vp, 1 / vs]), stations, events, arrivals, h)
+
+
+def selftest_case():
+    """The reference's device self-test case (Forward/EikonalOpenCl.cs:348-358)."""
+    g = GridDef(10, 12, 42, 44, -2, 120, 22, 20, 16)
+    dep = g.depth()
+    i = np.arange(g.nx)[None, None, :]
+    j = np.arange(g.ny)[None, :, None]
+    s = 1 / (5.8 + 0.02 * dep[:, None, None] + 0.2 * np.sin(0.7 * i) + 0.15 * np.cos(0.5 * j))
+    return g, s.reshape(-1), (10.37, 42.61, 8.3)
