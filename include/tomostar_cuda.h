@@ -42,9 +42,10 @@ extern "C" {
 #define TS_MODE_ENGINE 0  /* batched tiled engine: tile-wavefront sweeps, one cooperative launch */
 #define TS_MODE_PLAIN 1   /* the reference scheme as-is: one launch per diagonal plane, one field at a time */
 
-/* Output element types. */
+/* Output element types. TS_OUT_NONE keeps the fields on the device (ts_eik_solve_model only). */
 #define TS_OUT_F64 0
 #define TS_OUT_F32 1
+#define TS_OUT_NONE 2
 
 typedef struct ts_ctx ts_ctx;
 
@@ -100,6 +101,18 @@ int32_t ts_point_source(const ts_grid* grid, const double* slowness, double lon,
 int ts_eik_solve(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32_t n_fields,
                  const int32_t* seed_offsets, const int32_t* seed_index, const double* seed_time, int32_t precision,
                  int32_t mode, double tol, int32_t max_rounds, void* out, int32_t out_type, ts_eik_stats* stats);
+
+/* Resident models (ForwardModel, Forward/TravelTimeTable.cs:167-241, kept on the device between
+ * solves the way TravelTimeTableSet reuses tables by ModelKey, :176-183, 278-279): the slowness of
+ * n_phases phases (phase p at p*n) and the grid's metric, uploaded once in `precision`. */
+int ts_model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32_t n_phases, int32_t precision,
+                 int32_t* model_id);
+int ts_model_drop(ts_ctx* ctx, int32_t model_id);
+/* ts_eik_solve on a resident model's phase (no slowness upload). out_type TS_OUT_NONE leaves the
+ * fields on the device (out may be NULL); otherwise as ts_eik_solve. */
+int ts_eik_solve_model(ts_ctx* ctx, int32_t model_id, int32_t phase, int32_t n_fields, const int32_t* seed_offsets,
+                       const int32_t* seed_index, const double* seed_time, int32_t mode, double tol,
+                       int32_t max_rounds, void* out, int32_t out_type, ts_eik_stats* stats);
 
 /* EikonalOpenCl.SelfTest (EikonalOpenCl.cs:346-374): the reference's 22x20x16 heterogeneous case
  * solved on the device and by the host sweeping solver; *rel_err = max |dt| / field range. The

@@ -808,7 +808,8 @@ int32_t or_kernel(const or_grid_def* inv, const double* pts, int32_t n_pts, int3
 
 // One arrival of RayKernels.Compute (Tomography/RayKernels.cs:77-97): backtrack on the station's
 // table, TCalc and the source gradient, the kernel on the inversion grid, nodes ascending, lengths
-// cast to float32. Returns nnz, 0 for a dropped arrival, or -needed when cap is too small.
+// cast to float32. Returns nnz (>= 0, an empty row is kept), -1 for an arrival the reference drops,
+// or -2 - needed when cap is too small.
 int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, double st_lat, double st_dep,
                    const or_grid_def* inv, double ev_lon, double ev_lat, double ev_dep, double step_km,
                    int32_t* nodes, float* lens, int32_t cap, double* tcalc_grad4) {
@@ -816,15 +817,15 @@ int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, do
     Grid ig(*inv);
     Table tb{g, table, st_lon, st_lat, st_dep};
     std::vector<Geo> path;
-    if (!backtrack(tb, ev_lon, ev_lat, ev_dep, step_km, path)) return 0;
+    if (!backtrack(tb, ev_lon, ev_lat, ev_dep, step_km, path)) return -1;
     double tcalc = tb.time(ev_lon, ev_lat, ev_dep);
     double ge, gn, gz;
     tb.gradient(ev_lon, ev_lat, ev_dep, ge, gn, gz);
-    if (!std::isfinite(tcalc)) return 0;
+    if (!std::isfinite(tcalc)) return -1;
     std::vector<int> keys;
     std::vector<double> vals;
     ray_kernel(ig, path, keys, vals);
-    if (int(keys.size()) > cap) return -int(keys.size());
+    if (int(keys.size()) > cap) return -2 - int(keys.size());
     std::vector<int> order(keys.size());
     for (size_t q = 0; q < order.size(); q++) order[q] = int(q);
     std::sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
@@ -837,7 +838,8 @@ int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, do
 }
 
 // Many arrivals on a thread pool (RayKernels.cs:67): arrival a traces on table tables + tab_of[a]*n
-// with station st[3*a..]; writes row a's nnz into nnz[a] and its entries at [a*cap_per_row, ...).
+// with station st[3*a..]; writes row a's result (as or_ray_row returns it) into nnz[a] and its entries
+// at [a*cap_per_row, ...).
 void or_ray_rows_many(const or_grid_def* fwd, const float* tables, const int32_t* tab_of, const double* st,
                       const or_grid_def* inv, const double* ev, int32_t n_rays, double step_km, int32_t cap_per_row,
                       int32_t* nnz, int32_t* nodes, float* lens, double* tcalc_grad4, int32_t threads) {

@@ -272,15 +272,16 @@ def ray_row(fwd: Grid, table, station, inv: Grid, event, step_km):
         n = lib().or_ray_row(fwd.ref, _p(tb, C.c_float), station[0], station[1], station[2], inv.ref, event[0],
                              event[1], event[2], step_km, _p(nodes, C.c_int32), _p(lens, C.c_float), cap,
                              _p(tg, C.c_double))
-        if n == 0:
+        if n == -1:
             return None
-        if n > 0:
+        if n >= 0:
             return nodes[:n].copy(), lens[:n].copy(), tg[0], tg[1:].copy()
-        cap = -n
+        cap = -2 - n
 
 
 def ray_rows_many(fwd: Grid, tables, tab_of, stations, inv: Grid, events, step_km, cap_per_row=4096, threads=None):
-    """Many arrivals on a thread pool. tables (n_tables, n) float32; stations/events (n_rays, 3)."""
+    """Many arrivals on a thread pool. tables (n_tables, n) float32; stations/events (n_rays, 3).
+    nnz[a] >= 0 for a kept row (possibly empty), -1 for an arrival the reference drops."""
     tb = np.ascontiguousarray(tables, np.float32)
     to = np.ascontiguousarray(tab_of, np.int32)
     st = np.ascontiguousarray(stations, np.float64)

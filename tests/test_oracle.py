@@ -1,0 +1,147 @@
+"""The CPU oracle against the reference's known-answer tests (tests/golden/kat.json) and its own
+invariants. No GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kat.json")))
+
+
+def grid_of(d):
+    return O.Grid(d["min_lon"], d["max_lon"], d["min_lat"], d["max_lat"], d["min_depth_km"], d["max_depth_km"],
+                  d["nx"], d["ny"], d["nz"])
+
+
+def test_fast_marching_homogeneous_corners():
+    """NumericsTests.FastMarchingMatchesStraightRaysInAHomogeneousModel (NumericsTests.cs:88-104)."""
+    k = KAT["homogeneous_corners"]
+    g = grid_of(k["grid"])
+    assert (g.nx, g.ny, g.nz) == (61, 61, 31)
+    s = np.full(g.count, 1 / k["velocity"])
+    si, st = O.point_source(g, s, *k["source"])
+    t = O.fmm(g, s, si, st)
+    worst = max(abs(t[(kk * g.ny + j) * g.nx + i] - ex) / ex for (i, j, kk), ex in zip(k["nodes"], k["exact"]))
+    assert worst < k["tolerance"]
+
+
+def test_relax_homogeneous_corners():
+    """The sweeping solver (the device scheme's host reference) meets the same known answer."""
+    k = KAT["homogeneous_corners"]
+    g = grid_of(k["grid"])
+    s = np.full(g.count, 1 / k["velocity"])
+    si, st = O.point_source(g, s, *k["source"])
+    t, ok, rounds = O.relax(g, s, si, st)
+    assert ok and rounds[0] >= 1 and rounds[1] >= 1
+    worst = max(abs(t[(kk * g.ny + j) * g.nx + i] - ex) / ex for (i, j, kk), ex in zip(k["nodes"], k["exact"]))
+    assert worst < k["tolerance"]
+
+
+def test_trilinear_weights_known_answer():
+    """NumericsTests.TrilinearWeightsSumToOneAndInterpolateLinearFieldsExactly (:107-123)."""
+    k = KAT["trilinear"]
+    g = grid_of(k["grid"])
+    nodes, w = O.trilinear(g, *k["point"])
+    assert abs(w.sum() - 1) < 1e-12
+    lon, lat, cl, dep = O.coords(g)
+    L, A, D = np.meshgrid(lon, lat, dep, indexing="ij")
+    field = (2 * L - A + 0.1 * D).transpose(2, 1, 0).reshape(-1)
+    assert abs(O.interpolate(g, field, *k["point"]) - k["linear_value"]) < 1e-9
+
+
+def test_fast_marching_gradient_model_analytic():
+    """Validation case eikonal-gradient (Program.cs:107-132): v = 4 + 0.05 z against the closed form,
+    within the validation threshold (common.py: 5 %)."""
+    k = KAT["gradient_model"]
+    g = grid_of(k["grid"])
+    lon, lat, cl, dep = O.coords(g)
+    v = k["v0"] + k["gradient"] * dep
+    s = np.broadcast_to((1 / v)[:, None, None], (g.nz, g.ny, g.nx)).reshape(-1).copy()
+    si, st = O.point_source(g, s, *k["source"])
+    t = O.fmm(g, s, si, st)
+    rows = np.array(k["rows"])
+    idx = ((rows[:, 2] * g.ny + rows[:, 1]) * g.nx + rows[:, 0]).astype(int)
+    rel = np.abs(t[idx] - rows[:, 4]) / rows[:, 4]
+    assert rel.max() < k["tolerance"]
+    assert rel.mean() < 0.01
+
+
+def test_relax_tolerance_zero_is_a_fixed_point():
+    """tol = 0 runs to the exact fixed point: one more round changes nothing."""
+    g = O.Grid(10, 11, 42, 43, 0, 30, 17, 15, 11)
+    rng = np.random.default_rng(7)
+    s = 1 / (5 + rng.uniform(-0.5, 0.5, g.count))
+    si, st = O.point_source(g, s, 10.4, 42.3, 7)
+    t, ok, rounds = O.relax(g, s, si, st, tol=0.0)
+    assert ok
+    t2, ok2, _ = O.relax(g, s, si, st, tol=0.0)
+    assert np.array_equal(t, t2)
+
+
+def test_relax_close_to_fast_marching():
+    """Sweeping and marching solve the same discrete equations: close, not equal."""
+    g = O.Grid(10, 11, 42, 43, 0, 30, 25, 21, 13)
+    lon, lat, cl, dep = O.coords(g)
+    s = np.broadcast_to((1 / (5 + 0.04 * dep))[:, None, None], (g.nz, g.ny, g.nx)).reshape(-1).copy()
+    si, st = O.point_source(g, s, 10.5, 42.5, 5)
+    a = O.fmm(g, s, si, st)
+    b, ok, _ = O.relax(g, s, si, st)
+    assert ok
+    assert np.max(np.abs(a - b) / np.maximum(a, 1e-9)) < 0.02
+
+
+def test_relax_unsettled_reports():
+    g = O.Grid(10, 11, 42, 43, 0, 30, 25, 21, 13)
+    s = np.full(g.count, 0.2)
+    si, st = O.point_source(g, s, 10.5, 42.5, 5)
+    _, ok, rounds = O.relax(g, s, si, st, max_rounds=1)
+    assert not ok and rounds[0] == 1
+
+
+def test_table_rounding():
+    """TravelTimeTable.Write (TravelTimeTable.cs:73): float32, non-finite → +inf."""
+    t = np.array([1.0, 1 / 3, np.inf, np.nan, -np.inf, 1e40])
+    f = O.to_table(t)
+    assert f[0] == 1.0 and f[1] == np.float32(1 / 3)
+    assert np.isinf(f[2]) and np.isinf(f[3]) and f[4] == np.inf and np.isinf(f[5])
+
+
+def test_ray_row_consistent_with_field_time():
+    """Validation 'rays' case (Program.cs:173-183): Σ length·slowness along a traced ray is close to
+    the field time (reference max 2.13 %, threshold 5 %)."""
+    g = O.Grid(13, 13.5, 43, 43.4, 0, 20, 41, 45, 21)
+    lon, lat, cl, dep = O.coords(g)
+    s = np.broadcast_to((1 / (5 + 0.05 * dep))[:, None, None], (g.nz, g.ny, g.nx)).reshape(-1).copy()
+    src = (13.25, 43.2, 0.0)
+    si, st = O.point_source(g, s, *src)
+    t, ok, _ = O.relax(g, s, si, st)
+    tb = O.to_table(t)
+    step = 0.25 * O.min_spacing_km(g)
+    worst = 0
+    for ev in [(13.05, 43.05, 12.0), (13.45, 43.35, 8.0), (13.3, 43.1, 18.0)]:
+        ray = O.backtrack(g, tb, src, *ev, step)
+        assert ray is not None and len(ray) > 3
+        nodes, lens = O.kernel(g, ray)
+        kt = float(np.sum(lens * s[nodes]))
+        ft = O.table_time(g, tb, *ev)
+        worst = max(worst, abs(kt - ft) / ft)
+    assert worst < 0.05
+
+
+def test_variable_spacing_uniform_limit():
+    """Extension: an explicit depth array equal to the uniform one reproduces the uniform result closely
+    (the non-uniform stencil reduces to the uniform one up to rounding)."""
+    d = dict(min_lon=10, max_lon=11, min_lat=42, max_lat=43, min_depth_km=0, max_depth_km=24, nx=17, ny=15, nz=13)
+    g = grid_of(d)
+    gv = O.Grid(10, 11, 42, 43, 0, 24, 17, 15, 13, depth_km=np.linspace(0, 24, 13))
+    s = np.full(g.count, 0.18)
+    si, st = O.point_source(g, s, 10.5, 42.5, 6)
+    a, ok, _ = O.relax(g, s, si, st)
+    si2, st2 = O.point_source(gv, s, 10.5, 42.5, 6)
+    b, ok2, _ = O.relax(gv, s, si2, st2)
+    assert ok and ok2
+    fin = np.isfinite(a)
+    assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(a[fin], 1e-9)) < 1e-3

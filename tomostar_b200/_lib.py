@@ -14,7 +14,7 @@ TS_OK, TS_E_ARG, TS_E_CUDA, TS_E_NOMEM, TS_E_UNSETTLED, TS_E_CANCELLED = 0, 1, 2
 TS_E_TIMEOUT, TS_E_CAPACITY, TS_E_NOSEEDS, TS_E_SELFTEST, TS_E_NODEVICE = 6, 7, 8, 9, 10
 F64, F32 = 64, 32
 MODE_ENGINE, MODE_PLAIN = 0, 1
-OUT_F64, OUT_F32 = 0, 1
+OUT_F64, OUT_F32, OUT_NONE = 0, 1, 2
 
 ERROR_NAMES = {
     TS_E_ARG: "invalid argument", TS_E_CUDA: "CUDA error", TS_E_NOMEM: "out of device memory",
@@ -67,6 +67,9 @@ SIGNATURES = {
     "ts_engine_set_tile": (C.c_int, [_vp, _i32, _i32]),
     "ts_point_source": (_i32, [_gp, _dp, _d, _d, _d, _d, _d, _ip, _dp, _i32]),
     "ts_eik_solve": (C.c_int, [_vp, _gp, _dp, _i32, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32, _P(EikStats)]),
+    "ts_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _i32, _ip]),
+    "ts_model_drop": (C.c_int, [_vp, _i32]),
+    "ts_eik_solve_model": (C.c_int, [_vp, _i32, _i32, _i32, _ip, _ip, _dp, _i32, _d, _i32, _vp, _i32, _P(EikStats)]),
     "ts_cuda_selftest": (C.c_int, [_vp, _i32, _dp, C.c_char_p, _i32]),
     "ts_rays_trace": (C.c_int, [_vp, _gp, _i32, _fp, _dp, _gp, _i32, _ip, _dp, _d, _P(_vp)]),
     "ts_forward": (C.c_int, [_vp, _gp, _dp, _i32, _gp, _i32, _dp, _i32, _dp, _i32, _ip, _ip, _ip, _i32, _d, _P(_vp),

@@ -18,6 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtomostar_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NO_FMA = {"rays.cu"}
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
           "-I", os.path.join(HERE, "..", "include")]
 
@@ -29,16 +30,25 @@ def _deps() -> list[str]:
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    newest = max(os.path.getmtime(p) for p in [src, *_deps()])
-    if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
+    # The ray tracer rounds every operation on its own, as the reference's .NET arithmetic does:
+    # a contracted multiply-add at one call site and not another breaks identities such as
+    # "the same point twice gives a zero-length segment".
+    flags = ["-fmad=false"] if os.path.basename(src) in NO_FMA else []
+    cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", src, "-o", obj]
+    stamp = obj + ".cmd"
+    newest = max(os.path.getmtime(p) for p in [src, *_deps(), os.path.abspath(__file__)])
+    if (os.path.exists(obj) and os.path.getmtime(obj) >= newest and os.path.exists(stamp)
+            and open(stamp).read() == " ".join(cmd)):
         return obj
-    extra = ["-Xptxas", "-v"] if verbose and src.endswith(".cu") else []
-    cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", src, "-o", obj]
+    if verbose and src.endswith(".cu"):
+        cmd = cmd[:-4] + ["-Xptxas", "-v"] + cmd[-4:]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n{r.stdout}\n{r.stderr}")
     if verbose:
         sys.stderr.write(r.stderr)
+    with open(stamp, "w") as f:
+        f.write(" ".join(c for c in cmd if c not in ("-Xptxas", "-v")))
     return obj
 
 

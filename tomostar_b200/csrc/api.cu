@@ -72,6 +72,7 @@ void ts_cuda_destroy(ts_ctx* ctx) {
         std::lock_guard<std::recursive_mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        ts::eik::models_free(ctx);
         for (auto& kv : ctx->bufs)
             if (kv.second.p) cudaFree(kv.second.p);
         ctx->bufs.clear();
@@ -155,13 +156,69 @@ int ts_eik_solve(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32
     if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN) return ctx->fail(TS_E_ARG, "unknown mode");
     if (out_type != TS_OUT_F64 && out_type != TS_OUT_F32) return ctx->fail(TS_E_ARG, "unknown output type");
     if (!(tol >= 0)) return ctx->fail(TS_E_ARG, "tolerance must be >= 0");
-    ts::eik::SolveIn in{grid, slowness, n_fields, seed_offsets, seed_index, seed_time, precision, mode, tol, max_rounds};
-    void* dev = nullptr;
+    ts::eik::SolveIn in{};
+    in.grid = grid;
+    in.slowness = slowness;
+    in.n_fields = n_fields;
+    in.seed_offsets = seed_offsets;
+    in.seed_index = seed_index;
+    in.seed_time = seed_time;
+    in.precision = precision;
+    in.mode = mode;
+    in.tol = tol;
+    in.max_rounds = max_rounds;
     ts_eik_stats local{};
-    rc = ts::eik::solve_to_device(ctx, in, &dev, stats ? stats : &local);
-    if (rc) return rc;
-    int64_t count = int64_t(n_fields) * grid->nx * grid->ny * grid->nz;
-    return ts::eik::copy_fields_out(ctx, dev, precision, count, out, out_type);
+    return ts::eik::solve(ctx, in, out, out_type, stats ? stats : &local);
+}
+
+int ts_model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32_t n_phases, int32_t precision,
+                 int32_t* model_id) {
+    if (!ctx || !model_id) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!grid || !slowness || n_phases <= 0) return ctx->fail(TS_E_ARG, "null grid or slowness");
+    int id = 0;
+    int rc = ts::eik::model_put(ctx, grid, slowness, n_phases, precision, &id);
+    *model_id = id;
+    return rc;
+}
+
+int ts_model_drop(ts_ctx* ctx, int32_t model_id) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return ts::eik::model_drop(ctx, model_id);
+}
+
+int ts_eik_solve_model(ts_ctx* ctx, int32_t model_id, int32_t phase, int32_t n_fields, const int32_t* seed_offsets,
+                       const int32_t* seed_index, const double* seed_time, int32_t mode, double tol,
+                       int32_t max_rounds, void* out, int32_t out_type, ts_eik_stats* stats) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    auto it = ctx->models.find(model_id);
+    if (it == ctx->models.end()) return ctx->fail(TS_E_ARG, "unknown model");
+    if (!seed_offsets || n_fields <= 0) return ctx->fail(TS_E_ARG, "no fields");
+    if (seed_offsets[n_fields] > 0 && (!seed_index || !seed_time)) return ctx->fail(TS_E_ARG, "null seed arrays");
+    if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN) return ctx->fail(TS_E_ARG, "unknown mode");
+    if (out_type != TS_OUT_F64 && out_type != TS_OUT_F32 && out_type != TS_OUT_NONE)
+        return ctx->fail(TS_E_ARG, "unknown output type");
+    if (out_type != TS_OUT_NONE && !out) return ctx->fail(TS_E_ARG, "null output");
+    if (!(tol >= 0)) return ctx->fail(TS_E_ARG, "tolerance must be >= 0");
+    ts::eik::SolveIn in{};
+    in.model_id = model_id;
+    in.phase = phase;
+    in.grid = &it->second->def;
+    in.n_fields = n_fields;
+    in.seed_offsets = seed_offsets;
+    in.seed_index = seed_index;
+    in.seed_time = seed_time;
+    in.precision = it->second->precision;
+    in.mode = mode;
+    in.tol = tol;
+    in.max_rounds = max_rounds;
+    ts_eik_stats local{};
+    return ts::eik::solve(ctx, in, out, out_type, stats ? stats : &local);
 }
 
 int ts_cuda_selftest(ts_ctx* ctx, int32_t precision, double* rel_err, char* msg, int32_t cap) {

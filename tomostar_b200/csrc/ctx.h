@@ -7,8 +7,10 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/tomostar_cuda.h"
+#include "host_geo.h"
 
 struct ts_ctx {
     int device = 0;
@@ -22,6 +24,10 @@ struct ts_ctx {
     volatile int* cancel_host = nullptr;  // host-mapped, read by kernels between rounds
     int* cancel_dev = nullptr;
     int tile_f64 = 0, tile_f32 = 0;       // engine tile shape per precision
+
+    struct Model;
+    std::map<int, Model*> models;
+    int next_model = 1;
 
     struct Buf {
         void* p = nullptr;
@@ -72,11 +78,29 @@ struct ts_ctx {
     type* var = static_cast<type*>((ctx)->buf((key), sizeof(type) * size_t(count))); \
     if (!var) return TS_E_NOMEM
 
+// A resident model: grid, metric and the device slowness of its phases (ts_model_put).
+struct ts_ctx::Model {
+    ts_grid def{};
+    std::vector<double> depth;
+    ts::host::Grid* grid = nullptr;
+    ts::host::Metric* metric = nullptr;
+    int precision = 64;
+    int n_phases = 1;
+    void* slowness = nullptr;  // device, n_phases * n values of the precision
+    ~Model() {
+        delete metric;
+        delete grid;
+        if (slowness) cudaFree(slowness);
+    }
+};
+
 namespace ts {
 namespace eik {
 
 // Host-side entry points of the eikonal solvers (eik_host.cu).
 struct SolveIn {
+    int model_id = 0;         // > 0: solve on a resident model (grid, slowness and metric from it)
+    int phase = 0;
     const ts_grid* grid;
     const double* slowness;
     int n_fields;
@@ -89,7 +113,12 @@ struct SolveIn {
     int max_rounds;
 };
 
-int solve_to_device(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_stats* stats);
+int model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int n_phases, int precision, int* id);
+int model_drop(ts_ctx* ctx, int id);
+void models_free(ts_ctx* ctx);
+
+// Solves and writes the fields to host `out` (dense, field-major, out_type).
+int solve(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, ts_eik_stats* stats);
 int copy_fields_out(ts_ctx* ctx, const void* fields_dev, int precision, int64_t count, void* out, int out_type);
 
 }  // namespace eik

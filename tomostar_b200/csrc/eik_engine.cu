@@ -35,7 +35,7 @@ __global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, c
                                    uint8_t* __restrict__ dirty_base, const int64_t* __restrict__ dirty_off) {
     const FieldDesc<Real>& fd = fields[blockIdx.y];
     const GridDesc& g = grids[fd.grid];
-    int64_t n = int64_t(g.nx) * g.ny * g.nz;
+    int64_t n = int64_t(g.pitch) * g.ny * g.nz;  // the pads too: they must read as +inf
     const Real inf = real_inf<Real>();
     for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < n; q += int64_t(gridDim.x) * blockDim.x)
         fd.T[q] = inf;
@@ -46,15 +46,33 @@ __global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, c
 }
 
 template <typename Real>
-__global__ void seed_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const int* __restrict__ field_of,
-                                   const int32_t* __restrict__ node, const double* __restrict__ t, int count) {
+__global__ void seed_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const GridDesc* __restrict__ grids,
+                                   const int* __restrict__ field_of, const int32_t* __restrict__ node,
+                                   const double* __restrict__ t, int count) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < count) fields[field_of[q]].T[node[q]] = Real(t[q]);
+    if (q >= count) return;
+    const FieldDesc<Real>& fd = fields[field_of[q]];
+    const GridDesc& g = grids[fd.grid];
+    int n = node[q], i = n % g.nx, row = n / g.nx;
+    fd.T[int64_t(row) * g.pitch + Layout<Real>::HX + i] = Real(t[q]);
+}
+
+// Padded engine fields → dense grid order of another precision (one field per blockIdx.y).
+template <typename From, typename To>
+__global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_stride, int pitch, int xoff, int nx,
+                                     int64_t rows, To* __restrict__ b) {
+    const From* src = a + blockIdx.y * field_stride;
+    To* dst = b + int64_t(blockIdx.y) * rows * nx;
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < rows * nx; q += int64_t(gridDim.x) * blockDim.x) {
+        int64_t r = q / nx;
+        From v = src[r * pitch + xoff + (q - r * nx)];
+        dst[q] = isfinite(v) ? To(v) : To(__int_as_float(0x7f800000));
+    }
 }
 
 template <typename Real, int BX, int BY, int BZ, int WARPS>
 int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
-    using S = Shape<BX, BY, BZ>;
+    using S = Shape<Real, BX, BY, BZ>;
     const int nf = int(job.fields.size());
     const int ng = int(job.grids.size());
     bool any_var = false;
@@ -62,7 +80,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
 
     Arena A;
     // Grids.
-    std::vector<size_t> o_diag_off(ng), o_diag_tiles(ng), o_hlon(ng), o_hlat(ng), o_zc(ng);
+    std::vector<size_t> o_diag_off(ng), o_diag_tiles(ng), o_wx(ng), o_wy(ng), o_zc(ng);
     std::vector<int> tx(ng), ty(ng), tz(ng), ndiag(ng);
     size_t o_grids = A.add(sizeof(GridDesc) * ng);
     for (int gi = 0; gi < ng; gi++) {
@@ -89,10 +107,10 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         for (int c = 0; c < tz[gi]; c++)
             for (int b = 0; b < ty[gi]; b++)
                 for (int a = 0; a < tx[gi]; a++) dt[pos[a + b + c]++] = uint32_t(a) | (uint32_t(b) << 10) | (uint32_t(c) << 20);
-        o_hlon[gi] = A.add(sizeof(Real) * m.hlon.size());
-        for (size_t q = 0; q < m.hlon.size(); q++) A.at<Real>(o_hlon[gi])[q] = Real(m.hlon[q]);
-        o_hlat[gi] = A.add(sizeof(Real) * m.hlat.size());
-        for (size_t q = 0; q < m.hlat.size(); q++) A.at<Real>(o_hlat[gi])[q] = Real(m.hlat[q]);
+        o_wx[gi] = A.add(sizeof(Real) * m.wx.size());
+        for (size_t q = 0; q < m.wx.size(); q++) A.at<Real>(o_wx[gi])[q] = Real(m.wx[q]);
+        o_wy[gi] = A.add(sizeof(Real) * m.wy.size());
+        for (size_t q = 0; q < m.wy.size(); q++) A.at<Real>(o_wy[gi])[q] = Real(m.wy[q]);
         o_zc[gi] = A.add(sizeof(Real) * std::max<size_t>(1, m.zc.size()));
         for (size_t q = 0; q < m.zc.size(); q++) A.at<Real>(o_zc[gi])[q] = Real(m.zc[q]);
     }
@@ -203,6 +221,18 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         dirty_total += int64_t(tx[gi]) * ty[gi] * tz[gi];
     }
 
+    // The fields, padded rows (Layout): one buffer, field f at its offset.
+    job.pitch.assign(ng, 0);
+    job.xoff = S::HX;
+    for (int gi = 0; gi < ng; gi++) job.pitch[gi] = Layout<Real>::pitch(tx[gi], BX);
+    std::vector<int64_t> foff(nf + 1, 0);
+    for (int f = 0; f < nf; f++) {
+        const host::Grid& g = *job.grids[job.fields[f].grid];
+        foff[f + 1] = foff[f] + int64_t(job.pitch[job.fields[f].grid]) * g.ny * g.nz;
+    }
+    Real* fields = static_cast<Real*>(ctx->buf("eng.fields", sizeof(Real) * size_t(foff[nf])));
+    if (!fields) return TS_E_NOMEM;
+    for (int f = 0; f < nf; f++) job.fields[f].T = fields + foff[f];
     uint8_t* D = static_cast<uint8_t*>(ctx->buf("eng.arena", A.h.size()));
     if (!D) return TS_E_NOMEM;
     uint8_t* dirty = static_cast<uint8_t*>(ctx->buf("eng.dirty", size_t(dirty_total)));
@@ -216,10 +246,12 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         gd.varz = g.variable ? 1 : 0;
         gd.diag_off = reinterpret_cast<const int*>(D + o_diag_off[gi]);
         gd.diag_tiles = reinterpret_cast<const uint32_t*>(D + o_diag_tiles[gi]);
-        gd.hlon = D + o_hlon[gi];
-        gd.hlat = D + o_hlat[gi];
+        gd.wx = D + o_wx[gi];
+        gd.wy = D + o_wy[gi];
         gd.zc = D + o_zc[gi];
-        gd.hr = job.metrics[gi]->hr;
+        gd.wz1 = job.metrics[gi]->wz1;
+        gd.wz2 = job.metrics[gi]->wz2;
+        gd.pitch = job.pitch[gi];
         A.at<GridDesc>(o_grids)[gi] = gd;
     }
     for (int f = 0; f < nf; f++) {
@@ -240,7 +272,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(D, A.h.data(), A.h.size(), cudaMemcpyHostToDevice, s));
     {
         int64_t maxn = 0;
-        for (auto* g : job.grids) maxn = std::max(maxn, g->count());
+        for (int gi = 0; gi < ng; gi++) maxn = std::max(maxn, int64_t(job.pitch[gi]) * job.grids[gi]->ny * job.grids[gi]->nz);
         dim3 grid(unsigned(std::min<int64_t>((maxn + 255) / 256, 512)), unsigned(nf));
         fill_fields_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
                                                       reinterpret_cast<const GridDesc*>(D + o_grids), dirty,
@@ -248,7 +280,8 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         int cnt = int(sc_node.size());
         if (cnt > 0)
             seed_fields_kernel<Real><<<(cnt + 255) / 256, 256, 0, s>>>(
-                reinterpret_cast<const FieldDesc<Real>*>(D + o_fields), reinterpret_cast<const int*>(D + o_sc_field),
+                reinterpret_cast<const FieldDesc<Real>*>(D + o_fields), reinterpret_cast<const GridDesc*>(D + o_grids),
+                reinterpret_cast<const int*>(D + o_sc_field),
                 reinterpret_cast<const int32_t*>(D + o_sc_node), reinterpret_cast<const double*>(D + o_sc_t), cnt);
         TS_CUDA_TRY(ctx, cudaGetLastError());
     }
@@ -274,7 +307,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     args.barrier_timeout_ns = 5000000000LL;
     args.tol = Real(job.tol);
 
-    const int smem = engine_smem_bytes<S>(WARPS, int(sizeof(Real)));
+    const int smem = engine_smem_bytes<Real, S>(WARPS);
     void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, true>
                         : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, false>;
     TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -305,6 +338,62 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
 }
 
 }  // namespace
+
+// Fields of the job in dense grid order: same precision → strided copies; otherwise converted on the
+// device in blocks of fields, then copied.
+int fields_to_dense_host(ts_ctx* ctx, const EngineJob& job, int precision, void* out, int out_type) {
+    const size_t rsz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t osz = out_type == TS_OUT_F64 ? 8 : 4;
+    char* dst = static_cast<char*>(out);
+    for (size_t f = 0; f < job.fields.size(); f++) {
+        const host::Grid& g = *job.grids[job.fields[f].grid];
+        const int pitch = job.pitch[job.fields[f].grid];
+        const int64_t rows = int64_t(g.ny) * g.nz, n = rows * g.nx;
+        const char* src = static_cast<const char*>(job.fields[f].T);
+        if (rsz == osz) {
+            TS_CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, g.nx * osz, src + job.xoff * rsz, pitch * rsz, g.nx * rsz, rows,
+                                               cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            void* stage = ctx->buf("out.stage", size_t(n) * osz);
+            if (!stage) return TS_E_NOMEM;
+            int blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
+            if (rsz == 8)
+                dense_convert_kernel<double, float><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
+                    reinterpret_cast<const double*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<float*>(stage));
+            else
+                dense_convert_kernel<float, double><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
+                    reinterpret_cast<const float*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<double*>(stage));
+            TS_CUDA_TRY(ctx, cudaGetLastError());
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(dst, stage, size_t(n) * osz, cudaMemcpyDeviceToHost, ctx->stream));
+            TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        dst += size_t(n) * osz;
+    }
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return TS_OK;
+}
+
+// Fields of a one-grid job as dense float32 tables on the device (the .qttb rounding).
+int fields_to_dense_f32_device(ts_ctx* ctx, const EngineJob& job, int precision, float* out) {
+    if (job.fields.empty()) return TS_OK;
+    const host::Grid& g = *job.grids[0];
+    const int pitch = job.pitch[0];
+    const int64_t rows = int64_t(g.ny) * g.nz, n = rows * g.nx;
+    const int64_t stride = int64_t(pitch) * rows;
+    const int nf = int(job.fields.size());
+    int blocks = int(std::min<int64_t>((n + 255) / 256, 1024));
+    for (int f0 = 0; f0 < nf; f0 += 65535) {
+        int cnt = std::min(65535, nf - f0);
+        if (precision == TS_PRECISION_F64)
+            dense_convert_kernel<double, float><<<dim3(blocks, cnt), 256, 0, ctx->stream>>>(
+                static_cast<const double*>(job.fields[f0].T), stride, pitch, job.xoff, g.nx, rows, out + f0 * n);
+        else
+            dense_convert_kernel<float, float><<<dim3(blocks, cnt), 256, 0, ctx->stream>>>(
+                static_cast<const float*>(job.fields[f0].T), stride, pitch, job.xoff, g.nx, rows, out + f0 * n);
+        TS_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    return TS_OK;
+}
 
 template <typename Real>
 int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {

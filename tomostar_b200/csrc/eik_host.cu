@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "ctx.h"
@@ -64,10 +65,10 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
                        int rounds_out[2], ts_eik_stats* stats) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t n = g.count();
-    Real *hlon, *hlat, *zc = nullptr;
+    Real *wx, *wy, *zc = nullptr;
     int rc;
-    if ((rc = upload_real<Real>(ctx, "plain.hlon", m.hlon.data(), m.hlon.size(), &hlon))) return rc;
-    if ((rc = upload_real<Real>(ctx, "plain.hlat", m.hlat.data(), m.hlat.size(), &hlat))) return rc;
+    if ((rc = upload_real<Real>(ctx, "plain.wx", m.wx.data(), m.wx.size(), &wx))) return rc;
+    if ((rc = upload_real<Real>(ctx, "plain.wy", m.wy.data(), m.wy.size(), &wy))) return rc;
     if (g.variable && (rc = upload_real<Real>(ctx, "plain.zc", m.zc.data(), m.zc.size(), &zc))) return rc;
     TS_BUF(ctx, fixed, uint8_t, "plain.fixed", n);
     TS_BUF(ctx, dirty, uint8_t, "plain.dirty", n);
@@ -98,12 +99,12 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
                     int k0 = std::max(0, p - (nx - 1) - (ny - 1)), k1 = std::min(nz - 1, p);
                     dim3 grid((i1 - i0 + 1 + 127) / 128, k1 - k0 + 1);
                     if (g.variable)
-                        plain_sweep_kernel<Real, true><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, hlon, hlat,
-                                                                              Real(m.hr), zc, nx, ny, nz, phase,
+                        plain_sweep_kernel<Real, true><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, wx, wy,
+                                                                              Real(m.wz1), Real(m.wz2), zc, nx, ny, nz, phase,
                                                                               changed, dir, p, Real(tol), updates);
                     else
-                        plain_sweep_kernel<Real, false><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, hlon, hlat,
-                                                                               Real(m.hr), zc, nx, ny, nz, phase,
+                        plain_sweep_kernel<Real, false><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, wx, wy,
+                                                                               Real(m.wz1), Real(m.wz2), zc, nx, ny, nz, phase,
                                                                                changed, dir, p, Real(tol), updates);
                     launches++;
                 }
@@ -129,14 +130,83 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
     return TS_OK;
 }
 
+// ---- resident models -----------------------------------------------------------------------------------
+
+}  // namespace eik
+}  // namespace ts
+
+namespace ts {
+namespace eik {
+
+int model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int n_phases, int precision, int* id) {
+    if (const char* bad = host::Grid::validate(*grid)) return ctx->fail(TS_E_ARG, bad);
+    if (precision != TS_PRECISION_F64 && precision != TS_PRECISION_F32) return ctx->fail(TS_E_ARG, "precision");
+    auto* m = new ts_ctx::Model();
+    m->def = *grid;
+    if (grid->depth_km) {
+        m->depth.assign(grid->depth_km, grid->depth_km + grid->nz);
+        m->def.depth_km = m->depth.data();
+    }
+    m->grid = new host::Grid(m->def);
+    m->metric = new host::Metric(*m->grid);
+    m->precision = precision;
+    m->n_phases = n_phases;
+    const size_t count = size_t(m->grid->count()) * n_phases;
+    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    if (cudaMalloc(&m->slowness, count * esz) != cudaSuccess) {
+        cudaGetLastError();
+        m->slowness = nullptr;
+        delete m;
+        return ctx->fail(TS_E_NOMEM, "model slowness");
+    }
+    int rc = TS_OK;
+    if (precision == TS_PRECISION_F64) {
+        if (cudaMemcpy(m->slowness, slowness, count * 8, cudaMemcpyHostToDevice) != cudaSuccess) rc = TS_E_CUDA;
+    } else {
+        std::vector<float> tmp(count);
+        for (size_t q = 0; q < count; q++) tmp[q] = float(slowness[q]);
+        if (cudaMemcpy(m->slowness, tmp.data(), count * 4, cudaMemcpyHostToDevice) != cudaSuccess) rc = TS_E_CUDA;
+    }
+    if (rc) {
+        delete m;
+        return ctx->fail(rc, "model upload");
+    }
+    *id = ctx->next_model++;
+    ctx->models[*id] = m;
+    return TS_OK;
+}
+
+int model_drop(ts_ctx* ctx, int id) {
+    auto it = ctx->models.find(id);
+    if (it == ctx->models.end()) return ctx->fail(TS_E_ARG, "unknown model");
+    delete it->second;
+    ctx->models.erase(it);
+    return TS_OK;
+}
+
+void models_free(ts_ctx* ctx) {
+    for (auto& kv : ctx->models) delete kv.second;
+    ctx->models.clear();
+}
+
 // ---- C-ABI front end ---------------------------------------------------------------------------------
 
 template <typename Real>
-static int solve_impl(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_stats* stats) {
-    const char* bad = host::Grid::validate(*in.grid);
-    if (bad) return ctx->fail(TS_E_ARG, bad);
-    host::Grid g(*in.grid);
-    host::Metric m(g);
+static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, ts_eik_stats* stats) {
+    ts_ctx::Model* model = nullptr;
+    if (in.model_id > 0) {
+        auto it = ctx->models.find(in.model_id);
+        if (it == ctx->models.end()) return ctx->fail(TS_E_ARG, "unknown model");
+        model = it->second;
+        if (in.phase < 0 || in.phase >= model->n_phases) return ctx->fail(TS_E_ARG, "phase out of range");
+    } else {
+        const char* bad = host::Grid::validate(*in.grid);
+        if (bad) return ctx->fail(TS_E_ARG, bad);
+    }
+    std::unique_ptr<host::Grid> own_g(model ? nullptr : new host::Grid(*in.grid));
+    std::unique_ptr<host::Metric> own_m(model ? nullptr : new host::Metric(*own_g));
+    const host::Grid& g = model ? *model->grid : *own_g;
+    const host::Metric& m = model ? *model->metric : *own_m;
     const int64_t n = g.count();
     const int nf = in.n_fields;
     // Seeds of every field.
@@ -154,16 +224,20 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_
         if (sidx[f].empty()) return ctx->fail(TS_E_NOSEEDS, "no seed nodes for field " + std::to_string(f));
     // Slowness on the device in the solve's precision (the float kernel never meets a double).
     Real* slow_d;
-    int rc;
-    if ((rc = upload_real<Real>(ctx, "solve.slowness", in.slowness, size_t(n), &slow_d))) return rc;
-    TS_BUF(ctx, T, Real, "solve.fields", size_t(nf) * n);
+    int rc = TS_OK;
+    if (model) slow_d = static_cast<Real*>(model->slowness) + size_t(n) * in.phase;
+    else if ((rc = upload_real<Real>(ctx, "solve.slowness", in.slowness, size_t(n), &slow_d))) return rc;
     const int cap = in.max_rounds > 0 ? in.max_rounds : std::max(32, (g.nx + g.ny + g.nz) / 4);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, ctx->stream);
     int rounds_max[2] = {0, 0};
+    EngineJob job;
+    Real* T = nullptr;
     if (in.mode == TS_MODE_PLAIN) {
+        T = static_cast<Real*>(ctx->buf("solve.fields", sizeof(Real) * size_t(nf) * n));
+        if (!T) return TS_E_NOMEM;
         for (int f = 0; f < nf && rc == TS_OK; f++) {
             int r[2] = {0, 0};
             rc = plain_solve<Real>(ctx, g, m, slow_d, T + size_t(f) * n, sidx[f], st[f], in.tol, cap, r, stats);
@@ -171,7 +245,6 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_
             rounds_max[1] = std::max(rounds_max[1], r[1]);
         }
     } else {
-        EngineJob job;
         job.grids.push_back(&g);
         job.metrics.push_back(&m);
         job.tol = in.tol;
@@ -180,7 +253,6 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_
             EngineField ef;
             ef.grid = 0;
             ef.slowness = slow_d;
-            ef.T = T + size_t(f) * n;
             ef.seed_idx = &sidx[f];
             ef.seed_t = &st[f];
             ef.cap = cap;
@@ -211,14 +283,17 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_
         stats->device_ms = ms;
     }
     ctx->stats = std::to_string(rounds_max[0]) + "+" + std::to_string(rounds_max[1]) + " rounds of 8 sweeps";
-    *fields_dev = T;
-    return rc;
+    if (rc) return rc;
+    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    if (out_type == TS_OUT_NONE) return TS_OK;  // the fields stay on the device
+    if (in.mode == TS_MODE_PLAIN) return copy_fields_out(ctx, T, precision, int64_t(nf) * n, out, out_type);
+    return fields_to_dense_host(ctx, job, precision, out, out_type);
 }
 
-int solve_to_device(ts_ctx* ctx, const SolveIn& in, void** fields_dev, ts_eik_stats* stats) {
+int solve(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, ts_eik_stats* stats) {
     if (stats) std::memset(stats, 0, sizeof(*stats));
-    if (in.precision == TS_PRECISION_F64) return solve_impl<double>(ctx, in, fields_dev, stats);
-    if (in.precision == TS_PRECISION_F32) return solve_impl<float>(ctx, in, fields_dev, stats);
+    if (in.precision == TS_PRECISION_F64) return solve_impl<double>(ctx, in, out, out_type, stats);
+    if (in.precision == TS_PRECISION_F32) return solve_impl<float>(ctx, in, out, out_type, stats);
     return ctx->fail(TS_E_ARG, "precision must be 64 or 32");
 }
 

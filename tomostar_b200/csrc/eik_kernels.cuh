@@ -24,8 +24,8 @@ namespace eik {
 
 template <typename Real, bool VARZ>
 __global__ void plain_sweep_kernel(Real* __restrict__ T, const Real* __restrict__ slow, const uint8_t* __restrict__ fixed,
-                                   uint8_t* __restrict__ dirty, const Real* __restrict__ hlon,
-                                   const Real* __restrict__ hlat, Real hr, const Real* __restrict__ zc, int nx, int ny,
+                                   uint8_t* __restrict__ dirty, const Real* __restrict__ wx,
+                                   const Real* __restrict__ wy, Real wz1, Real wz2, const Real* __restrict__ zc, int nx, int ny,
                                    int nz, int second, int* changed, int dir, int p, Real tol,
                                    unsigned long long* updates) {
     int i0 = max(0, p - (ny - 1) - (nz - 1));
@@ -52,8 +52,8 @@ __global__ void plain_sweep_kernel(Real* __restrict__ T, const Real* __restrict_
                     j + 1 < ny ? T[node + nx] : inf, j > 1 ? T[node - 2 * nx] : inf,
                     j + 2 < ny ? T[node + 2 * nx] : inf, k > 0 ? T[node - nxy] : inf,
                     k + 1 < nz ? T[node + nxy] : inf, k > 1 ? T[node - 2 * nxy] : inf,
-                    k + 2 < nz ? T[node + 2 * nxy] : inf, hlon[k * ny + j], hlat[k], hr,
-                    VARZ ? zc + kZCoef * k : nullptr, second != 0);
+                    k + 2 < nz ? T[node + 2 * nxy] : inf, wx[2 * (k * ny + j)], wx[2 * (k * ny + j) + 1],
+                    wy[2 * k], wy[2 * k + 1], wz1, wz2, VARZ ? zc + kZCoef * k : nullptr, second != 0);
                 if (cand < cur) {
                     T[node] = cand;
                     if (counts_as_change<Real>(cur, cand, tol)) atomicOr(changed, 1);
@@ -107,15 +107,26 @@ struct GridDesc {
     int varz;                  // variable vertical spacing (extension)
     const int* diag_off;       // [ndiag + 1] offsets into diag_tiles
     const uint32_t* diag_tiles;// canonical tile coords (a | b << 10 | c << 20), ordered by a + b + c
-    const void* hlon;          // Real[nz * ny]
-    const void* hlat;          // Real[nz]
+    const void* wx;            // Real[2 * nz * ny]: longitude-axis weights (w1, w2) per (k, j)
+    const void* wy;            // Real[2 * nz]: latitude-axis weights per k
     const void* zc;            // Real[kZCoef * nz] when varz
-    double hr;
+    double wz1, wz2;           // depth-axis weights of a uniform grid
+    int pitch;                 // elements per padded field row (see FieldDesc::T)
+    int pad;
+};
+
+// The engine's field layout: every (k, j) row is padded to `pitch` elements, node (i, j, k) at
+// (k·ny + j)·pitch + HX + i with HX = 16 / sizeof(Real); the pads hold +inf and are never written.
+// A tile's row segment with its two-node x halo is then one 16-byte-aligned run of whole chunks.
+template <typename Real>
+struct Layout {
+    static constexpr int HX = 16 / int(sizeof(Real));
+    TS_HDINL static int pitch(int tiles_x, int bx) { return HX + tiles_x * bx + HX; }
 };
 
 template <typename Real>
 struct FieldDesc {
-    Real* T;              // the field, grid order
+    Real* T;              // the field, padded rows (Layout)
     const Real* s;        // its slowness
     uint8_t* dirty;       // one flag per tile
     int grid;             // GridDesc index
@@ -211,35 +222,41 @@ TS_DEVINL bool grid_barrier(Control* c, unsigned nblocks, long long timeout_ns) 
     return ok != 0;
 }
 
-template <int BX_, int BY_, int BZ_>
+template <typename Real, int BX_, int BY_, int BZ_>
 struct Shape {
     static constexpr int BX = BX_, BY = BY_, BZ = BZ_;
     static constexpr int N = BX * BY * BZ;
-    static constexpr int CX = BX + 4, CY = BY + 4, CZ = BZ + 4;
+    static constexpr int HX = Layout<Real>::HX;
+    static constexpr int CX = BX + 2 * HX, CY = BY + 4, CZ = BZ + 4;
     static constexpr int CUBE = CX * CY * CZ;
+    static constexpr int NCH = CX / HX;  // 16-byte chunks per cube row
     static constexpr int NPLANES = BX + BY + BZ - 2;
     static constexpr int MW = (N + 31) / 32;
-    TS_HDINL static int cidx(int i, int j, int k) { return ((k + 2) * CY + (j + 2)) * CX + (i + 2); }
+    static_assert(BX % HX == 0, "tile rows must be whole 16-byte chunks");
+    TS_HDINL static int cidx(int i, int j, int k) { return ((k + 2) * CY + (j + 2)) * CX + (i + HX); }
 };
 
 // Shared memory of one warp's tile: the node cube with a two-node halo on each face, the tile's
-// slowness, its metric rows and its fixed-node mask.
+// slowness, its axis weights and its fixed-node mask.
+template <class S>
+constexpr int warp_reals() {
+    return S::CUBE + S::N + 2 * S::BY * S::BZ + 2 * S::BZ + kZCoef * S::BZ;
+}
+
 template <typename Real, class S>
 struct WarpSmem {
-    static constexpr int kReals = S::CUBE + S::N + S::BY * S::BZ + S::BZ + kZCoef * S::BZ;
-    static constexpr int kBytes = ((kReals * int(sizeof(Real)) + S::MW * 4) + 15) / 16 * 16;
+    static constexpr int kBytes = ((warp_reals<S>() * int(sizeof(Real)) + S::MW * 4) + 15) / 16 * 16;
 };
 
-template <class S>
-constexpr int engine_smem_bytes(int warps, int real_size) {
-    return warps * ((((S::CUBE + S::N + S::BY * S::BZ + S::BZ + kZCoef * S::BZ) * real_size + S::MW * 4) + 15) / 16 * 16) +
-           ((S::N * 2 + 15) / 16 * 16) + (S::NPLANES + 1) * 4;
+template <typename Real, class S>
+constexpr int engine_smem_bytes(int warps) {
+    return warps * WarpSmem<Real, S>::kBytes + ((S::N * 2 + 15) / 16 * 16) + (S::NPLANES + 1) * 4;
 }
 
 // Processes one tile of one field for sweep ordering `dir`. Returns the node evaluations made.
 template <typename Real, class S, bool VARZ>
 TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
-                           int tz, int dir, bool second, Real* cube, Real* ss, Real* mhlon, Real* mhlat, Real* mzc,
+                           int tz, int dir, bool second, Real* cube, Real* ss, Real* mwx, Real* mwy, Real* mzc,
                            uint32_t* mask, const uint16_t* ptab, const int* poff, int lane) {
     const Real inf = real_inf<Real>();
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -250,14 +267,14 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
     const Real* __restrict__ slow = fd.s;
     if (lane == 0) __stcg(&fd.dirty[tid], (uint8_t)0);
 
-    // Metric rows of the tile.
-    const Real* hlon = static_cast<const Real*>(g.hlon);
-    const Real* hlat = static_cast<const Real*>(g.hlat);
-    for (int q = lane; q < S::BY * S::BZ; q += 32) {
-        int j = y0 + q % S::BY, k = z0 + q / S::BY;
-        mhlon[q] = (j < ny && k < nz) ? __ldg(&hlon[int64_t(k) * ny + j]) : Real(1);
+    // Axis weights of the tile's rows.
+    const Real* wx = static_cast<const Real*>(g.wx);
+    const Real* wy = static_cast<const Real*>(g.wy);
+    for (int q = lane; q < 2 * S::BY * S::BZ; q += 32) {
+        int r = q >> 1, j = y0 + r % S::BY, k = z0 + r / S::BY;
+        mwx[q] = (j < ny && k < nz) ? __ldg(&wx[2 * (int64_t(k) * ny + j) + (q & 1)]) : Real(1);
     }
-    for (int q = lane; q < S::BZ; q += 32) mhlat[q] = (z0 + q < nz) ? __ldg(&hlat[z0 + q]) : Real(1);
+    for (int q = lane; q < 2 * S::BZ; q += 32) mwy[q] = (z0 + (q >> 1) < nz) ? __ldg(&wy[2 * z0 + q]) : Real(1);
     if (VARZ) {
         const Real* zc = static_cast<const Real*>(g.zc);
         for (int q = lane; q < kZCoef * S::BZ; q += 32) {
@@ -265,36 +282,30 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
             mzc[q] = k < nz ? __ldg(&zc[int64_t(k) * kZCoef + q % kZCoef]) : Real(1);
         }
     }
-    // Interior nodes and slowness.
+    // The cube: every row segment the stencil reads (the interior rows with their x halo, and the
+    // y and z halo rows; the corner rows are never read), as asynchronous 16-byte copies, +inf for
+    // rows off the grid. The pads of a field row hold +inf, so x needs no check.
+    const int pitch = g.pitch;
+    for (int q = lane; q < S::CY * S::CZ * S::NCH; q += 32) {
+        int row = q / S::NCH, ch = q - row * S::NCH;
+        int jj = row % S::CY - 2, kk = row / S::CY - 2;
+        bool yin = jj >= 0 && jj < S::BY, zin = kk >= 0 && kk < S::BZ;
+        if (!yin && !zin) continue;
+        Real* dst = cube + row * S::CX + ch * S::HX;
+        int gy = y0 + jj, gz = z0 + kk;
+        if (gy >= 0 && gy < ny && gz >= 0 && gz < nz) {
+            cp_async16_cg(dst, T + (int64_t(gz) * ny + gy) * pitch + x0 + ch * S::HX);
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::HX; e++) dst[e] = inf;
+        }
+    }
+    // Slowness of the tile's nodes (read-only, dense grid order).
     for (int q = lane; q < S::N; q += 32) {
         int i = q % S::BX, j = (q / S::BX) % S::BY, k = q / (S::BX * S::BY);
         int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-        bool in = gx < nx && gy < ny && gz < nz;
-        int64_t idx = gz * nxy + int64_t(gy) * nx + gx;
-        cube[S::cidx(i, j, k)] = in ? ld_cg(&T[idx]) : inf;
-        ss[q] = in ? __ldg(&slow[idx]) : Real(0);
-    }
-    // Halo: two layers on each face (+inf off the grid).
-    for (int q = lane; q < 4 * S::BY * S::BZ; q += 32) {
-        int h = q & 3, r = q >> 2, j = r % S::BY, k = r / S::BY;
-        int i = h < 2 ? h - 2 : S::BX + h - 2;
-        int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-        bool in = gx >= 0 && gx < nx && gy < ny && gz < nz;
-        cube[S::cidx(i, j, k)] = in ? ld_cg(&T[gz * nxy + int64_t(gy) * nx + gx]) : inf;
-    }
-    for (int q = lane; q < 4 * S::BX * S::BZ; q += 32) {
-        int i = q % S::BX, r = q / S::BX, h = r & 3, k = r >> 2;
-        int j = h < 2 ? h - 2 : S::BY + h - 2;
-        int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-        bool in = gx < nx && gy >= 0 && gy < ny && gz < nz;
-        cube[S::cidx(i, j, k)] = in ? ld_cg(&T[gz * nxy + int64_t(gy) * nx + gx]) : inf;
-    }
-    for (int q = lane; q < 4 * S::BX * S::BY; q += 32) {
-        int i = q % S::BX, r = q / S::BX, j = r % S::BY, h = r / S::BY;
-        int k = h < 2 ? h - 2 : S::BZ + h - 2;
-        int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-        bool in = gx < nx && gy < ny && gz >= 0 && gz < nz;
-        cube[S::cidx(i, j, k)] = in ? ld_cg(&T[gz * nxy + int64_t(gy) * nx + gx]) : inf;
+        if (gx < nx && gy < ny && gz < nz) cp_async_ro(&ss[q], &slow[gz * nxy + int64_t(gy) * nx + gx]);
+        else ss[q] = Real(0);
     }
     // Fixed (seed) nodes of this tile, if any: binary search of the field's seed tiles.
     {
@@ -308,6 +319,7 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
         for (int q = lane; q < S::MW; q += 32)
             mask[q] = has ? __ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * S::MW + q]) : 0u;
     }
+    cp_async_wait_all();
     __syncwarp();
 
     // Node planes of the tile in the mirrored order of `dir`.
@@ -332,8 +344,9 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
             Real cand = Update<Real, VARZ>::eval(
                 ss[L], cube[c - 1], cube[c + 1], cube[c - 2], cube[c + 2], cube[c - S::CX], cube[c + S::CX],
                 cube[c - 2 * S::CX], cube[c + 2 * S::CX], cube[c - S::CX * S::CY], cube[c + S::CX * S::CY],
-                cube[c - 2 * S::CX * S::CY], cube[c + 2 * S::CX * S::CY], mhlon[k * S::BY + j], mhlat[k],
-                Real(g.hr), VARZ ? mzc + kZCoef * k : nullptr, second);
+                cube[c - 2 * S::CX * S::CY], cube[c + 2 * S::CX * S::CY], mwx[2 * (k * S::BY + j)],
+                mwx[2 * (k * S::BY + j) + 1], mwy[2 * k], mwy[2 * k + 1], Real(g.wz1), Real(g.wz2),
+                VARZ ? mzc + kZCoef * k : nullptr, second);
             if (cand < cur) {
                 cube[c] = cand;
                 any = true;
@@ -351,7 +364,7 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
         for (int q = lane; q < S::N; q += 32) {
             int i = q % S::BX, j = (q / S::BX) % S::BY, k = q / (S::BX * S::BY);
             int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-            if (gx < nx && gy < ny && gz < nz) st_cg(&T[gz * nxy + int64_t(gy) * nx + gx], cube[S::cidx(i, j, k)]);
+            if (gx < nx && gy < ny && gz < nz) st_cg(&T[(int64_t(gz) * ny + gy) * pitch + S::HX + gx], cube[S::cidx(i, j, k)]);
         }
         // A node of this tile may read a node that changed after it was evaluated: visit the tile
         // again next sweep. Neighbour tiles within two nodes of a changed node are woken too.
@@ -370,16 +383,16 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
 
 template <typename Real, int BX, int BY, int BZ, int WARPS, bool VARZ_ANY>
 __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
-    using S = Shape<BX, BY, BZ>;
+    using S = Shape<Real, BX, BY, BZ>;
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int kWarpBytes = WarpSmem<Real, S>::kBytes;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* mine = smem + warp * kWarpBytes;
     Real* cube = reinterpret_cast<Real*>(mine);
     Real* ss = cube + S::CUBE;
-    Real* mhlon = ss + S::N;
-    Real* mhlat = mhlon + S::BY * S::BZ;
-    Real* mzc = mhlat + S::BZ;
+    Real* mwx = ss + S::N;
+    Real* mwy = mwx + 2 * S::BY * S::BZ;
+    Real* mzc = mwy + 2 * S::BZ;
     uint32_t* mask = reinterpret_cast<uint32_t*>(mzc + kZCoef * S::BZ);
     uint16_t* ptab = reinterpret_cast<uint16_t*>(smem + WARPS * kWarpBytes);
     int* poff = reinterpret_cast<int*>(smem + WARPS * kWarpBytes + (S::N * 2 + 15) / 16 * 16);
@@ -444,11 +457,11 @@ __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
                         bool second = *(volatile const int*)&a.state[ff].phase == 1;
                         int ev;
                         if (VARZ_ANY && g.varz)
-                            ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mhlon,
-                                                             mhlat, mzc, mask, ptab, poff, lane);
+                            ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
+                                                             mwy, mzc, mask, ptab, poff, lane);
                         else
-                            ev = process_tile<Real, S, false>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mhlon,
-                                                              mhlat, mzc, mask, ptab, poff, lane);
+                            ev = process_tile<Real, S, false>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
+                                                              mwy, mzc, mask, ptab, poff, lane);
                         my_updates += ev;
                         my_visits += 1;
                     }

@@ -19,13 +19,18 @@
 
 namespace ts {
 
-// Per-level coefficients of a non-uniform z axis, 12 per level k:
-//   [0..5]  minus side: h1 (spacing to k-1), a, b, c, 1/a, c/a   (second partner k-2)
-//   [6..11] plus side:  h1 (spacing to k+1), a, b, c, 1/a, c/a   (second partner k+2)
+// Per-level coefficients of a non-uniform z axis, 16 per level k:
+//   [0..7]  minus side (first neighbour k-1, second k-2): w1, w2, a, b, c, c/a, -, -
+//   [8..15] plus side  (first neighbour k+1, second k+2): w1, w2, a, b, c, c/a, -, -
 // with the one-sided three-point derivative a·T0 − b·T1 + c·T2, a = (2h1+h2)/(h1(h1+h2)),
-// b = (h1+h2)/(h1 h2), c = h1/(h2(h1+h2)). Uniform spacing gives a = 3/(2h), b = 2/h, c = 1/(2h),
-// i.e. the reference's (4T1 − T2)/3 and 2h/3.
-constexpr int kZCoef = 12;
+// b = (h1+h2)/(h1 h2), c = h1/(h2(h1+h2)) (h1 = spacing to the first neighbour, h2 from there to
+// the second), w1 = 1/(h1·h1) the first-order weight and w2 = 1/((1/a)·(1/a)) the second-order one.
+// Uniform spacing gives a = 3/(2h), b = 2/h, c = 1/(2h): the reference's (4T1 − T2)/3 and 2h/3.
+constexpr int kZCoef = 16;
+
+// The weights of an axis term are precomputed per axis and level on the host with the reference's
+// own operations (w1 = 1.0 / (h * h), w2 = 1.0 / (he * he) with he = 2 * h / 3;
+// SphericalEikonal.cs:369, 391), so they are the same bits the reference divides out per update.
 
 // ---- FP64, exact --------------------------------------------------------------------------------
 
@@ -35,10 +40,11 @@ TS_DEVINL double dsub(double a, double b) { return __dadd_rn(a, -b); }
 TS_DEVINL double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // One axis's term (SphericalEikonal.cs:381-395): the smaller neighbour, promoted to second order
-// when its partner beyond is finite and not larger. Unused terms keep t = +inf and sort last.
+// when its partner beyond is finite and not larger. Produces (effective time, weight, neighbour
+// time); unused terms keep t = +inf and sort last.
 template <bool VARZ>
-TS_DEVINL void axis64(double minus, double plus, double minus2, double plus2, double h, const double* zc,
-                      bool second, double& te, double& he, double& tn, int& used) {
+TS_DEVINL void axis64(double minus, double plus, double minus2, double plus2, double w1, double w2, const double* zc,
+                      bool second, double& te, double& we, double& tn, int& used) {
     double first, t2;
     bool minus_side = minus <= plus;
     if (minus_side) { first = minus; t2 = minus2; }
@@ -46,12 +52,12 @@ TS_DEVINL void axis64(double minus, double plus, double minus2, double plus2, do
     if (!(first <= 1.7976931348623157e308)) return;  // not finite (first is never NaN)
     bool promote = second && (t2 <= 1.7976931348623157e308) && t2 <= first;
     if (!VARZ) {
-        if (promote) { te = ddiv(dsub(dmul(4.0, first), t2), 3.0); he = ddiv(dmul(2.0, h), 3.0); }
-        else { te = first; he = h; }
+        if (promote) { te = ddiv(dsub(dmul(4.0, first), t2), 3.0); we = w2; }
+        else { te = first; we = w1; }
     } else {
-        const double* c = zc + (minus_side ? 0 : 6);
-        if (promote) { te = ddiv(dsub(dmul(c[2], first), dmul(c[3], t2)), c[1]); he = c[4]; }
-        else { te = first; he = c[0]; }
+        const double* c = zc + (minus_side ? 0 : 8);
+        if (promote) { te = ddiv(dsub(dmul(c[3], first), dmul(c[4], t2)), c[2]); we = c[1]; }
+        else { te = first; we = c[0]; }
     }
     tn = first;
     used++;
@@ -74,15 +80,14 @@ TS_DEVINL void sort3(R* t, R* h, R* n) {
 
 // The Godunov root over the first `terms` sorted terms; false when the discriminant is negative
 // or the root falls below a neighbour it used (SphericalEikonal.cs:364-378).
-TS_DEVINL bool root64(int terms, const double* t, const double* h, const double* n, double s, double& root) {
+TS_DEVINL bool root64(int terms, const double* t, const double* w, const double* n, double s, double& root) {
     double sw = 0.0, swt = 0.0, swt2 = 0.0;
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         if (r < terms) {
-            double w = ddiv(1.0, dmul(h[r], h[r]));
-            sw = dadd(sw, w);
-            swt = dadd(swt, dmul(w, t[r]));
-            swt2 = dadd(swt2, dmul(dmul(w, t[r]), t[r]));
+            sw = dadd(sw, w[r]);
+            swt = dadd(swt, dmul(w[r], t[r]));
+            swt2 = dadd(swt2, dmul(dmul(w[r], t[r]), t[r]));
         }
     }
     double disc = dsub(dmul(swt, swt), dmul(sw, dsub(swt2, dmul(s, s))));
@@ -95,24 +100,25 @@ TS_DEVINL bool root64(int terms, const double* t, const double* h, const double*
 }
 
 // RelaxNode (SphericalEikonal.cs:349-379): the candidate time of a node from its 12 neighbour
-// values (+inf off the grid). xm/xp = i∓1, xm2/xp2 = i∓2, likewise y and z.
+// values (+inf off the grid). xm/xp = i∓1, xm2/xp2 = i∓2, likewise y and z; (w1, w2) are each
+// axis's first- and second-order weights.
 template <bool VARZ>
 TS_DEVINL double update64(double s, double xm, double xp, double xm2, double xp2, double ym, double yp, double ym2,
-                          double yp2, double zm, double zp, double zm2, double zp2, double hx, double hy, double hz,
-                          const double* zc, bool second) {
+                          double yp2, double zm, double zp, double zm2, double zp2, double wx1, double wx2,
+                          double wy1, double wy2, double wz1, double wz2, const double* zc, bool second) {
     const double inf = dinf();
     if (!(s > 0.0)) return inf;
-    double t[3] = {inf, inf, inf}, h[3] = {1.0, 1.0, 1.0}, n[3] = {inf, inf, inf};
+    double t[3] = {inf, inf, inf}, w[3] = {1.0, 1.0, 1.0}, n[3] = {inf, inf, inf};
     int used = 0;
-    axis64<false>(xm, xp, xm2, xp2, hx, nullptr, second, t[0], h[0], n[0], used);
-    axis64<false>(ym, yp, ym2, yp2, hy, nullptr, second, t[1], h[1], n[1], used);
-    axis64<VARZ>(zm, zp, zm2, zp2, hz, zc, second, t[2], h[2], n[2], used);
+    axis64<false>(xm, xp, xm2, xp2, wx1, wx2, nullptr, second, t[0], w[0], n[0], used);
+    axis64<false>(ym, yp, ym2, yp2, wy1, wy2, nullptr, second, t[1], w[1], n[1], used);
+    axis64<VARZ>(zm, zp, zm2, zp2, wz1, wz2, zc, second, t[2], w[2], n[2], used);
     if (used == 0) return inf;
-    sort3(t, h, n);
+    sort3(t, w, n);
     double root;
-    if (used >= 3 && root64(3, t, h, n, s, root)) return root;
-    if (used >= 2 && root64(2, t, h, n, s, root)) return root;
-    if (root64(1, t, h, n, s, root)) return root;
+    if (used >= 3 && root64(3, t, w, n, s, root)) return root;
+    if (used >= 2 && root64(2, t, w, n, s, root)) return root;
+    if (root64(1, t, w, n, s, root)) return root;
     return inf;
 }
 
@@ -140,31 +146,30 @@ TS_DEVINL Pick32 pick32(float minus, float plus, float minus2, float plus2) {
 }
 
 template <bool VARZ>
-TS_DEVINL void term32(const Pick32& p, float r, float h, const float* zc, bool second, float& te, float& he,
+TS_DEVINL void term32(const Pick32& p, float r, float w1, float w2, const float* zc, bool second, float& te, float& we,
                       float& tn) {
     float of = fsub(p.first, r);
     bool promote = second && (p.t2 <= 3.4028234663852886e38f) && p.t2 <= p.first;
     if (!VARZ) {
-        if (promote) { te = ffma(fsub(p.first, p.t2), 0.333333343f, of); he = fmul(h, 0.666666687f); }
-        else { te = of; he = h; }
+        if (promote) { te = ffma(fsub(p.first, p.t2), 0.333333343f, of); we = w2; }
+        else { te = of; we = w1; }
     } else {
-        const float* c = zc + (p.minus_side ? 0 : 6);
-        if (promote) { te = ffma(fsub(p.first, p.t2), c[5], of); he = c[4]; }
-        else { te = of; he = c[0]; }
+        const float* c = zc + (p.minus_side ? 0 : 8);
+        if (promote) { te = ffma(fsub(p.first, p.t2), c[5], of); we = c[1]; }
+        else { te = of; we = c[0]; }
     }
     tn = of;
 }
 
-TS_DEVINL bool root32(int terms, const float* t, const float* h, const float* n, float s, float& root) {
+TS_DEVINL bool root32(int terms, const float* t, const float* w, const float* n, float s, float& root) {
     float base = t[0];
     float sw = 0.f, swd = 0.f, swd2 = 0.f;
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         if (r < terms) {
-            float w = fdiv(1.0f, fmul(h[r], h[r]));
             float d = fsub(t[r], base);
-            sw = fadd(sw, w);
-            float wd = fmul(w, d);
+            sw = fadd(sw, w[r]);
+            float wd = fmul(w[r], d);
             swd = fadd(swd, wd);
             swd2 = ffma(wd, d, swd2);
         }
@@ -181,22 +186,22 @@ TS_DEVINL bool root32(int terms, const float* t, const float* h, const float* n,
 // The FP32 candidate time of a node (same inputs as update64).
 template <bool VARZ>
 TS_DEVINL float update32(float s, float xm, float xp, float xm2, float xp2, float ym, float yp, float ym2, float yp2,
-                         float zm, float zp, float zm2, float zp2, float hx, float hy, float hz, const float* zc,
-                         bool second) {
+                         float zm, float zp, float zm2, float zp2, float wx1, float wx2, float wy1, float wy2,
+                         float wz1, float wz2, const float* zc, bool second) {
     const float inf = real_inf<float>();
     if (!(s > 0.f)) return inf;
     Pick32 px = pick32(xm, xp, xm2, xp2), py = pick32(ym, yp, ym2, yp2), pz = pick32(zm, zp, zm2, zp2);
     int used = int(px.ok) + int(py.ok) + int(pz.ok);
     if (used == 0) return inf;
     float r = fminf(px.ok ? px.first : inf, fminf(py.ok ? py.first : inf, pz.ok ? pz.first : inf));
-    float t[3] = {inf, inf, inf}, h[3] = {1.f, 1.f, 1.f}, n[3] = {inf, inf, inf};
-    if (px.ok) term32<false>(px, r, hx, nullptr, second, t[0], h[0], n[0]);
-    if (py.ok) term32<false>(py, r, hy, nullptr, second, t[1], h[1], n[1]);
-    if (pz.ok) term32<VARZ>(pz, r, hz, zc, second, t[2], h[2], n[2]);
-    sort3(t, h, n);
+    float t[3] = {inf, inf, inf}, w[3] = {1.f, 1.f, 1.f}, n[3] = {inf, inf, inf};
+    if (px.ok) term32<false>(px, r, wx1, wx2, nullptr, second, t[0], w[0], n[0]);
+    if (py.ok) term32<false>(py, r, wy1, wy2, nullptr, second, t[1], w[1], n[1]);
+    if (pz.ok) term32<VARZ>(pz, r, wz1, wz2, zc, second, t[2], w[2], n[2]);
+    sort3(t, w, n);
     float root;
-    bool found = (used >= 3 && root32(3, t, h, n, s, root)) || (used >= 2 && root32(2, t, h, n, s, root)) ||
-                 root32(1, t, h, n, s, root);
+    bool found = (used >= 3 && root32(3, t, w, n, s, root)) || (used >= 2 && root32(2, t, w, n, s, root)) ||
+                 root32(1, t, w, n, s, root);
     return found ? fadd(r, root) : inf;
 }
 
@@ -207,18 +212,21 @@ struct Update;
 template <bool VARZ>
 struct Update<double, VARZ> {
     TS_DEVINL static double eval(double s, double xm, double xp, double xm2, double xp2, double ym, double yp,
-                                 double ym2, double yp2, double zm, double zp, double zm2, double zp2, double hx,
-                                 double hy, double hz, const double* zc, bool second) {
-        return update64<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, hx, hy, hz, zc, second);
+                                 double ym2, double yp2, double zm, double zp, double zm2, double zp2, double wx1,
+                                 double wx2, double wy1, double wy2, double wz1, double wz2, const double* zc,
+                                 bool second) {
+        return update64<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
+                              zc, second);
     }
 };
 
 template <bool VARZ>
 struct Update<float, VARZ> {
     TS_DEVINL static float eval(float s, float xm, float xp, float xm2, float xp2, float ym, float yp, float ym2,
-                                float yp2, float zm, float zp, float zm2, float zp2, float hx, float hy, float hz,
-                                const float* zc, bool second) {
-        return update32<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, hx, hy, hz, zc, second);
+                                float yp2, float zm, float zp, float zm2, float zp2, float wx1, float wx2, float wy1,
+                                float wy2, float wz1, float wz2, const float* zc, bool second) {
+        return update32<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
+                              zc, second);
     }
 };
 

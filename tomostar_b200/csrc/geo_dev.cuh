@@ -1,0 +1,139 @@
+// Device geometry for the ray tracer: GeoMath (Geo/GeoMath.cs:49-80, 146-151), SphericalGrid
+// fractional coordinates and trilinear weights (Geo/SphericalGrid.cs:179-224), and the float32
+// travel-time table's Time and Gradient (Forward/TravelTimeTable.cs:116-157), in double with the
+// reference's expression order.
+#pragma once
+
+#include "ts_common.cuh"
+
+namespace ts {
+namespace geo {
+
+struct V3 {
+    double x, y, z;
+};
+TS_DEVINL V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+TS_DEVINL V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+TS_DEVINL V3 scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+TS_DEVINL double norm(V3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+struct GeoPt {
+    double lon, lat, dep;
+};
+
+// GeoMath.ToCartesian.
+TS_DEVINL V3 to_cartesian(double lon_deg, double lat_deg, double depth_km) {
+    double r = kEarthRadiusKm - depth_km;
+    double sl, cl, so, co;
+    sincos(lat_deg * kDeg2Rad, &sl, &cl);
+    sincos(lon_deg * kDeg2Rad, &so, &co);
+    return {r * cl * co, r * cl * so, r * sl};
+}
+
+// GeoMath.FromCartesian.
+TS_DEVINL GeoPt from_cartesian(V3 v) {
+    double r = norm(v);
+    if (r <= 0) return {0, 0, kEarthRadiusKm};
+    double z = fmin(fmax(v.z / r, -1.0), 1.0);
+    return {atan2(v.y, v.x) * kRad2Deg, asin(z) * kRad2Deg, kEarthRadiusKm - r};
+}
+
+// GeoMath.UnwrapLon.
+TS_DEVINL double unwrap_lon(double lon, double ref) {
+    if (lon < ref - 180) lon += 360 * ceil((ref - 180 - lon) / 360);
+    else if (lon > ref + 180) lon -= 360 * ceil((lon - ref - 180) / 360);
+    return lon;
+}
+
+// A uniform spherical grid as the tracer needs it (GridDefinition + SphericalGrid fields).
+struct RGrid {
+    int nx, ny, nz, pad;
+    double min_lon, min_lat, min_dep;
+    double dlon, dlat, ddep;          // degrees, degrees, km
+    double dlon_rad, dlat_rad;
+    double centre_lon;
+    double lon_last, lat_last, dep_last;  // LonDeg[^1], LatDeg[^1], DepthKm[^1]
+    double min_spacing_km;            // MinSpacingKm
+};
+
+// SphericalGrid.Fractional.
+TS_DEVINL void fractional(const RGrid& g, double lon, double lat, double dep, double& fx, double& fy, double& fz) {
+    if (lon < g.centre_lon - 180 || lon > g.centre_lon + 180) lon = unwrap_lon(lon, g.centre_lon);
+    fx = (lon - g.min_lon) / g.dlon;
+    fy = (lat - g.min_lat) / g.dlat;
+    fz = (dep - g.min_dep) / g.ddep;
+}
+
+// SphericalGrid.TrilinearWeightsFractional: base corner and the eight weights (di fastest).
+TS_DEVINL void weights(const RGrid& g, double fx, double fy, double fz, int& i0, int& j0, int& k0, double* w) {
+    fx = fmin(fmax(fx, 0.0), double(g.nx - 1));
+    fy = fmin(fmax(fy, 0.0), double(g.ny - 1));
+    fz = fmin(fmax(fz, 0.0), double(g.nz - 1));
+    i0 = min(int(fx), g.nx - 2);
+    j0 = min(int(fy), g.ny - 2);
+    k0 = min(int(fz), g.nz - 2);
+    double tx = fx - i0, ty = fy - j0, tz = fz - k0;
+    int n = 0;
+#pragma unroll
+    for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+            for (int di = 0; di < 2; di++) {
+                w[n] = (di == 0 ? 1 - tx : tx) * (dj == 0 ? 1 - ty : ty) * (dk == 0 ? 1 - tz : tz);
+                n++;
+            }
+}
+
+// TravelTimeTable.TimeFractional: trilinear on float32 nodes; +inf if a weighted corner is not finite.
+TS_DEVINL double time_fractional(const RGrid& g, const float* __restrict__ tb, double fx, double fy, double fz) {
+    int i0, j0, k0;
+    double w[8];
+    weights(g, fx, fy, fz, i0, j0, k0, w);
+    const int64_t nxy = int64_t(g.nx) * g.ny;
+    const int64_t base = k0 * nxy + int64_t(j0) * g.nx + i0;
+    double t = 0;
+    int n = 0;
+#pragma unroll
+    for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+            for (int di = 0; di < 2; di++) {
+                if (w[n] != 0) {
+                    float v = __ldg(&tb[base + dk * nxy + dj * g.nx + di]);
+                    if (!isfinite(v)) return dinf();
+                    t += double(v) * w[n];
+                }
+                n++;
+            }
+    return t;
+}
+
+TS_DEVINL double table_time(const RGrid& g, const float* tb, double lon, double lat, double dep) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    return time_fractional(g, tb, fx, fy, fz);
+}
+
+// TravelTimeTable.Gradient: central differences of the interpolant half a node each side, in
+// (east, north, down) s/km.
+TS_DEVINL void table_gradient(const RGrid& g, const float* tb, double lon, double lat, double dep, double& ge,
+                              double& gn, double& gz) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    const double d = 0.5;
+    double tx = (time_fractional(g, tb, fx + d, fy, fz) - time_fractional(g, tb, fx - d, fy, fz)) / (2 * d);
+    double ty = (time_fractional(g, tb, fx, fy + d, fz) - time_fractional(g, tb, fx, fy - d, fz)) / (2 * d);
+    double tz = (time_fractional(g, tb, fx, fy, fz + d) - time_fractional(g, tb, fx, fy, fz - d)) / (2 * d);
+    double r = kEarthRadiusKm - dep;
+    double hx = r * cos(lat * kDeg2Rad) * g.dlon_rad;
+    double hy = r * g.dlat_rad;
+    double hz = g.ddep;
+    ge = tx / hx;
+    gn = ty / hy;
+    gz = tz / hz;
+}
+
+}  // namespace geo
+}  // namespace ts

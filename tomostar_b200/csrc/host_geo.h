@@ -141,35 +141,53 @@ struct Grid {
     }
 };
 
-// GridMetric (Forward/SphericalEikonal.cs:15-35) and the per-level z coefficients of the extension
-// (layout documented in eik_update.cuh).
+// GridMetric (Forward/SphericalEikonal.cs:15-35), the axis weights of the upwind terms and the
+// per-level z coefficients of the extension (layout documented in eik_update.cuh). The weights are
+// the reference's own divisions (SphericalEikonal.cs:369, 391): w1 = 1.0 / (h * h) first order,
+// w2 = 1.0 / (he * he) with he = 2 * h / 3 second order, computed once per axis and level.
 struct Metric {
     std::vector<double> hlon, hlat, zc;
-    double hr = 0;
+    std::vector<double> wx;  // 2 per (k, j): w1, w2 of the longitude axis
+    std::vector<double> wy;  // 2 per k: latitude axis
+    double hr = 0, wz1 = 1, wz2 = 1;
+    static void weights(double h, double& w1, double& w2) {
+        w1 = 1.0 / (h * h);
+        double he = 2 * h / 3;
+        w2 = 1.0 / (he * he);
+    }
     explicit Metric(const Grid& g) {
         hlon.resize(size_t(g.ny) * g.nz);
         hlat.resize(g.nz);
+        wx.resize(2 * hlon.size());
+        wy.resize(2 * size_t(g.nz));
         for (int k = 0; k < g.nz; k++) {
             hlat[k] = g.rad[k] * g.dlat_rad;
-            for (int j = 0; j < g.ny; j++) hlon[size_t(k) * g.ny + j] = std::max(1e-9, g.rad[k] * g.coslat[j] * g.dlon_rad);
+            weights(hlat[k], wy[2 * k], wy[2 * k + 1]);
+            for (int j = 0; j < g.ny; j++) {
+                size_t q = size_t(k) * g.ny + j;
+                hlon[q] = std::max(1e-9, g.rad[k] * g.coslat[j] * g.dlon_rad);
+                weights(hlon[q], wx[2 * q], wx[2 * q + 1]);
+            }
         }
         hr = g.ddep;
+        weights(hr, wz1, wz2);
         if (g.variable) {
-            zc.assign(size_t(12) * g.nz, 1.0);
+            zc.assign(size_t(16) * g.nz, 1.0);
             auto side = [&](double* c, double h1, double h2) {
                 double a = (2 * h1 + h2) / (h1 * (h1 + h2));
                 double b = (h1 + h2) / (h1 * h2);
                 double cc = h1 / (h2 * (h1 + h2));
-                c[0] = h1; c[1] = a; c[2] = b; c[3] = cc; c[4] = 1 / a; c[5] = cc / a;
+                double he = 1 / a;
+                c[0] = 1.0 / (h1 * h1); c[1] = 1.0 / (he * he); c[2] = a; c[3] = b; c[4] = cc; c[5] = cc / a;
             };
             for (int k = 0; k < g.nz; k++) {
-                double* c = &zc[size_t(12) * k];
+                double* c = &zc[size_t(16) * k];
                 double hm = k > 0 ? g.dep[k] - g.dep[k - 1] : 1.0;
                 double hm2 = k > 1 ? g.dep[k - 1] - g.dep[k - 2] : hm;
                 double hp = k + 1 < g.nz ? g.dep[k + 1] - g.dep[k] : 1.0;
                 double hp2 = k + 2 < g.nz ? g.dep[k + 2] - g.dep[k + 1] : hp;
                 side(c, hm, hm2);
-                side(c + 6, hp, hp2);
+                side(c + 8, hp, hp2);
             }
         }
     }

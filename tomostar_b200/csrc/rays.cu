@@ -1,0 +1,550 @@
+// Rays and Jacobian rows on the device: RayTracing.Backtrack (Forward/RayTracing.cs:73-111),
+// RayTracing.Kernel (:118-159) and RayKernels' row finalisation (Tomography/RayKernels.cs:79-97).
+//
+// Three kernels per chunk of rays, none with atomics:
+//   trace_kernel  one thread per ray: steepest descent on the station's float32 table, each new
+//                 polyline segment integrated at once against the trilinear basis of the inversion
+//                 grid. Pieces falling in the same inversion cell are summed before a record
+//                 (node, length) is written, so a ray writes about one record per node per cell.
+//   merge_kernel  one warp per ray: sorts the ray's records by node (bitonic, shared memory, the
+//                 record index breaking ties so equal nodes keep visit order), sums each node's
+//                 lengths in that order and writes the unique nodes ascending, lengths as float32.
+//   emit_kernel   one warp per ray: copies the row into the CSR arrays at its scanned offset.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+#include "geo_dev.cuh"
+#include "host_geo.h"
+#include "rays.h"
+
+namespace ts {
+namespace rays {
+
+using geo::GeoPt;
+using geo::RGrid;
+using geo::V3;
+
+constexpr int kDropped = -1;   // the reference returns null: the row is left out
+constexpr int kOverflow = -2;  // more records than the chunk's capacity: traced again with more
+
+struct TraceArgs {
+    RGrid fwd, inv;
+    const float* tables;
+    int64_t table_n;
+    const double* table_station;  // 3 per table
+    const int* table_of;          // per ray
+    const double* events;         // 3 per ray
+    int ray0, nrays;
+    double step_km, piece_km;
+    int cap;
+    int* rec_node;                // [nrays * cap]
+    double* rec_val;
+    int* rec_count;               // per chunk ray
+    double* tcg;                  // 4 per ray (global index)
+};
+
+// Per-ray record writer with the current inversion cell's eight accumulators.
+struct Recorder {
+    int ci = -1, cj = 0, ck = 0;
+    unsigned touched = 0;
+    double acc[8];
+    int count = 0;
+    bool overflow = false;
+
+    TS_DEVINL void flush(const TraceArgs& a, int r) {
+        if (ci < 0 || !touched) return;
+        const int nx = a.inv.nx;
+        const int64_t nxy = int64_t(a.inv.nx) * a.inv.ny;
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            if (!((touched >> n) & 1u)) continue;
+            if (count >= a.cap) {
+                overflow = true;
+                continue;
+            }
+            int di = n & 1, dj = (n >> 1) & 1, dk = n >> 2;
+            int64_t slot = int64_t(r) * a.cap + count;
+            a.rec_node[slot] = int((ck + dk) * nxy + int64_t(cj + dj) * nx + (ci + di));
+            a.rec_val[slot] = acc[n];
+            count++;
+        }
+        touched = 0;
+    }
+
+    // RayTracing.Kernel for one polyline segment (RayTracing.cs:133-157).
+    TS_DEVINL void segment(const TraceArgs& a, int r, GeoPt pa, GeoPt pb) {
+        V3 A = geo::to_cartesian(pa.lon, pa.lat, pa.dep);
+        V3 B = geo::to_cartesian(pb.lon, pb.lat, pb.dep);
+        V3 d = geo::sub(B, A);
+        double len = geo::norm(d);
+        if (len <= 0) return;
+        int pieces = max(1, int(ceil(len / a.piece_km)));
+        double dl = len / pieces;
+        for (int q = 0; q < pieces; q++) {
+            GeoPt mid = geo::from_cartesian(geo::add(A, geo::scale(d, (q + 0.5) / pieces)));
+            double fx, fy, fz;
+            geo::fractional(a.inv, mid.lon, mid.lat, mid.dep, fx, fy, fz);
+            int i0, j0, k0;
+            double w[8];
+            geo::weights(a.inv, fx, fy, fz, i0, j0, k0, w);
+            if (i0 != ci || j0 != cj || k0 != ck) {
+                flush(a, r);
+                ci = i0; cj = j0; ck = k0;
+#pragma unroll
+                for (int n = 0; n < 8; n++) acc[n] = 0.0;
+            }
+#pragma unroll
+            for (int n = 0; n < 8; n++) {
+                if (w[n] == 0) continue;
+                acc[n] += dl * w[n] * 1.0;
+                touched |= 1u << n;
+            }
+        }
+    }
+};
+
+__global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nrays) return;
+    const int ray = a.ray0 + r;
+    const int tab = a.table_of[ray];
+    const float* tb = a.tables + int64_t(tab) * a.table_n;
+    const RGrid& g = a.fwd;
+    const double st_lon = a.table_station[3 * tab], st_lat = a.table_station[3 * tab + 1];
+    const double st_dep = fmin(fmax(a.table_station[3 * tab + 2], g.min_dep), g.dep_last);
+    const GeoPt ev{a.events[3 * ray], a.events[3 * ray + 1], a.events[3 * ray + 2]};
+    double* tcg = a.tcg + 4 * int64_t(ray);
+
+    // Backtrack (RayTracing.cs:75-110).
+    V3 station = geo::to_cartesian(st_lon, st_lat, st_dep);
+    V3 p = geo::to_cartesian(ev.lon, ev.lat, ev.dep);
+    double t0 = geo::table_time(g, tb, ev.lon, ev.lat, ev.dep);
+    tcg[0] = t0;
+    if (!isfinite(t0)) {
+        a.rec_count[r] = kDropped;
+        return;
+    }
+    geo::table_gradient(g, tb, ev.lon, ev.lat, ev.dep, tcg[1], tcg[2], tcg[3]);
+    const double step = a.step_km;
+    const int max_steps = 20 * int(ceil(geo::norm(geo::sub(p, station)) / step + 10));
+    double last_t = t0;
+    int stalls = 0;
+    Recorder rec;
+    GeoPt prev = ev;
+    for (int s = 0; s < max_steps; s++) {
+        if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
+        GeoPt gp = geo::from_cartesian(p);
+        double ge, gn, gz;
+        geo::table_gradient(g, tb, gp.lon, gp.lat, gp.dep, ge, gn, gz);
+        if (!isfinite(ge) || !isfinite(gn) || !isfinite(gz)) {
+            a.rec_count[r] = kDropped;
+            return;
+        }
+        // LocalFrame (GeoMath.cs:71-80) and the step against the gradient.
+        double sl, cl, so, co;
+        sincos(gp.lat * kDeg2Rad, &sl, &cl);
+        sincos(gp.lon * kDeg2Rad, &so, &co);
+        V3 e{-so, co, 0}, nn{-sl * co, -sl * so, cl}, up{cl * co, cl * so, sl};
+        V3 grad = geo::add(geo::add(geo::scale(e, ge), geo::scale(nn, gn)), geo::scale(up, -gz));
+        double nrm = geo::norm(grad);
+        if (nrm < 1e-12) {
+            a.rec_count[r] = kDropped;
+            return;
+        }
+        p = geo::sub(p, geo::scale(grad, step / nrm));
+        GeoPt q = geo::from_cartesian(p);
+        q.lon = fmin(fmax(geo::unwrap_lon(q.lon, g.centre_lon), g.min_lon), g.lon_last);
+        q.lat = fmin(fmax(q.lat, g.min_lat), g.lat_last);
+        q.dep = fmin(fmax(q.dep, g.min_dep), g.dep_last);
+        p = geo::to_cartesian(q.lon, q.lat, q.dep);
+        rec.segment(a, r, prev, q);
+        prev = q;
+        double t = geo::table_time(g, tb, q.lon, q.lat, q.dep);
+        if (!(t < last_t)) {
+            if (++stalls > 20) {
+                a.rec_count[r] = kDropped;
+                return;
+            }
+        } else {
+            stalls = 0;
+        }
+        last_t = fmin(last_t, t);
+    }
+    rec.segment(a, r, prev, GeoPt{st_lon, st_lat, st_dep});
+    rec.flush(a, r);
+    a.rec_count[r] = rec.overflow ? kOverflow : rec.count;
+}
+
+// One warp per ray: sort records by (node, record index), sum each node in record order, write
+// the unique nodes ascending. P is the power-of-two sort size of one warp's shared memory.
+// A pass handles the rays with lo < records <= P; the first pass (lo = 0) also writes the empty
+// and dropped rows and marks the rays left for a larger pass.
+__global__ void merge_kernel(const int* __restrict__ rec_node, const double* __restrict__ rec_val,
+                             const int* __restrict__ rec_count, int cap, int nrays, int P, int lo,
+                             int* __restrict__ out_node, float* __restrict__ out_len, int* __restrict__ nnz) {
+    extern __shared__ unsigned long long keys_all[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    unsigned long long* keys = keys_all + size_t(warp) * P;
+    for (int r = blockIdx.x * wpb + warp; r < nrays; r += gridDim.x * wpb) {
+        int c = rec_count[r];
+        if (c <= lo) {
+            if (lane == 0 && lo == 0) nnz[r] = c;  // 0, kDropped or kOverflow
+            continue;
+        }
+        if (c > P) {
+            if (lane == 0 && lo == 0) nnz[r] = kOverflow;  // for the larger pass to overwrite
+            continue;
+        }
+        int n2 = 32;
+        while (n2 < c) n2 <<= 1;
+        const int64_t base = int64_t(r) * cap;
+        for (int q = lane; q < n2; q += 32)
+            keys[q] = q < c ? (static_cast<unsigned long long>(unsigned(rec_node[base + q])) << 32) | unsigned(q)
+                            : ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= n2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int q = lane; q < n2; q += 32) {
+                    int l = q ^ j;
+                    if (l > q) {
+                        unsigned long long x = keys[q], y = keys[l];
+                        bool up = (q & k) == 0;
+                        if ((x > y) == up) {
+                            keys[q] = y;
+                            keys[l] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // Segment starts, ranked by a running warp scan; each start sums its node in record order.
+        int written = 0;
+        for (int q0 = 0; q0 < c; q0 += 32) {
+            int q = q0 + lane;
+            bool start = false;
+            unsigned node = 0;
+            if (q < c) {
+                node = unsigned(keys[q] >> 32);
+                start = q == 0 || unsigned(keys[q - 1] >> 32) != node;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, start);
+            if (start) {
+                int rank = written + __popc(m & ((1u << lane) - 1u));
+                double sum = 0;
+                for (int e = q; e < c && unsigned(keys[e] >> 32) == node; e++) sum += rec_val[base + unsigned(keys[e])];
+                out_node[base + rank] = int(node);
+                out_len[base + rank] = float(sum);  // RayKernels.cs:97: (float)kernel[x]
+            }
+            written += __popc(m);
+        }
+        if (lane == 0) nnz[r] = written;
+        __syncwarp();
+    }
+}
+
+// Exclusive scan of the chunk's row sizes (negative = empty row) in one block; total and the
+// number of rows still marked for the large pass go to sums[0], sums[1].
+__global__ void scan_kernel(const int* __restrict__ nnz, int n, int* __restrict__ off, long long* __restrict__ sums) {
+    __shared__ long long part[1024];
+    __shared__ int over[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int per = (n + T - 1) / T;
+    const int b = t * per, e = min(n, b + per);
+    long long s = 0;
+    int ov = 0;
+    for (int q = b; q < e; q++) {
+        int v = nnz[q];
+        s += v > 0 ? v : 0;
+        ov += v == kOverflow;
+    }
+    part[t] = s;
+    over[t] = ov;
+    __syncthreads();
+    for (int d = 1; d < T; d <<= 1) {
+        long long x = t >= d ? part[t - d] : 0;
+        int y = t >= d ? over[t - d] : 0;
+        __syncthreads();
+        part[t] += x;
+        over[t] += y;
+        __syncthreads();
+    }
+    long long run = part[t] - s;
+    for (int q = b; q < e; q++) {
+        off[q] = int(run);
+        int v = nnz[q];
+        run += v > 0 ? v : 0;
+    }
+    if (t == T - 1) {
+        sums[0] = part[T - 1];
+        sums[1] = over[T - 1];
+    }
+}
+
+__global__ void emit_kernel(const int* __restrict__ out_node, const float* __restrict__ out_len,
+                            const int* __restrict__ nnz, const int* __restrict__ off, int cap, int nrays, int ray0,
+                            long long base, int* __restrict__ row_ptr, int* __restrict__ col, float* __restrict__ len,
+                            uint8_t* __restrict__ ok) {
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nrays; r += gridDim.x * wpb) {
+        int c = nnz[r];
+        long long o = base + off[r];
+        if (lane == 0) {
+            row_ptr[ray0 + r] = int(o);
+            ok[ray0 + r] = c >= 0 ? 1 : 0;
+        }
+        for (int q = lane; q < c; q += 32) {
+            col[o + q] = out_node[int64_t(r) * cap + q];
+            len[o + q] = out_len[int64_t(r) * cap + q];
+        }
+    }
+}
+
+RGrid make_rgrid(const host::Grid& g) {
+    RGrid r{};
+    r.nx = g.nx; r.ny = g.ny; r.nz = g.nz;
+    r.min_lon = g.min_lon; r.min_lat = g.min_lat; r.min_dep = g.min_dep;
+    r.dlon = g.dlon; r.dlat = g.dlat; r.ddep = g.ddep;
+    r.dlon_rad = g.dlon_rad; r.dlat_rad = g.dlat_rad;
+    r.centre_lon = g.centre_lon;
+    r.lon_last = g.lon[g.nx - 1]; r.lat_last = g.lat[g.ny - 1]; r.dep_last = g.dep[g.nz - 1];
+    r.min_spacing_km = g.min_spacing_km();
+    return r;
+}
+
+}  // namespace rays
+}  // namespace ts
+
+using namespace ts;
+using namespace ts::rays;
+
+struct ts_rows {
+    ts_ctx* ctx = nullptr;
+    int n_rows = 0;
+    int64_t nnz = 0;
+    int* row_ptr = nullptr;   // device, n_rows + 1
+    int* col = nullptr;       // device, nnz
+    float* len = nullptr;
+    double* tcg = nullptr;    // device, 4 per row
+    uint8_t* ok = nullptr;
+    ~ts_rows() {
+        cudaFree(row_ptr);
+        cudaFree(col);
+        cudaFree(len);
+        cudaFree(tcg);
+        cudaFree(ok);
+    }
+};
+
+namespace ts {
+namespace rays {
+
+int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
+                    const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st) {
+    cudaStream_t s = ctx->stream;
+    const int64_t n = fwd.count();
+    for (int a = 0; a < n_rays; a++)
+        if (table_of_host[a] < 0 || table_of_host[a] >= n_tables) return ctx->fail(TS_E_ARG, "table_of out of range");
+    if (!(step_km > 0)) return ctx->fail(TS_E_ARG, "step must be positive");
+    if (fwd.variable || inv.variable) return ctx->fail(TS_E_ARG, "rays need uniform grids");
+    auto rows = new ts_rows();
+    rows->ctx = ctx;
+    rows->n_rows = n_rays;
+    auto bail = [&](int code) {
+        delete rows;
+        return code;
+    };
+    if (cudaMalloc(&rows->row_ptr, sizeof(int) * (n_rays + 1)) != cudaSuccess ||
+        cudaMalloc(&rows->tcg, sizeof(double) * 4 * std::max(1, n_rays)) != cudaSuccess ||
+        cudaMalloc(&rows->ok, std::max(1, n_rays)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->fail(TS_E_NOMEM, "row buffers");
+        return bail(TS_E_NOMEM);
+    }
+    TS_BUF(ctx, d_station, double, "rays.station", 3 * std::max(1, n_tables));
+    TS_BUF(ctx, d_table_of, int, "rays.table_of", std::max(1, n_rays));
+    TS_BUF(ctx, d_events, double, "rays.events", 3 * std::max(1, n_rays));
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_station, table_station_host, sizeof(double) * 3 * n_tables, cudaMemcpyHostToDevice, s));
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_table_of, table_of_host, sizeof(int) * n_rays, cudaMemcpyHostToDevice, s));
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_events, events_host, sizeof(double) * 3 * n_rays, cudaMemcpyHostToDevice, s));
+
+    TraceArgs a{};
+    a.fwd = make_rgrid(fwd);
+    a.inv = make_rgrid(inv);
+    a.tables = tables_dev;
+    a.table_n = n;
+    a.table_station = d_station;
+    a.table_of = d_table_of;
+    a.events = d_events;
+    a.step_km = step_km;
+    a.piece_km = 0.5 * inv.min_spacing_km();  // RayTracing.cs:130
+    a.tcg = rows->tcg;
+
+    // Record capacity: one record per node per inversion cell crossed, with room for a path
+    // three times the straight length; a ray that needs more is traced again with more room.
+    const int CH = 16384;
+    int64_t csr_cap = 0;
+    int64_t total = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    for (int ray0 = 0; ray0 < n_rays; ray0 += CH) {
+        const int nr = std::min(CH, n_rays - ray0);
+        double maxd = 0;
+        for (int q = ray0; q < ray0 + nr; q++) {
+            const double* ev = events_host + 3 * q;
+            const double* stn = table_station_host + 3 * table_of_host[q];
+            host::V3 A = host::to_cartesian(ev[0], ev[1], ev[2]);
+            host::V3 B = host::to_cartesian(stn[0], stn[1], stn[2]);
+            maxd = std::max(maxd, host::dist(A, B));
+        }
+        constexpr int kMaxCap = 16384;  // the larger merge pass sorts up to this many in 128 KB
+        int cap = int(std::min(double(kMaxCap), 8.0 * (3.0 * maxd / a.piece_km + 32)));
+        for (int attempt = 0;; attempt++) {
+            a.ray0 = ray0;
+            a.nrays = nr;
+            a.cap = cap;
+            TS_BUF(ctx, rec_node, int, "rays.rec_node", size_t(nr) * cap);
+            TS_BUF(ctx, rec_val, double, "rays.rec_val", size_t(nr) * cap);
+            TS_BUF(ctx, rec_count, int, "rays.rec_count", nr);
+            TS_BUF(ctx, out_node, int, "rays.out_node", size_t(nr) * cap);
+            TS_BUF(ctx, out_len, float, "rays.out_len", size_t(nr) * cap);
+            TS_BUF(ctx, nnz, int, "rays.nnz", nr);
+            TS_BUF(ctx, off, int, "rays.off", nr);
+            TS_BUF(ctx, sums, long long, "rays.sums", 2);
+            a.rec_node = rec_node;
+            a.rec_val = rec_val;
+            a.rec_count = rec_count;
+            trace_kernel<<<(nr + 127) / 128, 128, 0, s>>>(a);
+            TS_CUDA_TRY(ctx, cudaGetLastError());
+            // Small sort size for most rays; the rest in a second pass with one warp per block.
+            const int Psmall = 2048, W = 4;
+            int Pbig = Psmall;
+            while (Pbig < cap) Pbig <<= 1;
+            TS_CUDA_TRY(ctx, cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  std::max(W * Psmall, Pbig) * 8));
+            merge_kernel<<<std::min((nr + W - 1) / W, ctx->sm_count * 8), W * 32, size_t(W) * Psmall * 8, s>>>(
+                rec_node, rec_val, rec_count, cap, nr, Psmall, 0, out_node, out_len, nnz);
+            TS_CUDA_TRY(ctx, cudaGetLastError());
+            if (Pbig > Psmall) {
+                merge_kernel<<<std::min(nr, ctx->sm_count * 2), 32, size_t(Pbig) * 8, s>>>(
+                    rec_node, rec_val, rec_count, cap, nr, Pbig, Psmall, out_node, out_len, nnz);
+                TS_CUDA_TRY(ctx, cudaGetLastError());
+            }
+            scan_kernel<<<1, 1024, 0, s>>>(nnz, nr, off, sums);
+            long long h_sums[2] = {0, 0};
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(h_sums, sums, sizeof h_sums, cudaMemcpyDeviceToHost, s));
+            TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+            if (h_sums[1] > 0) {
+                if (cap >= kMaxCap) return bail(ctx->fail(TS_E_CAPACITY, "a ray needs more records than supported"));
+                cap = std::min(kMaxCap, cap * 4);
+                if (st) st->retraced_chunks++;
+                continue;
+            }
+            if (total + h_sums[0] > INT32_MAX) return bail(ctx->fail(TS_E_CAPACITY, "more than 2^31 non-zeros"));
+            if (total + h_sums[0] > csr_cap) {
+                int64_t want = std::max<int64_t>(total + h_sums[0], csr_cap * 2);
+                want = std::max<int64_t>(want, 1024);
+                int* ncol = nullptr;
+                float* nlen = nullptr;
+                if (cudaMalloc(&ncol, sizeof(int) * want) != cudaSuccess ||
+                    cudaMalloc(&nlen, sizeof(float) * want) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaFree(ncol);
+                    return bail(ctx->fail(TS_E_NOMEM, "CSR arrays"));
+                }
+                if (total > 0) {
+                    cudaMemcpyAsync(ncol, rows->col, sizeof(int) * total, cudaMemcpyDeviceToDevice, s);
+                    cudaMemcpyAsync(nlen, rows->len, sizeof(float) * total, cudaMemcpyDeviceToDevice, s);
+                    cudaStreamSynchronize(s);
+                }
+                cudaFree(rows->col);
+                cudaFree(rows->len);
+                rows->col = ncol;
+                rows->len = nlen;
+                csr_cap = want;
+            }
+            emit_kernel<<<std::min((nr + 7) / 8, ctx->sm_count * 16), 256, 0, s>>>(
+                out_node, out_len, nnz, off, cap, nr, ray0, total, rows->row_ptr, rows->col, rows->len, rows->ok);
+            TS_CUDA_TRY(ctx, cudaGetLastError());
+            total += h_sums[0];
+            break;
+        }
+    }
+    int tot32 = int(total);
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(rows->row_ptr + n_rays, &tot32, sizeof(int), cudaMemcpyHostToDevice, s));
+    cudaEventRecord(e1, s);
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rows->nnz = total;
+    if (st) st->device_ms += ms;
+    *out = rows;
+    return TS_OK;
+}
+
+}  // namespace rays
+}  // namespace ts
+
+extern "C" {
+
+int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float* tables, const double* table_station,
+                  const ts_grid* inv, int32_t n_rays, const int32_t* table_of, const double* events, double step_km,
+                  ts_rows** out) {
+    if (!ctx || !out) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    *out = nullptr;
+    if (!fwd || !inv || host::Grid::validate(*fwd) || host::Grid::validate(*inv))
+        return ctx->fail(TS_E_ARG, "invalid grid");
+    if (n_tables <= 0 || n_rays < 0 || !tables || !table_station || (n_rays > 0 && (!table_of || !events)))
+        return ctx->fail(TS_E_ARG, "null array or empty table set");
+    host::Grid gf(*fwd), gi(*inv);
+    const size_t bytes = sizeof(float) * size_t(n_tables) * size_t(gf.count());
+    float* d_tables = static_cast<float*>(ctx->buf("rays.tables", bytes));
+    if (!d_tables) return TS_E_NOMEM;
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_tables, tables, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return ts::rays::trace_on_device(ctx, gf, d_tables, n_tables, table_station, gi, n_rays, table_of, events, step_km,
+                                     out, nullptr);
+}
+
+int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz) {
+    if (!rows) return TS_E_ARG;
+    if (n_rows) *n_rows = rows->n_rows;
+    if (nnz) *nnz = rows->nnz;
+    return TS_OK;
+}
+
+int ts_rows_copy(ts_rows* rows, int32_t* row_ptr, int32_t* col, float* len, double* tcalc_grad, uint8_t* ok) {
+    if (!rows) return TS_E_ARG;
+    ts_ctx* ctx = rows->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int n = rows->n_rows;
+    if (row_ptr) TS_CUDA_TRY(ctx, cudaMemcpyAsync(row_ptr, rows->row_ptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    if (col && rows->nnz) TS_CUDA_TRY(ctx, cudaMemcpyAsync(col, rows->col, sizeof(int) * rows->nnz, cudaMemcpyDeviceToHost, s));
+    if (len && rows->nnz) TS_CUDA_TRY(ctx, cudaMemcpyAsync(len, rows->len, sizeof(float) * rows->nnz, cudaMemcpyDeviceToHost, s));
+    if (tcalc_grad && n) TS_CUDA_TRY(ctx, cudaMemcpyAsync(tcalc_grad, rows->tcg, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+    if (ok && n) TS_CUDA_TRY(ctx, cudaMemcpyAsync(ok, rows->ok, size_t(n), cudaMemcpyDeviceToHost, s));
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return TS_OK;
+}
+
+void ts_rows_free(ts_rows* rows) {
+    if (!rows) return;
+    {
+        std::lock_guard<std::recursive_mutex> lk(rows->ctx->mu);
+        cudaSetDevice(rows->ctx->device);
+    }
+    delete rows;
+}
+
+}  // extern "C"

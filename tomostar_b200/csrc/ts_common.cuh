@@ -33,4 +33,21 @@ TS_DEVINL double ld_cg(const double* p) { return __ldcg(p); }
 TS_DEVINL void st_cg(float* p, float v) { __stcg(p, v); }
 TS_DEVINL void st_cg(double* p, double v) { __stcg(p, v); }
 
+// Asynchronous global → shared copies (LDGSTS): a warp issues every copy of a tile before it
+// waits once, instead of one round trip per loop iteration. The 16-byte .cg form bypasses L1, so it
+// never serves a line another SM has rewritten since; the 4/8-byte .ca form is for read-only data.
+TS_DEVINL void cp_async16_cg(void* smem, const void* gmem) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+TS_DEVINL void cp_async_ro(float* smem, const float* gmem) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+TS_DEVINL void cp_async_ro(double* smem, const double* gmem) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+TS_DEVINL void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 }  // namespace ts
