@@ -1,0 +1,345 @@
+"""Benchmark of the forward engine: travel-time fields/s on the large regional forward step
+(401×401×121 nodes at 0.25 km, 400 stations × P and S = 800 fields), FP64 sweeping, float32 tables.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = every field of the job solved once by the batched engine (two launches: the P and the
+S fields). `value` is fields/s with the velocity model resident in HBM and the fields left on the
+device; `e2e` is the same job through the C-ABI entry point a host calls (ts_eik_solve: slowness and
+seeds from host memory, float32 tables read back into pinned host memory). Under torchrun every rank
+solves its own job of 800 fields (different stations; weak scaling, no collective on the data path);
+rank 0 prints one JSON line with the max-over-ranks time. `--impl reference` times the reference's
+CPU solver (fast marching, restated in oracle/) on the host cores on a bounded sample of the job.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "travel-time fields/s (FP64 sweeping, float32 tables, err vs FP64 oracle 0)"
+UNIT = "fields/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.out), exist_ok=True)
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.out):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def setup_dist(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    return world, rank, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, local, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_fmm_sample(problem, n_fields: int, threads: int):
+    """The reference's CPU path (SphericalEikonal.Solve, one field per thread as TravelTimeTableSet
+    does) on n_fields fields of the job; returns (fields/s, seconds)."""
+    from oracle import oracle as O
+
+    og = O.Grid.of(problem.grid)
+    seeds, sl_of = [], []
+    for q in range(n_fields):
+        st, ph = q // 2, q % 2
+        seeds.append(O.point_source(og, problem.slowness[ph], *problem.stations[st]))
+        sl_of.append(ph)
+    t0 = time.perf_counter()
+    O.fmm_many(og, problem.slowness, np.array(sl_of, np.int32), seeds, threads=threads)
+    dt = time.perf_counter() - t0
+    return n_fields / dt, dt
+
+
+def run_reference(args, problem_fn):
+    world, rank, local, dist = setup_dist(args)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    p = problem_fn(0)
+    n = threads  # one field per host thread: ~one fast-marching solve of time per step
+    rates = []
+    for step in range(args.warmup + args.steps):
+        r, dt = cpu_fmm_sample(p, n, threads)
+        if step >= args.warmup:
+            rates.append(r)
+    v = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "config4: 401x401x121 at 0.25 km, 800 P+S fields (400 stations)",
+                   "sample": f"{n} fields per step"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} of 800 fields per step, fast marching (oracle/oracle.cpp or_fmm_many)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, problem_fn):
+    world, rank, local, dist = setup_dist(args)
+    from tomostar_b200 import _lib as L
+    from tomostar_b200.eikonal import EikonalCuda, pack_seeds, point_source
+
+    lib = L.load()
+    p = problem_fn(rank)
+    g = p.grid
+    n = g.count
+    n_st = len(p.stations)
+    solver = EikonalCuda.create(local, 64)
+    rel, msg = solver.self_test()
+    if not (rel <= 1e-6):
+        raise SystemExit(f"self-test failed: {msg}")
+    lib.ts_engine_set_tile(solver.handle, 64, args.tile)
+    # Seeds of every (station, phase) field, on the host before timing (PointSource, C ABI).
+    seeds = {ph: [point_source(g, p.slowness[ph], *p.stations[q]) for q in range(n_st)] for ph in (0, 1)}
+    packed = {ph: pack_seeds(seeds[ph]) for ph in (0, 1)}
+    gs = g.struct()
+    mid = C.c_int32()
+    s_all = np.ascontiguousarray(p.slowness)
+    rc = lib.ts_model_put(solver.handle, C.byref(gs), s_all.ctypes.data_as(C.POINTER(C.c_double)), 2, 64,
+                          C.byref(mid))
+    if rc:
+        raise SystemExit(f"model upload failed: {solver.last_error}")
+    P = C.POINTER
+    stats = L.EikStats()
+
+    def step_resident():
+        dev_ms = kern_ms = 0.0
+        upd = 0
+        for ph in (0, 1):
+            off, idx, t = packed[ph]
+            rc = lib.ts_eik_solve_model(solver.handle, mid.value, ph, n_st, off.ctypes.data_as(P(C.c_int32)),
+                                        idx.ctypes.data_as(P(C.c_int32)), t.ctypes.data_as(P(C.c_double)),
+                                        L.MODE_ENGINE, 1e-7, 0, None, L.OUT_NONE, C.byref(stats))
+            if rc:
+                raise SystemExit(f"solve failed: {solver.last_error}")
+            dev_ms += stats.device_ms
+            kern_ms += stats.kernel_ms
+            upd += stats.node_updates
+        return dev_ms, kern_ms, upd, (stats.rounds[0], stats.rounds[1])
+
+    for _ in range(args.warmup):
+        step_resident()
+    barrier(dist)
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev = kern = 0.0
+    updates = 0
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        d, k, u, rounds = step_resident()
+        dev += d
+        kern += k
+        updates += u
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    barrier(dist)
+    dev_max = max_over_ranks(dist, local, dev)
+    fields_total = 2 * n_st * world * args.steps
+    value = fields_total / (dev_max / 1e3)
+
+    # Roofline of the sweeping kernel: algorithmic bytes per node update (FP64: the node's time read
+    # and written, its slowness read = 24 B) over the kernel's event time.
+    peak, peak_kind = measured_hbm_peak()
+    launches = 2 * args.steps
+    achieved = updates * 24 / (kern / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "engine_traffic.json")
+    if os.path.exists(prof):
+        try:
+            bpu = json.load(open(prof))["dram_bytes_per_node_update_f64"]
+            traffic = bpu * updates / launches
+        except Exception:
+            traffic = None
+
+    # End to end through ts_eik_solve: host slowness and seeds in, float32 tables out to pinned memory.
+    e2e = None
+    if not args.no_e2e:
+        import torch
+
+        out = torch.empty((n_st, n), dtype=torch.float32, pin_memory=True)
+        out_np = out.numpy()
+        s_pin = [torch.from_numpy(np.ascontiguousarray(p.slowness[ph])).pin_memory() for ph in (0, 1)]
+        h2d = d2h = 0
+
+        def step_e2e():
+            nonlocal h2d, d2h
+            for ph in (0, 1):
+                off, idx, t = packed[ph]
+                rc = lib.ts_eik_solve(solver.handle, C.byref(gs), C.cast(s_pin[ph].data_ptr(), P(C.c_double)), n_st,
+                                      off.ctypes.data_as(P(C.c_int32)), idx.ctypes.data_as(P(C.c_int32)),
+                                      t.ctypes.data_as(P(C.c_double)), 64, L.MODE_ENGINE, 1e-7, 0,
+                                      out_np.ctypes.data_as(C.c_void_p), L.OUT_F32, C.byref(stats))
+                if rc:
+                    raise SystemExit(f"e2e solve failed: {solver.last_error}")
+                h2d += n * 8 + off.nbytes + idx.nbytes + t.nbytes
+                d2h += n_st * n * 4
+
+        step_e2e()  # warm-up (allocations)
+        h2d = d2h = 0
+        barrier(dist)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            step_e2e()
+        e2e_s = max_over_ranks(dist, local, time.perf_counter() - t0)
+        e2e = {"value": 2 * n_st * world * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
+               "steps": args.e2e_steps}
+
+    # Baselines on rank 0: the plain per-plane GPU path on one field, the CPU solver on a sample.
+    plain = cpu = None
+    if rank == 0 and not args.no_baselines:
+        off, idx, t = pack_seeds(seeds[0][:1])
+        rc = lib.ts_eik_solve_model(solver.handle, mid.value, 0, 1, off.ctypes.data_as(P(C.c_int32)),
+                                    idx.ctypes.data_as(P(C.c_int32)), t.ctypes.data_as(P(C.c_double)), L.MODE_PLAIN,
+                                    1e-7, 0, None, L.OUT_NONE, C.byref(stats))
+        if rc == 0:
+            plain = {"value": 1e3 / stats.device_ms, "unit": UNIT, "sample": "1 P field, one launch per plane",
+                     "launches": int(stats.launches)}
+        threads = os.cpu_count() or 1
+        r, dt = cpu_fmm_sample(p, threads, threads)
+        cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{threads} of 800 fields, fast marching one field per thread (oracle/oracle.cpp)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config4: 401x401x121 nodes at 0.25 km (19.46 M), 400 surface stations x P,S "
+                                   "= 800 fields per GPU, Vp 1-D gradient + 3 ellipsoids +-8 % (seed 5)",
+                       "global_fields": 2 * n_st * world, "tile": args.tile,
+                       "l2": "inputs larger than L2 (fields 2 x 65 GB per step)",
+                       "rounds_last": list(rounds)},
+            "gpu_launches": 3 * launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "engine_kernel (FP64), 24 B per node update"},
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "plain_gpu": plain,
+            "node_updates_per_step": updates // args.steps,
+            "wall_s_timed": t_wall,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tile", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-baselines", action="store_true")
+    args = ap.parse_args()
+    from tomostar_b200 import synthetic as syn
+
+    def problem(rank):
+        return syn.config4(seed=5 + rank)
+
+    if args.impl == "reference":
+        return run_reference(args, problem)
+    return run_ours(args, problem)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -63,7 +63,8 @@ typedef struct ts_eik_stats {
     int32_t reserved;
     int64_t node_updates;   /* node evaluations performed (one per node per tile or plane visit) */
     int64_t tile_visits;    /* tiles processed (engine) or planes launched (plain) */
-    double device_ms;       /* CUDA-event time of the solve on the device */
+    double device_ms;       /* CUDA-event time of the solve on the device (set-up kernels included) */
+    double kernel_ms;       /* CUDA-event time of the sweeping kernel launches alone */
 } ts_eik_stats;
 
 /* ---- context (EikonalOpenCl.TryCreate / Dispose / Device) ----------------------------------- */

@@ -47,6 +47,7 @@ class EikStats(C.Structure):
     _fields_ = [
         ("rounds", C.c_int32 * 2), ("launches", C.c_int32), ("reserved", C.c_int32),
         ("node_updates", C.c_int64), ("tile_visits", C.c_int64), ("device_ms", C.c_double),
+        ("kernel_ms", C.c_double),
     ]
 
 

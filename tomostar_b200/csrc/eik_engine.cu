@@ -316,12 +316,27 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     if (per_sm < 1) return ctx->fail(TS_E_CUDA, "engine kernel does not fit on an SM");
     int blocks = per_sm * ctx->sm_count;
     void* params[] = {&args};
-    TS_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s));
+    cudaEvent_t k0, k1;
+    cudaEventCreate(&k0);
+    cudaEventCreate(&k1);
+    cudaEventRecord(k0, s);
+    cudaError_t le = cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s);
+    cudaEventRecord(k1, s);
+    if (le != cudaSuccess) {
+        cudaEventDestroy(k0);
+        cudaEventDestroy(k1);
+        TS_CUDA_TRY(ctx, le);
+    }
     Control ctl{};
     std::vector<FieldState> st(nf);
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(&ctl, D + o_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(st.data(), D + o_state, sizeof(FieldState) * nf, cudaMemcpyDeviceToHost, s));
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    float kms = 0;
+    cudaEventElapsedTime(&kms, k0, k1);
+    cudaEventDestroy(k0);
+    cudaEventDestroy(k1);
+    if (stats) stats->kernel_ms += kms;
     for (int f = 0; f < nf; f++) {
         job.fields[f].status = st[f].status;
         job.fields[f].rounds[0] = st[f].rounds0;

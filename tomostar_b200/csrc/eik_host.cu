@@ -87,12 +87,19 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
     TS_CUDA_TRY(ctx, cudaGetLastError());
     const int planes = nx + ny + nz - 2;
     int launches = 0;
+    struct Ev {  // events bracketing each round's plane launches
+        cudaEvent_t e;
+        Ev() { cudaEventCreate(&e); }
+        ~Ev() { cudaEventDestroy(e); }
+    } ev0, ev1;
+    cudaEvent_t k0 = ev0.e, k1 = ev1.e;
     for (int phase = 0; phase < 2; phase++) {
         fill_u8_kernel<<<fill_blocks(n), 256, 0, s>>>(dirty, 1, n);
         bool settled = false;
         for (int round = 0; round < cap && !settled; round++) {
             if (ctx->cancel_host && *ctx->cancel_host) return ctx->fail(TS_E_CANCELLED, "cancelled");
             TS_CUDA_TRY(ctx, cudaMemsetAsync(changed, 0, sizeof(int), s));
+            cudaEventRecord(k0, s);
             for (int dir = 0; dir < 8; dir++) {
                 for (int p = 0; p < planes; p++) {
                     int i0 = std::max(0, p - (ny - 1) - (nz - 1)), i1 = std::min(nx - 1, p);
@@ -109,10 +116,14 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
                     launches++;
                 }
             }
+            cudaEventRecord(k1, s);
             TS_CUDA_TRY(ctx, cudaGetLastError());
             int ch = 0;
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(&ch, changed, sizeof(int), cudaMemcpyDeviceToHost, s));
             TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+            float kms = 0;
+            cudaEventElapsedTime(&kms, k0, k1);
+            if (stats) stats->kernel_ms += kms;
             rounds_out[phase] = round + 1;
             settled = ch == 0;
         }

@@ -126,3 +126,53 @@ def selftest_case():
     j = np.arange(g.ny)[None, :, None]
     s = 1 / (5.8 + 0.02 * dep[:, None, None] + 0.2 * np.sin(0.7 * i) + 0.15 * np.cos(0.5 * j))
     return g, s.reshape(-1), (10.37, 42.61, 8.3)
+
+
+def ellipsoid_bodies(grid: GridDef, h_km: float, rng, n: int = 3, amplitude: float = 0.08) -> np.ndarray:
+    """Fractional perturbation of n ellipsoidal bodies with smooth edges (the super-Gaussian edge of
+    the reference's TabularBody, ResolutionTests.cs:39-40: 1 inside, 1/2 at the nominal surface).
+    Amplitudes alternate +amplitude, −amplitude, …; centres and semi-axes are drawn from rng."""
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    x = np.arange(nx) * h_km
+    y = np.arange(ny) * h_km
+    z = grid.depth()
+    span_x, span_y, span_z = x[-1], y[-1], z[-1]
+    out = np.zeros((nz, ny, nx))
+    for b in range(n):
+        cx, cy = rng.uniform(0.2, 0.8) * span_x, rng.uniform(0.2, 0.8) * span_y
+        cz = rng.uniform(0.2, 0.8) * span_z
+        ax, ay = rng.uniform(0.08, 0.2) * span_x, rng.uniform(0.08, 0.2) * span_y
+        az = rng.uniform(0.1, 0.3) * span_z
+        amp = amplitude if b % 2 == 0 else -amplitude
+        r2 = (((z - cz) / az) ** 2)[:, None, None] + (((y - cy) / ay) ** 2)[None, :, None] + \
+            (((x - cx) / ax) ** 2)[None, None, :]
+        out += amp * np.exp(-np.log(2) * r2 ** 3)
+    return out.reshape(-1)
+
+
+def config4(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000, seed: int = 5) -> Problem:
+    """401×401×121 at 0.25 km (19.46 M nodes): Vp = 5 + 0.04 z km/s plus three ellipsoidal ±8 % bodies,
+    Vs = Vp / 1.73; 400 surface stations and 5,000 events (2–25 km deep) → 800 P and S fields;
+    1.5 M (event, station, phase) arrivals drawn uniformly without replacement. One generator,
+    seed 5, in that order."""
+    h = 0.25
+    g = regular_grid(401, 401, 121, h)
+    rng = np.random.default_rng(seed)
+    vp = vp_linear(g, 5.0, 0.04) * (1 + ellipsoid_bodies(g, h, rng))
+    vs = vp / 1.73
+    span = 400 * h
+    sxy = rng.uniform(0, span, size=(n_stations, 2))
+    slon, slat = km_to_geo(g, sxy[:, 0], sxy[:, 1], h)
+    stations = np.stack([slon, slat, np.zeros(n_stations)], axis=1)
+    exyz = np.column_stack([rng.uniform(0, span, n_events), rng.uniform(0, span, n_events),
+                            rng.uniform(2, 25, n_events)])
+    elon, elat = km_to_geo(g, exyz[:, 0], exyz[:, 1], h)
+    events = np.stack([elon, elat, exyz[:, 2]], axis=1)
+    pick = rng.choice(n_events * n_stations * 2, size=min(n_rays, n_events * n_stations * 2), replace=False)
+    ev, rest = np.divmod(pick, n_stations * 2)
+    st, ph = np.divmod(rest, 2)
+    arrivals = np.stack([ev, st, ph], axis=1).astype(np.int32)
+    slow = np.empty((2, g.count))
+    np.divide(1.0, vp, out=slow[0])
+    np.divide(1.0, vs, out=slow[1])
+    return Problem("config4", g, g.coarsened(2), slow, stations, events, arrivals, h)
