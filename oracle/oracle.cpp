@@ -880,3 +880,74 @@ void or_relax_many(const or_grid_def* d, const double* slowness, const int32_t* 
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// The reference's sweeping with node-level due flags (EikonalOpenCl.cs:528-532, 608-622), where a
+// node wakes its 12 stencil neighbours only when it dropped by more than wake_rel of its new value
+// (wake_rel = 0: every drop wakes, the reference's rule, identical to or_relax). Used to bound the
+// effect of not propagating last-digit changes. evals_out receives the node evaluations made.
+int32_t or_relax_wake(const or_grid_def* d, const double* slowness, int32_t n_seeds, const int32_t* seed_idx,
+                      const double* seed_t, double tol, double wake_rel, double* out, int32_t* rounds_out,
+                      int64_t* evals_out) {
+    Grid g(*d);
+    Metric m(g);
+    int n = g.count();
+    std::fill(out, out + n, kInf);
+    std::vector<uint8_t> fixed(n, 0), due(n, 1);
+    for (int q = 0; q < n_seeds; q++) {
+        int s = seed_idx[q];
+        if (unsigned(s) >= unsigned(n)) continue;
+        out[s] = std::min(out[s], seed_t[q]);
+        fixed[s] = 1;
+    }
+    int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+    int cap = sweep_round_cap(g);
+    int64_t evals = 0;
+    int settled_all = 1;
+    for (int phase = 0; phase < 2; phase++) {
+        std::fill(due.begin(), due.end(), 1);
+        int settled = 0, round = 0;
+        for (round = 0; round < cap; round++) {
+            bool changed = false;
+            for (int dir = 0; dir < 8; dir++)
+                for (int p = 0; p < nx + ny + nz - 2; p++) {
+                    int i0, i1, k0, k1;
+                    plane_bounds(nx, ny, nz, p, i0, i1, k0, k1);
+                    for (int kp = k0; kp <= k1; kp++)
+                        for (int ip = i0; ip <= i1; ip++) {
+                            int jp = p - ip - kp;
+                            if (jp < 0 || jp >= ny) continue;
+                            int i = (dir & 1) ? nx - 1 - ip : ip;
+                            int j = (dir & 2) ? ny - 1 - jp : jp;
+                            int k = (dir & 4) ? nz - 1 - kp : kp;
+                            int idx = g.index(i, j, k);
+                            if (fixed[idx] || !due[idx]) continue;
+                            due[idx] = 0;
+                            evals++;
+                            double cur = out[idx];
+                            double cand = relax_node(m, slowness, out, idx, i, j, k, phase == 1);
+                            if (!(cand < cur)) continue;
+                            out[idx] = cand;
+                            if (!std::isfinite(cur) || cur - cand > tol) changed = true;
+                            if (std::isfinite(cur) && cur - cand <= wake_rel * cand) continue;
+                            for (int s = 1; s <= 2; s++) {
+                                if (i >= s) due[idx - s] = 1;
+                                if (i + s < nx) due[idx + s] = 1;
+                                if (j >= s) due[idx - s * nx] = 1;
+                                if (j + s < ny) due[idx + s * nx] = 1;
+                                if (k >= s) due[idx - s * nxy] = 1;
+                                if (k + s < nz) due[idx + s * nxy] = 1;
+                            }
+                        }
+                }
+            if (!changed) { settled = 1; round++; break; }
+        }
+        if (rounds_out) rounds_out[phase] = round;
+        if (!settled) settled_all = 0;
+    }
+    if (evals_out) *evals_out = evals;
+    return settled_all;
+}
+
+}  // extern "C"

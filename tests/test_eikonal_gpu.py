@@ -231,3 +231,46 @@ def test_suggest_batch(solver):
     n = 401 * 401 * 121
     b32 = solver.suggest_batch(n)
     assert 100 < b32 <= 1024
+
+
+WAKE = 1e-13
+
+
+@pytest.mark.parametrize("shape", [(23, 19, 13), (33, 17, 21), (40, 40, 20)])
+def test_fast_mode_equals_wake_oracle(solver, shape):
+    """TS_MODE_FAST is the reference scheme with the wake threshold: equal to the oracle's
+    relax_wake to the bit, and within 1e-10 relative of the reference (Relax)."""
+    g, s, seeds = hetero_case(*shape, seed=3 * sum(shape))
+    og = O.Grid.of(g)
+    out = solver.solve(g, s, seeds, precision=64, mode=L.MODE_FAST)
+    for f, (si, st) in enumerate(seeds):
+        w, ok, _, _ = O.relax_wake(og, s, si, st, WAKE)
+        ref = O.relax(og, s, si, st)[0]
+        assert ok and np.array_equal(out[f], w)
+        assert rel_err(out[f], ref) <= 1e-10
+
+
+def test_fast_mode_config1_within_1e10(solver):
+    p = syn.config1()
+    for ph in (0, 1):
+        seeds = [point_source(p.grid, p.slowness[ph], *p.stations[q]) for q in (2, 13)]
+        ref = oracle_fields(p.grid, p.slowness[ph], seeds)
+        out = solver.solve(p.grid, p.slowness[ph], seeds, precision=64, mode=L.MODE_FAST)
+        for f in range(2):
+            assert rel_err(out[f], ref[f]) <= 1e-10
+
+
+def test_fast_mode_all_tile_shapes(solver):
+    g, s, seeds = hetero_case(37, 29, 19, seed=12, nsrc=3)
+    lib = L.load()
+    buf = (C.c_int32 * 64)()
+    n = lib.ts_engine_shapes(buf, 16)
+    og = O.Grid.of(g)
+    want = np.stack([O.relax_wake(og, s, si, st, WAKE)[0] for si, st in seeds])
+    try:
+        for q in range(n):
+            assert lib.ts_engine_set_tile(solver.handle, 64, buf[4 * q]) == 0
+            out = solver.solve(g, s, seeds, precision=64, mode=L.MODE_FAST)
+            assert np.array_equal(out, want)
+    finally:
+        lib.ts_engine_set_tile(solver.handle, 64, 0)

@@ -145,3 +145,27 @@ def test_variable_spacing_uniform_limit():
     assert ok and ok2
     fin = np.isfinite(a)
     assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(a[fin], 1e-9)) < 1e-3
+
+
+def test_relax_wake_zero_is_relax():
+    """Node-level due flags with every drop waking (the reference's rule) reproduce Relax to the bit."""
+    g = O.Grid(10, 11, 42, 43, 0, 30, 19, 17, 11)
+    rng = np.random.default_rng(17)
+    s = 1 / (5 + rng.uniform(-0.5, 0.5, g.count))
+    si, st = O.point_source(g, s, 10.4, 42.3, 7)
+    a, ok, r, _ = O.relax_wake(g, s, si, st, 0.0)
+    b, ok2, r2 = O.relax(g, s, si, st)
+    assert ok and ok2 and np.array_equal(a, b) and list(r) == list(r2)
+
+
+def test_relax_wake_threshold_bound():
+    """Not propagating drops below 1e-13 of the time keeps fields within 1e-10 relative of Relax."""
+    g = O.Grid(10, 11, 42, 43, 0, 30, 31, 29, 17)
+    rng = np.random.default_rng(19)
+    s = (1 / (5 + 0.04 * np.repeat(np.linspace(0, 30, 17), 31 * 29))) * (1 + 0.05 * rng.standard_normal(g.count))
+    si, st = O.point_source(g, s, 10.4, 42.3, 3)
+    a, ok, _, ev_fast = O.relax_wake(g, s, si, st, 1e-13)
+    b, ok2, _, ev_exact = O.relax_wake(g, s, si, st, 0.0)
+    fin = np.isfinite(b)
+    assert ok and ok2 and np.array_equal(fin, np.isfinite(a))
+    assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(b[fin], 1e-9)) < 1e-10

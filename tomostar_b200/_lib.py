@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "libtomostar_cuda.so")
 TS_OK, TS_E_ARG, TS_E_CUDA, TS_E_NOMEM, TS_E_UNSETTLED, TS_E_CANCELLED = 0, 1, 2, 3, 4, 5
 TS_E_TIMEOUT, TS_E_CAPACITY, TS_E_NOSEEDS, TS_E_SELFTEST, TS_E_NODEVICE = 6, 7, 8, 9, 10
 F64, F32 = 64, 32
-MODE_ENGINE, MODE_PLAIN = 0, 1
+MODE_ENGINE, MODE_PLAIN, MODE_FAST = 0, 1, 2
+WAKE_REL = 1e-13
 OUT_F64, OUT_F32, OUT_NONE = 0, 1, 2
 
 ERROR_NAMES = {

@@ -153,7 +153,7 @@ int ts_eik_solve(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32
     if (rc) return rc;
     if (!slowness || !seed_offsets || n_fields <= 0 || !out) return ctx->fail(TS_E_ARG, "null array or no fields");
     if (seed_offsets[n_fields] > 0 && (!seed_index || !seed_time)) return ctx->fail(TS_E_ARG, "null seed arrays");
-    if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN) return ctx->fail(TS_E_ARG, "unknown mode");
+    if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN && mode != TS_MODE_FAST) return ctx->fail(TS_E_ARG, "unknown mode");
     if (out_type != TS_OUT_F64 && out_type != TS_OUT_F32) return ctx->fail(TS_E_ARG, "unknown output type");
     if (!(tol >= 0)) return ctx->fail(TS_E_ARG, "tolerance must be >= 0");
     ts::eik::SolveIn in{};
@@ -200,7 +200,7 @@ int ts_eik_solve_model(ts_ctx* ctx, int32_t model_id, int32_t phase, int32_t n_f
     if (it == ctx->models.end()) return ctx->fail(TS_E_ARG, "unknown model");
     if (!seed_offsets || n_fields <= 0) return ctx->fail(TS_E_ARG, "no fields");
     if (seed_offsets[n_fields] > 0 && (!seed_index || !seed_time)) return ctx->fail(TS_E_ARG, "null seed arrays");
-    if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN) return ctx->fail(TS_E_ARG, "unknown mode");
+    if (mode != TS_MODE_ENGINE && mode != TS_MODE_PLAIN && mode != TS_MODE_FAST) return ctx->fail(TS_E_ARG, "unknown mode");
     if (out_type != TS_OUT_F64 && out_type != TS_OUT_F32 && out_type != TS_OUT_NONE)
         return ctx->fail(TS_E_ARG, "unknown output type");
     if (out_type != TS_OUT_NONE && !out) return ctx->fail(TS_E_ARG, "null output");

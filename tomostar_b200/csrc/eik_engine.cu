@@ -12,7 +12,7 @@ namespace ts {
 namespace eik {
 
 const std::vector<TileShapeInfo>& tile_shapes() {
-    static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}};
+    static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4}};
     return shapes;
 }
 
@@ -32,7 +32,7 @@ struct Arena {
 
 template <typename Real>
 __global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const GridDesc* __restrict__ grids,
-                                   uint8_t* __restrict__ dirty_base, const int64_t* __restrict__ dirty_off) {
+                                   uint8_t* __restrict__ dirty_base, const int64_t* __restrict__ dirty_off, int mw) {
     const FieldDesc<Real>& fd = fields[blockIdx.y];
     const GridDesc& g = grids[fd.grid];
     int64_t n = int64_t(g.pitch) * g.ny * g.nz;  // the pads too: they must read as +inf
@@ -43,6 +43,8 @@ __global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, c
     uint8_t* d = dirty_base + dirty_off[blockIdx.y];
     for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nt; q += int64_t(gridDim.x) * blockDim.x)
         d[q] = 1;
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nt * mw; q += int64_t(gridDim.x) * blockDim.x)
+        fd.dmask[q] = 0xffffffffu;  // every node due at the start (EikonalOpenCl.cs:411)
 }
 
 template <typename Real>
@@ -70,7 +72,7 @@ __global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_s
     }
 }
 
-template <typename Real, int BX, int BY, int BZ, int WARPS>
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB>
 int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     using S = Shape<Real, BX, BY, BZ>;
     const int nf = int(job.fields.size());
@@ -173,6 +175,22 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
             for (int j = 0; j < BY; j++)
                 for (int i = 0; i < BX; i++) pt[pos[i + j + k]++] = uint16_t(i | (j << 5) | (k << 10));
     }
+    // Wake masks: for each stencil offset, the tile nodes a changed node at that offset reaches
+    // without leaving its row, column or plane.
+    size_t o_wake = A.add(sizeof(uint32_t) * 12 * S::MW);
+    {
+        uint32_t* wm = A.at<uint32_t>(o_wake);
+        for (int d = 0; d < 12; d++) {
+            int axis = d >> 2, r = d & 3;
+            int delta = ((r & 1) ? -1 : 1) * ((r & 2) ? 2 : 1);
+            int B = axis == 0 ? BX : axis == 1 ? BY : BZ;
+            for (int L = 0; L < S::N; L++) {
+                int pos = axis == 0 ? L % BX : axis == 1 ? (L / BX) % BY : L / (BX * BY);
+                int src = pos - delta;
+                if (src >= 0 && src < B) wm[d * S::MW + L / 32] |= 1u << (L % 32);
+            }
+        }
+    }
     // Plan: one group per grid that has fields, fields ordered by group.
     std::vector<int> group_grid, group_first, field_list;
     std::vector<int> group_nf;
@@ -196,6 +214,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     size_t o_field_list = A.add(sizeof(int) * field_list.size());
     std::copy(field_list.begin(), field_list.end(), A.at<int>(o_field_list));
     size_t o_pre = A.add(sizeof(int) * size_t(maxdiag) * (G + 1));
+    int max_items = 0;
     for (int q = 0; q < maxdiag; q++) {
         int* pre = A.at<int>(o_pre) + size_t(q) * (G + 1);
         int64_t acc = 0;
@@ -206,8 +225,9 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
             if (q < ndiag[gi]) cnt = A.at<int>(o_diag_off[gi])[q + 1] - A.at<int>(o_diag_off[gi])[q];
             acc += int64_t(group_nf[gg]) * cnt;
         }
-        if (acc > INT32_MAX) return ctx->fail(TS_E_ARG, "too many tiles in one diagonal step");
+        if (acc > INT32_MAX / 2) return ctx->fail(TS_E_ARG, "too many tiles in one diagonal step");
         pre[G] = int(acc);
+        max_items = std::max(max_items, int(acc));
     }
     // Fields, states, control.
     size_t o_fields = A.add(sizeof(FieldDesc<Real>) * nf);
@@ -237,6 +257,10 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     if (!D) return TS_E_NOMEM;
     uint8_t* dirty = static_cast<uint8_t*>(ctx->buf("eng.dirty", size_t(dirty_total)));
     if (!dirty) return TS_E_NOMEM;
+    uint32_t* dmask = static_cast<uint32_t*>(ctx->buf("eng.dmask", sizeof(uint32_t) * size_t(dirty_total) * S::MW));
+    if (!dmask) return TS_E_NOMEM;
+    auto* worklist = static_cast<unsigned long long*>(ctx->buf("eng.worklist", 16 * size_t(std::max(1, max_items))));
+    if (!worklist) return TS_E_NOMEM;
     for (int gi = 0; gi < ng; gi++) {
         GridDesc gd{};
         const host::Grid& g = *job.grids[gi];
@@ -260,6 +284,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         fd.T = static_cast<Real*>(ef.T);
         fd.s = static_cast<const Real*>(ef.slowness);
         fd.dirty = dirty + A.at<int64_t>(o_dirty_off)[f];
+        fd.dmask = dmask + A.at<int64_t>(o_dirty_off)[f] * S::MW;
         fd.grid = ef.grid;
         fd.seed_begin = seed_begin[f];
         fd.seed_count = seed_count[f];
@@ -276,7 +301,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         dim3 grid(unsigned(std::min<int64_t>((maxn + 255) / 256, 512)), unsigned(nf));
         fill_fields_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
                                                       reinterpret_cast<const GridDesc*>(D + o_grids), dirty,
-                                                      reinterpret_cast<const int64_t*>(D + o_dirty_off));
+                                                      reinterpret_cast<const int64_t*>(D + o_dirty_off), S::MW);
         int cnt = int(sc_node.size());
         if (cnt > 0)
             seed_fields_kernel<Real><<<(cnt + 255) / 256, 256, 0, s>>>(
@@ -294,6 +319,7 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     args.seed_mask = reinterpret_cast<const uint32_t*>(D + o_seed_mask);
     args.plane_tab = reinterpret_cast<const uint16_t*>(D + o_ptab);
     args.plane_off = reinterpret_cast<const int*>(D + o_poff);
+    args.wake_mask = reinterpret_cast<const uint32_t*>(D + o_wake);
     args.ctl = reinterpret_cast<Control*>(D + o_ctl);
     args.cancel = ctx->cancel_dev;
     args.plan.ngroups = G;
@@ -303,13 +329,16 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     args.plan.field_list = reinterpret_cast<const int*>(D + o_field_list);
     args.plan.pre = reinterpret_cast<const int*>(D + o_pre);
     args.n_active = int(field_list.size());
+    args.worklist = worklist;
+    args.worklist_cap = std::max(1, max_items);
     args.max_rounds_per_launch = 0;
     args.barrier_timeout_ns = 5000000000LL;
     args.tol = Real(job.tol);
+    args.wake_rel = Real(job.wake_rel);
 
     const int smem = engine_smem_bytes<Real, S>(WARPS);
-    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, true>
-                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, false>;
+    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true>
+                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false>;
     TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
     TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
@@ -413,10 +442,13 @@ int fields_to_dense_f32_device(ts_ctx* ctx, const EngineJob& job, int precision,
 template <typename Real>
 int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     if (job.fields.empty()) return TS_OK;
-    constexpr int W = sizeof(Real) == 8 ? 4 : 8;
+    // Warps per block sized so that two or three blocks fill an SM's shared memory.
+    constexpr bool F64 = sizeof(Real) == 8;
     switch (job.tile) {
-        case 1: return launch_shape<Real, 16, 8, 4, W>(ctx, job, stats);
-        default: return launch_shape<Real, 8, 8, 8, W>(ctx, job, stats);
+        case 1: return launch_shape<Real, 16, 8, 4, F64 ? 5 : 8, 2>(ctx, job, stats);
+        case 2: return launch_shape<Real, 8, 8, 4, F64 ? 6 : 8, F64 ? 3 : 2>(ctx, job, stats);
+        case 3: return launch_shape<Real, 8, 4, 4, F64 ? 8 : 8, F64 ? 3 : 3>(ctx, job, stats);
+        default: return launch_shape<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, job, stats);
     }
 }
 

@@ -27,6 +27,7 @@ struct EngineJob {
     std::vector<const host::Metric*> metrics;
     std::vector<EngineField> fields;
     double tol = 1e-7;
+    double wake_rel = 0;     // 0: the reference's dirty rule (bitwise); TS_WAKE_REL for TS_MODE_FAST
     int tile = 0;            // tile shape id (0 = default for the precision)
     int warps = 0;           // warps per block (0 = default)
     // Set by engine_run: the padded field layout. Node (i, j, k) of a field on grid g sits at

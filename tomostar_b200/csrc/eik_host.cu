@@ -259,6 +259,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
         job.grids.push_back(&g);
         job.metrics.push_back(&m);
         job.tol = in.tol;
+        job.wake_rel = in.mode == TS_MODE_FAST ? TS_WAKE_REL : 0.0;
         job.tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
         for (int f = 0; f < nf; f++) {
             EngineField ef;

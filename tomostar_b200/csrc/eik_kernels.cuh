@@ -128,7 +128,8 @@ template <typename Real>
 struct FieldDesc {
     Real* T;              // the field, padded rows (Layout)
     const Real* s;        // its slowness
-    uint8_t* dirty;       // one flag per tile
+    uint8_t* dirty;       // one flag per tile: some node of the tile is due for an update
+    uint32_t* dmask;      // per tile, one bit per node (MW words): the node is due for an update
     int grid;             // GridDesc index
     int seed_begin;       // its seed tiles: seed_tile[seed_begin .. seed_begin + seed_count), by tile id
     int seed_count;
@@ -151,6 +152,8 @@ struct Control {
     int pad;
     unsigned long long updates;
     unsigned long long visits;
+    int produced[2];   // due tiles listed in the step's worklist (by step parity)
+    int consumed[2];   // worklist entries taken
 };
 
 struct Plan {
@@ -171,13 +174,17 @@ struct Args {
     const uint32_t* seed_mask;   // kMaskWords words per seed tile: the fixed nodes
     const uint16_t* plane_tab;   // canonical tile nodes ordered by plane
     const int* plane_off;        // [nplanes + 1]
+    const uint32_t* wake_mask;   // [12][MW] destination masks of the 12 stencil offsets (see wake)
     Control* ctl;
     const volatile int* cancel;  // host-mapped cancel flag
     Plan plan;
     int n_active;                // entries of plan.field_list
+    unsigned long long* worklist;  // 2 x worklist_cap due tiles: field << 32 | tx | ty << 10 | tz << 20
+    int worklist_cap;
     int max_rounds_per_launch;   // rounds this launch may run (<= 0: until every field is done)
     long long barrier_timeout_ns;
     Real tol;
+    Real wake_rel;               // a drop wakes the neighbours when it exceeds wake_rel × the new time
 };
 
 TS_DEVINL unsigned long long global_ns() {
@@ -243,21 +250,49 @@ constexpr int warp_reals() {
     return S::CUBE + S::N + 2 * S::BY * S::BZ + 2 * S::BZ + kZCoef * S::BZ;
 }
 
+// Per warp also four node bitsets of MW words: fixed (seed) nodes, due nodes, nodes changed in the
+// current plane, nodes changed in this visit.
 template <typename Real, class S>
 struct WarpSmem {
-    static constexpr int kBytes = ((warp_reals<S>() * int(sizeof(Real)) + S::MW * 4) + 15) / 16 * 16;
+    static constexpr int kBytes = ((warp_reals<S>() * int(sizeof(Real)) + 4 * S::MW * 4) + 15) / 16 * 16;
 };
+
+// The 12 stencil offsets in a tile's linear node index, in the order of the wake masks.
+template <class S>
+TS_HDINL int stencil_offset(int d) {
+    const int step[3] = {1, S::BX, S::BX * S::BY};
+    int axis = d >> 2, r = d & 3;  // r: +1, -1, +2, -2
+    int m = (r & 2) ? 2 : 1;
+    return ((r & 1) ? -m : m) * step[axis];
+}
 
 template <typename Real, class S>
 constexpr int engine_smem_bytes(int warps) {
-    return warps * WarpSmem<Real, S>::kBytes + ((S::N * 2 + 15) / 16 * 16) + (S::NPLANES + 1) * 4;
+    return warps * WarpSmem<Real, S>::kBytes + ((S::N * 2 + 15) / 16 * 16) + ((S::NPLANES + 1) * 4 + 15) / 16 * 16 +
+           12 * S::MW * 4;
+}
+
+// Word w of a tile bitset shifted so that bit L moves to L + d (bits shifted in are 0).
+TS_DEVINL uint32_t shifted_word(const uint32_t* src, int mw, int w, int d) {
+    int base = 32 * w - d;
+    int ws = base >> 5, bs = base & 31;
+    uint32_t lo = (ws >= 0 && ws < mw) ? src[ws] : 0u;
+    if (bs == 0) return lo;
+    uint32_t hi = (ws + 1 >= 0 && ws + 1 < mw) ? src[ws + 1] : 0u;
+    return (lo >> bs) | (hi << (32 - bs));
 }
 
 // Processes one tile of one field for sweep ordering `dir`. Returns the node evaluations made.
+//
+// Due nodes are tracked per node, as the reference's dirty flags do (EikonalOpenCl.cs:528-532,
+// 608-622): only due nodes are evaluated (a node that is not due would get the value it holds), a
+// node is no longer due once evaluated, and a node that changes makes its 12 stencil neighbours due
+// — inside the tile through the wake masks after each plane, in the neighbour tiles at the end.
 template <typename Real, class S, bool VARZ>
 TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                            int tz, int dir, bool second, Real* cube, Real* ss, Real* mwx, Real* mwy, Real* mzc,
-                           uint32_t* mask, const uint16_t* ptab, const int* poff, int lane) {
+                           uint32_t* fixedm, uint32_t* dm, uint32_t* chg, uint32_t* chg_all, const uint16_t* ptab,
+                           const int* poff, const uint32_t* wake, int lane) {
     const Real inf = real_inf<Real>();
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t nxy = int64_t(nx) * ny;
@@ -265,7 +300,7 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
     const int tid = (tz * g.ty + ty) * g.tx + tx;
     Real* __restrict__ T = fd.T;
     const Real* __restrict__ slow = fd.s;
-    if (lane == 0) __stcg(&fd.dirty[tid], (uint8_t)0);
+    const bool partial = x0 + S::BX > nx || y0 + S::BY > ny || z0 + S::BZ > nz;
 
     // Axis weights of the tile's rows.
     const Real* wx = static_cast<const Real*>(g.wx);
@@ -316,73 +351,143 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
             else hi = mid;
         }
         bool has = lo < fd.seed_count && __ldg(&a.seed_tile[fd.seed_begin + lo]) == tid;
-        for (int q = lane; q < S::MW; q += 32)
-            mask[q] = has ? __ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * S::MW + q]) : 0u;
+        for (int q = lane; q < S::MW; q += 32) {
+            uint32_t fx = has ? __ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * S::MW + q]) : 0u;
+            // Nodes off the grid (a partial tile) are treated as fixed: never evaluated, never due.
+            if (partial) {
+                for (int b = 0; b < 32; b++) {
+                    int L = 32 * q + b;
+                    int i = L % S::BX, j = (L / S::BX) % S::BY, k = L / (S::BX * S::BY);
+                    if (L >= S::N || x0 + i >= nx || y0 + j >= ny || z0 + k >= nz) fx |= 1u << b;
+                }
+            }
+            fixedm[q] = fx;
+            dm[q] = __ldcg(&fd.dmask[int64_t(tid) * S::MW + q]) & ~fx;
+            chg[q] = 0u;
+            chg_all[q] = 0u;
+        }
     }
+    if (lane == 0) __stcg(&fd.dirty[tid], (uint8_t)0);
     cp_async_wait_all();
     __syncwarp();
 
-    // Node planes of the tile in the mirrored order of `dir`.
+    // Node planes of the tile in the mirrored order of `dir`; only due nodes are evaluated.
     const Real tol = a.tol;
-    bool any = false, big = false;
-    unsigned faces = 0;
+    bool big = false, modified = false;
     int evals = 0;
     for (int p = 0; p < S::NPLANES; p++) {
-        int e1 = poff[p + 1];
-        for (int e = poff[p] + lane; e < e1; e += 32) {
-            unsigned pk = ptab[e];
-            int ip = pk & 31, jp = (pk >> 5) & 31, kp = pk >> 10;
-            int i = (dir & 1) ? S::BX - 1 - ip : ip;
-            int j = (dir & 2) ? S::BY - 1 - jp : jp;
-            int k = (dir & 4) ? S::BZ - 1 - kp : kp;
-            if (x0 + i >= nx || y0 + j >= ny || z0 + k >= nz) continue;
-            int L = (k * S::BY + j) * S::BX + i;
-            if ((mask[L >> 5] >> (L & 31)) & 1u) continue;
-            evals++;
-            int c = S::cidx(i, j, k);
-            Real cur = cube[c];
-            Real cand = Update<Real, VARZ>::eval(
-                ss[L], cube[c - 1], cube[c + 1], cube[c - 2], cube[c + 2], cube[c - S::CX], cube[c + S::CX],
-                cube[c - 2 * S::CX], cube[c + 2 * S::CX], cube[c - S::CX * S::CY], cube[c + S::CX * S::CY],
-                cube[c - 2 * S::CX * S::CY], cube[c + 2 * S::CX * S::CY], mwx[2 * (k * S::BY + j)],
-                mwx[2 * (k * S::BY + j) + 1], mwy[2 * k], mwy[2 * k + 1], Real(g.wz1), Real(g.wz2),
-                VARZ ? mzc + kZCoef * k : nullptr, second);
-            if (cand < cur) {
-                cube[c] = cand;
-                any = true;
-                if (counts_as_change<Real>(cur, cand, tol)) big = true;
-                faces |= (i < 2 ? 1u : 0u) | (i >= S::BX - 2 ? 2u : 0u) | (j < 2 ? 4u : 0u) |
-                         (j >= S::BY - 2 ? 8u : 0u) | (k < 2 ? 16u : 0u) | (k >= S::BZ - 2 ? 32u : 0u);
+        const int e0 = poff[p], e1 = poff[p + 1];
+        bool changed_here = false;
+        for (int eb = e0; eb < e1; eb += 32) {
+            int e = eb + lane;
+            int L = 0, i = 0, j = 0, k = 0;
+            bool due = false;
+            if (e < e1) {
+                unsigned pk = ptab[e];
+                int ip = pk & 31, jp = (pk >> 5) & 31, kp = pk >> 10;
+                i = (dir & 1) ? S::BX - 1 - ip : ip;
+                j = (dir & 2) ? S::BY - 1 - jp : jp;
+                k = (dir & 4) ? S::BZ - 1 - kp : kp;
+                L = (k * S::BY + j) * S::BX + i;
+                due = (dm[L >> 5] >> (L & 31)) & 1u;
+            }
+            if (!__any_sync(0xffffffffu, due)) continue;
+            if (due) {
+                atomicAnd(&dm[L >> 5], ~(1u << (L & 31)));
+                evals++;
+                int c = S::cidx(i, j, k);
+                Real cur = cube[c];
+                Real cand = Update<Real, VARZ>::eval(
+                    ss[L], cube[c - 1], cube[c + 1], cube[c - 2], cube[c + 2], cube[c - S::CX], cube[c + S::CX],
+                    cube[c - 2 * S::CX], cube[c + 2 * S::CX], cube[c - S::CX * S::CY], cube[c + S::CX * S::CY],
+                    cube[c - 2 * S::CX * S::CY], cube[c + 2 * S::CX * S::CY], mwx[2 * (k * S::BY + j)],
+                    mwx[2 * (k * S::BY + j) + 1], mwy[2 * k], mwy[2 * k + 1], Real(g.wz1), Real(g.wz2),
+                    VARZ ? mzc + kZCoef * k : nullptr, second);
+                if (cand < cur) {
+                    cube[c] = cand;
+                    modified = true;
+                    if (counts_as_change<Real>(cur, cand, tol)) big = true;
+                    if (wakes<Real>(cur, cand, a.wake_rel)) {
+                        atomicOr(&chg[L >> 5], 1u << (L & 31));
+                        changed_here = true;
+                    }
+                }
+            }
+        }
+        // Wake the stencil neighbours of this plane's changed nodes (they lie on other planes).
+        if (__any_sync(0xffffffffu, changed_here)) {
+            __syncwarp();
+            uint32_t wake_w = 0, c_w = 0;
+            if (lane < S::MW) {
+                c_w = chg[lane];
+#pragma unroll
+                for (int d = 0; d < 12; d++)
+                    wake_w |= shifted_word(chg, S::MW, lane, stencil_offset<S>(d)) & wake[d * S::MW + lane];
+            }
+            __syncwarp();
+            if (lane < S::MW) {
+                dm[lane] |= wake_w & ~fixedm[lane];
+                chg_all[lane] |= c_w;
+                chg[lane] = 0u;
             }
         }
         __syncwarp();
     }
-    bool any_w = __any_sync(0xffffffffu, any);
-    if (any_w) {
-        bool big_w = __any_sync(0xffffffffu, big);
-        unsigned faces_w = __reduce_or_sync(0xffffffffu, faces);
+    // Hand the due nodes back; wake nodes of the neighbour tiles within two nodes of a change.
+    bool any_due = false, any_chg = false;
+    if (lane < S::MW) {
+        uint32_t d = dm[lane] & ~fixedm[lane];
+        __stcg(&fd.dmask[int64_t(tid) * S::MW + lane], d);
+        any_due = d != 0u;
+        any_chg = chg_all[lane] != 0u;
+    }
+    any_due = __any_sync(0xffffffffu, any_due);
+    any_chg = __any_sync(0xffffffffu, any_chg);
+    if (lane == 0 && any_due) __stcg(&fd.dirty[tid], (uint8_t)1);
+    if (__any_sync(0xffffffffu, modified)) {
         for (int q = lane; q < S::N; q += 32) {
             int i = q % S::BX, j = (q / S::BX) % S::BY, k = q / (S::BX * S::BY);
             int gx = x0 + i, gy = y0 + j, gz = z0 + k;
             if (gx < nx && gy < ny && gz < nz) st_cg(&T[(int64_t(gz) * ny + gy) * pitch + S::HX + gx], cube[S::cidx(i, j, k)]);
         }
-        // A node of this tile may read a node that changed after it was evaluated: visit the tile
-        // again next sweep. Neighbour tiles within two nodes of a changed node are woken too.
-        if (lane == 0) __stcg(&fd.dirty[tid], (uint8_t)1);
-        if (lane == 1 && (faces_w & 1u) && tx > 0) __stcg(&fd.dirty[tid - 1], (uint8_t)1);
-        if (lane == 2 && (faces_w & 2u) && tx + 1 < g.tx) __stcg(&fd.dirty[tid + 1], (uint8_t)1);
-        if (lane == 3 && (faces_w & 4u) && ty > 0) __stcg(&fd.dirty[tid - g.tx], (uint8_t)1);
-        if (lane == 4 && (faces_w & 8u) && ty + 1 < g.ty) __stcg(&fd.dirty[tid + g.tx], (uint8_t)1);
-        if (lane == 5 && (faces_w & 16u) && tz > 0) __stcg(&fd.dirty[tid - g.tx * g.ty], (uint8_t)1);
-        if (lane == 6 && (faces_w & 32u) && tz + 1 < g.tz) __stcg(&fd.dirty[tid + g.tx * g.ty], (uint8_t)1);
-        if (lane == 7 && big_w) atomicExch(&a.state[f].changed, 1);
     }
+    if (any_chg) {
+        for (int q = lane; q < S::N; q += 32) {
+            int i = q % S::BX, j = (q / S::BX) % S::BY, k = q / (S::BX * S::BY);
+            if (!((chg_all[q >> 5] >> (q & 31)) & 1u)) continue;
+            // Neighbours at distance 1 and 2 across each face, in the neighbour tile's coordinates.
+#pragma unroll
+            for (int axis = 0; axis < 3; axis++) {
+                const int pos = axis == 0 ? i : axis == 1 ? j : k;
+                const int B = axis == 0 ? S::BX : axis == 1 ? S::BY : S::BZ;
+                const int tpos = axis == 0 ? tx : axis == 1 ? ty : tz;
+                const int tcount = axis == 0 ? g.tx : axis == 1 ? g.ty : g.tz;
+                const int tstride = axis == 0 ? 1 : axis == 1 ? g.tx : g.tx * g.ty;
+                const int nstride = axis == 0 ? 1 : axis == 1 ? S::BX : S::BX * S::BY;
+#pragma unroll
+                for (int dd = -2; dd <= 2; dd++) {
+                    if (dd == 0) continue;
+                    int np = pos + dd;
+                    if (np >= 0 && np < B) continue;  // inside this tile: woken already
+                    int nt = np < 0 ? tpos - 1 : tpos + 1;
+                    if (nt < 0 || nt >= tcount) continue;
+                    int local = np < 0 ? np + B : np - B;
+                    int nL = q + (local - pos) * nstride;
+                    int ntid = tid + (nt - tpos) * tstride;
+                    atomicOr(&fd.dmask[int64_t(ntid) * S::MW + (nL >> 5)], 1u << (nL & 31));
+                    __stcg(&fd.dirty[ntid], (uint8_t)1);
+                }
+            }
+        }
+    }
+    big = __any_sync(0xffffffffu, big);
+    if (lane == 0 && big) atomicExch(&a.state[f].changed, 1);
     __syncwarp();
     return evals;
 }
 
-template <typename Real, int BX, int BY, int BZ, int WARPS, bool VARZ_ANY>
-__global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool VARZ_ANY>
+__global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) {
     using S = Shape<Real, BX, BY, BZ>;
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int kWarpBytes = WarpSmem<Real, S>::kBytes;
@@ -393,11 +498,17 @@ __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
     Real* mwx = ss + S::N;
     Real* mwy = mwx + 2 * S::BY * S::BZ;
     Real* mzc = mwy + 2 * S::BZ;
-    uint32_t* mask = reinterpret_cast<uint32_t*>(mzc + kZCoef * S::BZ);
+    uint32_t* fixedm = reinterpret_cast<uint32_t*>(mzc + kZCoef * S::BZ);
+    uint32_t* dm = fixedm + S::MW;
+    uint32_t* chg = dm + S::MW;
+    uint32_t* chg_all = chg + S::MW;
     uint16_t* ptab = reinterpret_cast<uint16_t*>(smem + WARPS * kWarpBytes);
     int* poff = reinterpret_cast<int*>(smem + WARPS * kWarpBytes + (S::N * 2 + 15) / 16 * 16);
+    uint32_t* wake = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(poff) +
+                                                 ((S::NPLANES + 1) * 4 + 15) / 16 * 16);
     for (int q = threadIdx.x; q < S::N; q += blockDim.x) ptab[q] = a.plane_tab[q];
     for (int q = threadIdx.x; q <= S::NPLANES; q += blockDim.x) poff[q] = a.plane_off[q];
+    for (int q = threadIdx.x; q < 12 * S::MW; q += blockDim.x) wake[q] = a.wake_mask[q];
     __syncthreads();
 
     const unsigned nblocks = gridDim.x;
@@ -406,19 +517,28 @@ __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
     const int G = a.plan.ngroups;
     unsigned long long my_updates = 0, my_visits = 0;
     int rounds_this_launch = 0;
+    int step = 0;
 
     for (;;) {
         for (int dir = 0; dir < 8; dir++) {
             for (int q = 0; q < a.plan.maxdiag; q++) {
                 const int* pre = a.plan.pre + int64_t(q) * (G + 1);
                 const int total = __ldg(&pre[G]);
-                // Items are dealt round-robin to the warps (item = gwarp + j·nwarps), so a small step
-                // still spreads over the whole GPU. Each lane decodes one of the warp's next 32
-                // items; the warp then processes the dirty ones in turn.
+                // Two passes per step. First the step's items are dealt round-robin to the warps
+                // (item = gwarp + j·nwarps), each lane decoding one item, and the due tiles are
+                // appended to a worklist. Then the warps take worklist entries one at a time, so a
+                // step ends when the work does, not when the unluckiest warp's share does.
+                const int par = step & 1;
+                if (blockIdx.x == 0 && threadIdx.x == 0) {  // the previous step's counters: free since its barrier
+                    a.ctl->produced[par ^ 1] = 0;
+                    a.ctl->consumed[par ^ 1] = 0;
+                }
+                unsigned long long* wl = a.worklist + int64_t(par) * a.worklist_cap;
                 for (int64_t j0 = 0; gwarp + j0 * nwarps < total; j0 += 32) {
                     int64_t item64 = gwarp + (j0 + lane) * nwarps;
                     int item = item64 < total ? int(item64) : total;
-                    int f = -1, tx = 0, ty = 0, tz = 0;
+                    bool due = false;
+                    unsigned long long entry = 0;
                     if (item < total) {
                         int lo = 0, hi = G;  // first g with pre[g] > item, minus one
                         while (lo < hi) {
@@ -435,37 +555,53 @@ __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
                         int fld = __ldg(&a.plan.field_list[__ldg(&a.plan.group_first[grp]) + fi]);
                         uint32_t pk = __ldg(&g.diag_tiles[d0 + ti]);
                         int ca = pk & 1023, cb = (pk >> 10) & 1023, cc = pk >> 20;
-                        tx = (dir & 1) ? g.tx - 1 - ca : ca;
-                        ty = (dir & 2) ? g.ty - 1 - cb : cb;
-                        tz = (dir & 4) ? g.tz - 1 - cc : cc;
+                        int tx = (dir & 1) ? g.tx - 1 - ca : ca;
+                        int ty = (dir & 2) ? g.ty - 1 - cb : cb;
+                        int tz = (dir & 4) ? g.tz - 1 - cc : cc;
                         const FieldState* st = &a.state[fld];
                         if (*(volatile const int*)&st->status == kRunning) {
                             const FieldDesc<Real>& fd = a.fields[fld];
-                            if (__ldcg(&fd.dirty[(tz * g.ty + ty) * g.tx + tx])) f = fld;
+                            due = __ldcg(&fd.dirty[(tz * g.ty + ty) * g.tx + tx]) != 0;
                         }
+                        entry = (static_cast<unsigned long long>(unsigned(fld)) << 32) | unsigned(tx) |
+                                (unsigned(ty) << 10) | (unsigned(tz) << 20);
                     }
-                    unsigned m = __ballot_sync(0xffffffffu, f >= 0);
-                    while (m) {
-                        int src = __ffs(m) - 1;
-                        m &= m - 1;
-                        int ff = __shfl_sync(0xffffffffu, f, src);
-                        int sx = __shfl_sync(0xffffffffu, tx, src);
-                        int sy = __shfl_sync(0xffffffffu, ty, src);
-                        int sz = __shfl_sync(0xffffffffu, tz, src);
+                    unsigned m = __ballot_sync(0xffffffffu, due);
+                    if (m) {
+                        int base = 0;
+                        if (lane == 0) base = atomicAdd(&a.ctl->produced[par], __popc(m));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        if (due) __stcg(&wl[base + __popc(m & ((1u << lane) - 1u))], entry);
+                    }
+                }
+                if (!grid_barrier(a.ctl, nblocks, a.barrier_timeout_ns)) goto done;
+                {
+                    const int listed = *(volatile int*)&a.ctl->produced[par];
+                    for (;;) {
+                        int idx = 0;
+                        if (lane == 0) idx = atomicAdd(&a.ctl->consumed[par], 1);
+                        idx = __shfl_sync(0xffffffffu, idx, 0);
+                        if (idx >= listed) break;
+                        unsigned long long e = __ldcg(&wl[idx]);
+                        int ff = int(e >> 32);
+                        int sx = int(e & 1023u), sy = int((e >> 10) & 1023u), sz = int((e >> 20) & 1023u);
                         const FieldDesc<Real>& fd = a.fields[ff];
                         const GridDesc& g = a.grids[fd.grid];
                         bool second = *(volatile const int*)&a.state[ff].phase == 1;
                         int ev;
                         if (VARZ_ANY && g.varz)
                             ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
-                                                             mwy, mzc, mask, ptab, poff, lane);
+                                                             mwy, mzc, fixedm, dm, chg, chg_all, ptab, poff, wake,
+                                                             lane);
                         else
                             ev = process_tile<Real, S, false>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
-                                                              mwy, mzc, mask, ptab, poff, lane);
+                                                              mwy, mzc, fixedm, dm, chg, chg_all, ptab, poff, wake,
+                                                              lane);
                         my_updates += ev;
                         my_visits += 1;
                     }
                 }
+                step++;
                 if (!grid_barrier(a.ctl, nblocks, a.barrier_timeout_ns)) goto done;
             }
         }
@@ -511,6 +647,8 @@ __global__ void __launch_bounds__(WARPS * 32) engine_kernel(Args<Real> a) {
             const GridDesc& g = a.grids[fd.grid];
             int nt = g.tx * g.ty * g.tz;
             for (int q = threadIdx.x; q < nt; q += blockDim.x) __stcg(&fd.dirty[q], (uint8_t)1);
+            const int64_t words = int64_t(nt) * ((BX * BY * BZ + 31) / 32);
+            for (int64_t q = threadIdx.x; q < words; q += blockDim.x) __stcg(&fd.dmask[q], 0xffffffffu);
             __syncthreads();
             if (threadIdx.x == 0) a.state[fld].enter1 = 0;
         }

@@ -230,6 +230,19 @@ struct Update<float, VARZ> {
     }
 };
 
+// Whether a drop wakes the node's stencil neighbours: every drop when wake_rel is 0 (the reference),
+// otherwise a drop larger than wake_rel × the new time (or from +inf).
+template <typename Real>
+TS_DEVINL bool wakes(Real cur, Real cand, Real wake_rel);
+template <>
+TS_DEVINL bool wakes<double>(double cur, double cand, double wake_rel) {
+    return !(cur <= 1.7976931348623157e308) || dsub(cur, cand) > dmul(wake_rel, cand);
+}
+template <>
+TS_DEVINL bool wakes<float>(float cur, float cand, float wake_rel) {
+    return !(cur <= 3.4028234663852886e38f) || fsub(cur, cand) > fmul(wake_rel, cand);
+}
+
 // Whether a drop counts towards "the round changed something" (SphericalEikonal.cs:319).
 template <typename Real>
 TS_DEVINL bool counts_as_change(Real cur, Real cand, Real tol) {
