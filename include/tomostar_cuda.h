@@ -120,6 +120,31 @@ int ts_eik_solve_model(ts_ctx* ctx, int32_t model_id, int32_t phase, int32_t n_f
                        const int32_t* seed_index, const double* seed_time, int32_t mode, double tol,
                        int32_t max_rounds, void* out, int32_t out_type, ts_eik_stats* stats);
 
+/* ts_eik_solve_noalloc — no counterpart in the reference. The plain FP64 solve of one field for a
+ * caller that cannot allocate device memory: for instance a process whose device memory is all held
+ * by another allocator (a framework's caching pool, a serving budget reserved at start-up), a plug-in
+ * host that forbids device allocation after initialisation, or a latency-critical path that cannot
+ * take an allocation's implicit synchronisation. The caller passes its own device buffers:
+ * slowness_dev (nx*ny*nz doubles, grid order) and field_dev (the same size, written); seeds are host
+ * arrays as in ts_eik_solve. The function allocates no device memory: its working memory (due and
+ * fixed-node flags, axis weights, seeds, the round flag) is one static __device__ array of about
+ * 13 MB that every GPU which loads the library holds until the process exits. Limits: uniform grids
+ * (depth_km NULL), nx*ny*nz <= TS_NOALLOC_MAX_NODES, ny*nz <= TS_NOALLOC_MAX_ROWS,
+ * nz <= TS_NOALLOC_MAX_LEVELS, at most TS_NOALLOC_MAX_SEEDS distinct seed nodes; larger inputs
+ * return TS_E_CAPACITY. The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream capture.
+ * All calls share the one array, so calls that overlap on the GPU (other host threads, other
+ * streams) race: serialise them. The result equals SphericalEikonal.Relax to the bit (the reference
+ * scheme, one launch per diagonal plane, on `stream`, NULL for the default stream). rounds_out[2]
+ * receives the rounds of each phase. Errors: text in ts_last_error(NULL). */
+#define TS_NOALLOC_MAX_NODES 4194304
+#define TS_NOALLOC_MAX_ROWS 262144
+#define TS_NOALLOC_MAX_LEVELS 8192
+#define TS_NOALLOC_MAX_SEEDS 65536
+int ts_eik_solve_noalloc(const ts_grid* grid, const double* slowness_dev, int32_t n_seeds, const int32_t* seed_index,
+                         const double* seed_time, double* field_dev, double tol, int32_t max_rounds, void* stream,
+                         int32_t* rounds_out);
+
 /* EikonalOpenCl.SelfTest (EikonalOpenCl.cs:346-374): the reference's 22x20x16 heterogeneous case
  * solved on the device and by the host sweeping solver; *rel_err = max |dt| / field range. The
  * gate passes when *rel_err <= 1e-6 (SelfTestTolerance, :45); otherwise TS_E_SELFTEST. */

@@ -11,9 +11,12 @@
 
 using ts::host::Grid;
 
-namespace {
+std::string& ts_thread_error() {
+    thread_local std::string text;
+    return text;
+}
 
-thread_local std::string g_no_ctx_error;
+namespace {
 
 int check_grid(ts_ctx* ctx, const ts_grid* g) {
     if (!g) return ctx->fail(TS_E_ARG, "grid is null");
@@ -82,7 +85,7 @@ void ts_cuda_destroy(ts_ctx* ctx) {
     delete ctx;
 }
 
-const char* ts_last_error(ts_ctx* ctx) { return ctx ? ctx->err.c_str() : g_no_ctx_error.c_str(); }
+const char* ts_last_error(ts_ctx* ctx) { return ctx ? ctx->err.c_str() : ts_thread_error().c_str(); }
 
 int ts_device_name(ts_ctx* ctx, char* buf, int32_t cap) {
     if (!ctx || !buf || cap <= 0) return TS_E_ARG;

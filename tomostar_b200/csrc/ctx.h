@@ -78,6 +78,9 @@ struct ts_ctx {
     type* var = static_cast<type*>((ctx)->buf((key), sizeof(type) * size_t(count))); \
     if (!var) return TS_E_NOMEM
 
+// The error text of calls made without a context (ts_last_error(NULL)), per host thread.
+std::string& ts_thread_error();
+
 // A resident model: grid, metric and the device slowness of its phases (ts_model_put).
 struct ts_ctx::Model {
     ts_grid def{};
