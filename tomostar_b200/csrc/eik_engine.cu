@@ -289,6 +289,8 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         fd.seed_begin = seed_begin[f];
         fd.seed_count = seed_count[f];
         fd.cap = ef.cap;
+        fd.seed_tile_lo = seed_count[f] ? st_tile[seed_begin[f]] : 1;
+        fd.seed_tile_hi = seed_count[f] ? st_tile[seed_begin[f] + seed_count[f] - 1] : 0;
         A.at<FieldDesc<Real>>(o_fields)[f] = fd;
     }
     A.at<Control>(o_ctl)->running = nf;

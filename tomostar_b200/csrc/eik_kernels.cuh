@@ -134,6 +134,7 @@ struct FieldDesc {
     int seed_begin;       // its seed tiles: seed_tile[seed_begin .. seed_begin + seed_count), by tile id
     int seed_count;
     int cap;              // round cap per phase
+    int seed_tile_lo, seed_tile_hi;  // smallest and largest seed tile id (no search outside)
 };
 
 struct FieldState {
@@ -344,13 +345,14 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
     }
     // Fixed (seed) nodes of this tile, if any: binary search of the field's seed tiles.
     {
-        int lo = 0, hi = fd.seed_count;
+        const bool in_range = tid >= fd.seed_tile_lo && tid <= fd.seed_tile_hi;
+        int lo = 0, hi = in_range ? fd.seed_count : 0;
         while (lo < hi) {
             int mid = (lo + hi) >> 1;
             if (__ldg(&a.seed_tile[fd.seed_begin + mid]) < tid) lo = mid + 1;
             else hi = mid;
         }
-        bool has = lo < fd.seed_count && __ldg(&a.seed_tile[fd.seed_begin + lo]) == tid;
+        bool has = in_range && lo < fd.seed_count && __ldg(&a.seed_tile[fd.seed_begin + lo]) == tid;
         for (int q = lane; q < S::MW; q += 32) {
             uint32_t fx = has ? __ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * S::MW + q]) : 0u;
             // Nodes off the grid (a partial tile) are treated as fixed: never evaluated, never due.

@@ -39,6 +39,18 @@ TS_DEVINL double dadd(double a, double b) { return __dadd_rn(a, b); }
 TS_DEVINL double dsub(double a, double b) { return __dadd_rn(a, -b); }
 TS_DEVINL double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
+// a / 3 correctly rounded, for finite a >= 0 (the reference's (4·first − t2)/3, t2 <= first):
+// q0 = RN(a·RN(1/3)) is within an ulp of a/3, r = a − 3·q0 is exact (FMA), and RN(q0 + r·RN(1/3))
+// is the correctly rounded quotient because a/3 is never within a sixth of an ulp of a rounding
+// midpoint (its fraction in half-ulps is 0, 1/3 or 2/3) while q0 + r·RN(1/3) is within 2^-50 ulp of
+// a/3. Same bits as __ddiv_rn(a, 3.0), in three instructions.
+TS_DEVINL double ddiv3(double a) {
+    const double third = 0.33333333333333331;  // RN(1/3)
+    double q0 = __dmul_rn(a, third);
+    double r = __fma_rn(-3.0, q0, a);
+    return __fma_rn(r, third, q0);
+}
+
 // One axis's term (SphericalEikonal.cs:381-395): the smaller neighbour, promoted to second order
 // when its partner beyond is finite and not larger. Produces (effective time, weight, neighbour
 // time); unused terms keep t = +inf and sort last.
@@ -52,7 +64,7 @@ TS_DEVINL void axis64(double minus, double plus, double minus2, double plus2, do
     if (!(first <= 1.7976931348623157e308)) return;  // not finite (first is never NaN)
     bool promote = second && (t2 <= 1.7976931348623157e308) && t2 <= first;
     if (!VARZ) {
-        if (promote) { te = ddiv(dsub(dmul(4.0, first), t2), 3.0); we = w2; }
+        if (promote) { te = ddiv3(dsub(dmul(4.0, first), t2)); we = w2; }
         else { te = first; we = w1; }
     } else {
         const double* c = zc + (minus_side ? 0 : 8);
