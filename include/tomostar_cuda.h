@@ -156,6 +156,27 @@ int32_t ts_engine_shapes(int32_t* shapes, int32_t cap);
 /* Selects the engine's tile shape for one precision on this context (the autotuner's knob). */
 int ts_engine_set_tile(ts_ctx* ctx, int32_t precision, int32_t shape_id);
 
+/* Many fields on grids of uneven size in one engine launch (the reference batches only fields of one
+ * grid and slowness, EikonalOpenCl.TrySolve). Grid g (grids[g], slowness[g]: its nx*ny*nz values on
+ * the host) may have a variable depth array. Field f lies on grid field_grid[f] with seeds
+ * [seed_offsets[f], seed_offsets[f+1]). mode: TS_MODE_ENGINE or TS_MODE_FAST. out: the fields one
+ * after another, each its grid's nx*ny*nz values of out_type, or nothing with TS_OUT_NONE. */
+int ts_eik_solve_multi(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const double* const* slowness,
+                       int32_t n_fields, const int32_t* field_grid, const int32_t* seed_offsets, const int32_t* seed_index,
+                       const double* seed_time, int32_t precision, int32_t mode, double tol, int32_t max_rounds,
+                       void* out, int32_t out_type, ts_eik_stats* stats);
+/* Captures each one-shot engine solve into a CUDA graph and replays it while the same job (the same
+ * grids, fields and seeds on the same buffers) is solved again. No reference counterpart. */
+int ts_engine_set_graph(ts_ctx* ctx, int32_t enable);
+int32_t ts_engine_graph_replays(ts_ctx* ctx);
+/* Times every tile shape on a sample batch (ts_eik_solve_multi arguments, best of `repeats`), selects
+ * the fastest for `precision` on this context and returns it; ms_per_shape[q] receives shape q's
+ * time (up to cap entries). No reference counterpart. */
+int ts_engine_autotune(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const double* const* slowness,
+                       int32_t n_fields, const int32_t* field_grid, const int32_t* seed_offsets, const int32_t* seed_index,
+                       const double* seed_time, int32_t precision, int32_t mode, int32_t repeats, int32_t* best_tile,
+                       double* ms_per_shape, int32_t cap);
+
 /* ---- rays and Jacobian rows (RayKernels.Compute's per-arrival body) ---------------------------- */
 
 typedef struct ts_rows ts_rows;

@@ -67,6 +67,12 @@ SIGNATURES = {
     "ts_eik_suggest_batch": (_i32, [_vp, _i64, _i32]),
     "ts_engine_shapes": (_i32, [_ip, _i32]),
     "ts_engine_set_tile": (C.c_int, [_vp, _i32, _i32]),
+    "ts_eik_solve_multi": (C.c_int, [_vp, _i32, _gp, _P(_dp), _i32, _ip, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32,
+                                     _P(EikStats)]),
+    "ts_engine_set_graph": (C.c_int, [_vp, _i32]),
+    "ts_engine_graph_replays": (_i32, [_vp]),
+    "ts_engine_autotune": (C.c_int, [_vp, _i32, _gp, _P(_dp), _i32, _ip, _ip, _ip, _dp, _i32, _i32, _i32, _ip, _dp,
+                                     _i32]),
     "ts_point_source": (_i32, [_gp, _dp, _d, _d, _d, _d, _d, _ip, _dp, _i32]),
     "ts_eik_solve": (C.c_int, [_vp, _gp, _dp, _i32, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32, _P(EikStats)]),
     "ts_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _i32, _ip]),
@@ -98,3 +104,16 @@ def load() -> C.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def check(rc: int, solver=None) -> None:
+    """Raises TsError for a non-zero return code, with the context's last error when there is one."""
+    if rc != TS_OK:
+        raise TsError(rc, solver.last_error if solver is not None else "")
+
+
+def engine_shapes() -> list[tuple[int, int, int, int]]:
+    """The engine's compiled tile shapes: (id, bx, by, bz)."""
+    buf = (C.c_int32 * 64)()
+    n = load().ts_engine_shapes(buf, 16)
+    return [tuple(buf[4 * q:4 * q + 4]) for q in range(min(n, 16))]

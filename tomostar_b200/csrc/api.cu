@@ -76,8 +76,11 @@ void ts_cuda_destroy(ts_ctx* ctx) {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         ts::eik::models_free(ctx);
+        ctx->drop_graph();
         for (auto& kv : ctx->bufs)
             if (kv.second.p) cudaFree(kv.second.p);
+        for (auto& kv : ctx->pinned)
+            if (kv.second.p) cudaFreeHost(kv.second.p);
         ctx->bufs.clear();
         if (ctx->cancel_host) cudaFreeHost(const_cast<int*>(ctx->cancel_host));
         cudaStreamDestroy(ctx->stream);

@@ -24,6 +24,11 @@ struct ts_ctx {
     volatile int* cancel_host = nullptr;  // host-mapped, read by kernels between rounds
     int* cancel_dev = nullptr;
     int tile_f64 = 0, tile_f32 = 0;       // engine tile shape per precision
+    // CUDA-graph replay of one-shot engine solves: the last captured solve and its signature.
+    bool use_graph = false;
+    unsigned long long graph_sig = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_replays = 0;
 
     struct Model;
     std::map<int, Model*> models;
@@ -34,6 +39,7 @@ struct ts_ctx {
         size_t n = 0;
     };
     std::map<std::string, Buf> bufs;
+    std::map<std::string, Buf> pinned;    // grow-only pinned host buffers
 
     int fail(int code, const std::string& msg) {
         err = msg;
@@ -55,6 +61,28 @@ struct ts_ctx {
         }
         b.n = want;
         return b.p;
+    }
+    // A grow-only named pinned host buffer.
+    void* host_buf(const std::string& key, size_t bytes) {
+        Buf& b = pinned[key];
+        if (b.n >= bytes && b.p) return b.p;
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        if (cudaHostAlloc(&b.p, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            err = "pinned host buffer '" + key + "' of " + std::to_string(want) + " bytes";
+            return nullptr;
+        }
+        b.n = want;
+        return b.p;
+    }
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        graph_sig = 0;
     }
     void release(const std::string& key) {
         auto it = bufs.find(key);

@@ -30,21 +30,20 @@ struct Arena {
     T* at(size_t off) { return reinterpret_cast<T*>(h.data() + off); }
 };
 
+// New fields of an epoch: +inf everywhere (pads included), every tile and node due, state zero.
 template <typename Real>
-__global__ void fill_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const GridDesc* __restrict__ grids,
-                                   uint8_t* __restrict__ dirty_base, const int64_t* __restrict__ dirty_off, int mw) {
-    const FieldDesc<Real>& fd = fields[blockIdx.y];
+__global__ void init_fields_kernel(const FieldDesc<Real>* __restrict__ fields, const GridDesc* __restrict__ grids,
+                                   const int* __restrict__ init_list, int mw) {
+    const FieldDesc<Real>& fd = fields[init_list[blockIdx.y]];
     const GridDesc& g = grids[fd.grid];
-    int64_t n = int64_t(g.pitch) * g.ny * g.nz;  // the pads too: they must read as +inf
+    int64_t n = int64_t(g.pitch) * g.ny * g.nz;
     const Real inf = real_inf<Real>();
-    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < n; q += int64_t(gridDim.x) * blockDim.x)
-        fd.T[q] = inf;
+    const int64_t t0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x, stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = t0; q < n; q += stride) fd.T[q] = inf;
     int64_t nt = int64_t(g.tx) * g.ty * g.tz;
-    uint8_t* d = dirty_base + dirty_off[blockIdx.y];
-    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nt; q += int64_t(gridDim.x) * blockDim.x)
-        d[q] = 1;
-    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nt * mw; q += int64_t(gridDim.x) * blockDim.x)
-        fd.dmask[q] = 0xffffffffu;  // every node due at the start (EikonalOpenCl.cs:411)
+    for (int64_t q = t0; q < nt; q += stride) fd.dirty[q] = 1;
+    for (int64_t q = t0; q < nt * mw; q += stride) fd.dmask[q] = 0xffffffffu;  // every node due (EikonalOpenCl.cs:411)
+    if (t0 == 0) *fd.state = FieldState{};
 }
 
 template <typename Real>
@@ -57,6 +56,13 @@ __global__ void seed_fields_kernel(const FieldDesc<Real>* __restrict__ fields, c
     const GridDesc& g = grids[fd.grid];
     int n = node[q], i = n % g.nx, row = n / g.nx;
     fd.T[int64_t(row) * g.pitch + Layout<Real>::HX + i] = Real(t[q]);
+}
+
+// The epoch's field states, gathered for one copy to the host.
+template <typename Real>
+__global__ void gather_states_kernel(const FieldDesc<Real>* __restrict__ fields, int nf, FieldState* __restrict__ out) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < nf) out[f] = *fields[f].state;
 }
 
 // Padded engine fields → dense grid order of another precision (one field per blockIdx.y).
@@ -73,12 +79,14 @@ __global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_s
 }
 
 template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB>
-int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
+int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const std::vector<const host::Metric*>& metrics,
+                 const std::vector<EngineField*>& fl, double tol, double wake_rel, int max_rounds, ts_eik_stats* stats,
+                 cudaStream_t s) {
     using S = Shape<Real, BX, BY, BZ>;
-    const int nf = int(job.fields.size());
-    const int ng = int(job.grids.size());
+    const int nf = int(fl.size());
+    const int ng = int(grids.size());
     bool any_var = false;
-    for (auto* g : job.grids) any_var |= g->variable;
+    for (auto* g : grids) any_var |= g->variable;
 
     Arena A;
     // Grids.
@@ -86,8 +94,8 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     std::vector<int> tx(ng), ty(ng), tz(ng), ndiag(ng);
     size_t o_grids = A.add(sizeof(GridDesc) * ng);
     for (int gi = 0; gi < ng; gi++) {
-        const host::Grid& g = *job.grids[gi];
-        const host::Metric& m = *job.metrics[gi];
+        const host::Grid& g = *grids[gi];
+        const host::Metric& m = *metrics[gi];
         tx[gi] = (g.nx + BX - 1) / BX;
         ty[gi] = (g.ny + BY - 1) / BY;
         tz[gi] = (g.nz + BZ - 1) / BZ;
@@ -116,27 +124,31 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         o_zc[gi] = A.add(sizeof(Real) * std::max<size_t>(1, m.zc.size()));
         for (size_t q = 0; q < m.zc.size(); q++) A.at<Real>(o_zc[gi])[q] = Real(m.zc[q]);
     }
-    // Seed tiles of each field (sorted by tile id) with their fixed-node masks.
+    // Seed tiles of each field (sorted by tile id) with their fixed-node masks; seed writes of the
+    // fields this epoch initialises.
     std::vector<int> seed_begin(nf), seed_count(nf);
     std::vector<int> st_tile;
     std::vector<uint32_t> st_mask;
-    std::vector<int> sc_field;
+    std::vector<int> sc_field, init_list;
     std::vector<int32_t> sc_node;
     std::vector<double> sc_t;
     for (int f = 0; f < nf; f++) {
-        const EngineField& ef = job.fields[f];
-        const host::Grid& g = *job.grids[ef.grid];
+        const EngineField& ef = *fl[f];
+        const host::Grid& g = *grids[ef.grid];
         const int gi = ef.grid;
+        if (!ef.initialized) init_list.push_back(f);
         std::vector<std::pair<int, int>> tl;  // (tile, local)
-        for (size_t q = 0; q < ef.seed_idx->size(); q++) {
-            int node = (*ef.seed_idx)[q];
+        for (size_t q = 0; q < ef.seed_idx.size(); q++) {
+            int node = ef.seed_idx[q];
             int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
             int tid = ((k / BZ) * ty[gi] + j / BY) * tx[gi] + i / BX;
             int loc = ((k % BZ) * BY + j % BY) * BX + i % BX;
             tl.push_back({tid, loc});
-            sc_field.push_back(f);
-            sc_node.push_back(node);
-            sc_t.push_back((*ef.seed_t)[q]);
+            if (!ef.initialized) {
+                sc_field.push_back(f);
+                sc_node.push_back(node);
+                sc_t.push_back(ef.seed_t[q]);
+            }
         }
         std::sort(tl.begin(), tl.end());
         seed_begin[f] = int(st_tile.size());
@@ -159,6 +171,8 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     std::copy(sc_node.begin(), sc_node.end(), A.at<int32_t>(o_sc_node));
     size_t o_sc_t = A.add(sizeof(double) * sc_t.size(), 8);
     std::copy(sc_t.begin(), sc_t.end(), A.at<double>(o_sc_t));
+    size_t o_init = A.add(sizeof(int) * init_list.size());
+    std::copy(init_list.begin(), init_list.end(), A.at<int>(o_init));
     // Node planes of the canonical tile.
     size_t o_ptab = A.add(sizeof(uint16_t) * S::N);
     size_t o_poff = A.add(sizeof(int) * (S::NPLANES + 1));
@@ -191,29 +205,31 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
             }
         }
     }
-    // Plan: one group per grid that has fields, fields ordered by group.
+    // Plan: one group per grid with running fields, fields ordered by group.
     std::vector<int> group_grid, group_first, field_list;
     std::vector<int> group_nf;
+    int running = 0;
     for (int gi = 0; gi < ng; gi++) {
         int first = int(field_list.size());
         for (int f = 0; f < nf; f++)
-            if (job.fields[f].grid == gi) field_list.push_back(f);
+            if (fl[f]->grid == gi && fl[f]->status == 0) field_list.push_back(f);
         if (int(field_list.size()) > first) {
             group_grid.push_back(gi);
             group_first.push_back(first);
             group_nf.push_back(int(field_list.size()) - first);
         }
     }
+    running = int(field_list.size());
     const int G = int(group_grid.size());
     int maxdiag = 0;
     for (int gg = 0; gg < G; gg++) maxdiag = std::max(maxdiag, ndiag[group_grid[gg]]);
-    size_t o_group_grid = A.add(sizeof(int) * G);
+    size_t o_group_grid = A.add(sizeof(int) * std::max(1, G));
     std::copy(group_grid.begin(), group_grid.end(), A.at<int>(o_group_grid));
-    size_t o_group_first = A.add(sizeof(int) * G);
+    size_t o_group_first = A.add(sizeof(int) * std::max(1, G));
     std::copy(group_first.begin(), group_first.end(), A.at<int>(o_group_first));
-    size_t o_field_list = A.add(sizeof(int) * field_list.size());
+    size_t o_field_list = A.add(sizeof(int) * std::max<size_t>(1, field_list.size()));
     std::copy(field_list.begin(), field_list.end(), A.at<int>(o_field_list));
-    size_t o_pre = A.add(sizeof(int) * size_t(maxdiag) * (G + 1));
+    size_t o_pre = A.add(sizeof(int) * size_t(std::max(1, maxdiag)) * (G + 1));
     int max_items = 0;
     for (int q = 0; q < maxdiag; q++) {
         int* pre = A.at<int>(o_pre) + size_t(q) * (G + 1);
@@ -229,41 +245,18 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         pre[G] = int(acc);
         max_items = std::max(max_items, int(acc));
     }
-    // Fields, states, control.
+    // Fields, control, state copies.
     size_t o_fields = A.add(sizeof(FieldDesc<Real>) * nf);
-    size_t o_state = A.add(sizeof(FieldState) * nf);
     size_t o_ctl = A.add(sizeof(Control));
-    size_t o_dirty_off = A.add(sizeof(int64_t) * nf, 8);
-    int64_t dirty_total = 0;
-    for (int f = 0; f < nf; f++) {
-        A.at<int64_t>(o_dirty_off)[f] = dirty_total;
-        int gi = job.fields[f].grid;
-        dirty_total += int64_t(tx[gi]) * ty[gi] * tz[gi];
-    }
+    size_t o_states = A.add(sizeof(FieldState) * nf);
 
-    // The fields, padded rows (Layout): one buffer, field f at its offset.
-    job.pitch.assign(ng, 0);
-    job.xoff = S::HX;
-    for (int gi = 0; gi < ng; gi++) job.pitch[gi] = Layout<Real>::pitch(tx[gi], BX);
-    std::vector<int64_t> foff(nf + 1, 0);
-    for (int f = 0; f < nf; f++) {
-        const host::Grid& g = *job.grids[job.fields[f].grid];
-        foff[f + 1] = foff[f] + int64_t(job.pitch[job.fields[f].grid]) * g.ny * g.nz;
-    }
-    Real* fields = static_cast<Real*>(ctx->buf("eng.fields", sizeof(Real) * size_t(foff[nf])));
-    if (!fields) return TS_E_NOMEM;
-    for (int f = 0; f < nf; f++) job.fields[f].T = fields + foff[f];
     uint8_t* D = static_cast<uint8_t*>(ctx->buf("eng.arena", A.h.size()));
     if (!D) return TS_E_NOMEM;
-    uint8_t* dirty = static_cast<uint8_t*>(ctx->buf("eng.dirty", size_t(dirty_total)));
-    if (!dirty) return TS_E_NOMEM;
-    uint32_t* dmask = static_cast<uint32_t*>(ctx->buf("eng.dmask", sizeof(uint32_t) * size_t(dirty_total) * S::MW));
-    if (!dmask) return TS_E_NOMEM;
     auto* worklist = static_cast<unsigned long long*>(ctx->buf("eng.worklist", 16 * size_t(std::max(1, max_items))));
     if (!worklist) return TS_E_NOMEM;
     for (int gi = 0; gi < ng; gi++) {
         GridDesc gd{};
-        const host::Grid& g = *job.grids[gi];
+        const host::Grid& g = *grids[gi];
         gd.nx = g.nx; gd.ny = g.ny; gd.nz = g.nz;
         gd.tx = tx[gi]; gd.ty = ty[gi]; gd.tz = tz[gi];
         gd.ndiag = ndiag[gi];
@@ -273,50 +266,43 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
         gd.wx = D + o_wx[gi];
         gd.wy = D + o_wy[gi];
         gd.zc = D + o_zc[gi];
-        gd.wz1 = job.metrics[gi]->wz1;
-        gd.wz2 = job.metrics[gi]->wz2;
-        gd.pitch = job.pitch[gi];
+        gd.wz1 = metrics[gi]->wz1;
+        gd.wz2 = metrics[gi]->wz2;
+        gd.pitch = Layout<Real>::pitch(tx[gi], BX);
         A.at<GridDesc>(o_grids)[gi] = gd;
     }
     for (int f = 0; f < nf; f++) {
-        const EngineField& ef = job.fields[f];
+        const EngineField& ef = *fl[f];
         FieldDesc<Real> fd{};
         fd.T = static_cast<Real*>(ef.T);
         fd.s = static_cast<const Real*>(ef.slowness);
-        fd.dirty = dirty + A.at<int64_t>(o_dirty_off)[f];
-        fd.dmask = dmask + A.at<int64_t>(o_dirty_off)[f] * S::MW;
+        fd.dirty = ef.dirty;
+        fd.dmask = ef.dmask;
         fd.grid = ef.grid;
         fd.seed_begin = seed_begin[f];
         fd.seed_count = seed_count[f];
         fd.cap = ef.cap;
         fd.seed_tile_lo = seed_count[f] ? st_tile[seed_begin[f]] : 1;
         fd.seed_tile_hi = seed_count[f] ? st_tile[seed_begin[f] + seed_count[f] - 1] : 0;
+        fd.state = static_cast<FieldState*>(ef.state);
         A.at<FieldDesc<Real>>(o_fields)[f] = fd;
     }
-    A.at<Control>(o_ctl)->running = nf;
+    A.at<Control>(o_ctl)->running = running;
 
-    cudaStream_t s = ctx->stream;
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(D, A.h.data(), A.h.size(), cudaMemcpyHostToDevice, s));
-    {
-        int64_t maxn = 0;
-        for (int gi = 0; gi < ng; gi++) maxn = std::max(maxn, int64_t(job.pitch[gi]) * job.grids[gi]->ny * job.grids[gi]->nz);
-        dim3 grid(unsigned(std::min<int64_t>((maxn + 255) / 256, 512)), unsigned(nf));
-        fill_fields_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
-                                                      reinterpret_cast<const GridDesc*>(D + o_grids), dirty,
-                                                      reinterpret_cast<const int64_t*>(D + o_dirty_off), S::MW);
-        int cnt = int(sc_node.size());
-        if (cnt > 0)
-            seed_fields_kernel<Real><<<(cnt + 255) / 256, 256, 0, s>>>(
-                reinterpret_cast<const FieldDesc<Real>*>(D + o_fields), reinterpret_cast<const GridDesc*>(D + o_grids),
-                reinterpret_cast<const int*>(D + o_sc_field),
-                reinterpret_cast<const int32_t*>(D + o_sc_node), reinterpret_cast<const double*>(D + o_sc_t), cnt);
-        TS_CUDA_TRY(ctx, cudaGetLastError());
-    }
+    // The work of the epoch, enqueued on stream s: arena upload (from a pinned image), new fields'
+    // initialisation and seeds, the engine launch, and the control block and field states back to
+    // pinned host memory. Recorded directly, or captured once into a CUDA graph and replayed while
+    // the same job (same arena bytes, same buffers) is solved again.
+    uint8_t* image = static_cast<uint8_t*>(ctx->host_buf("eng.arena.image", A.h.size()));
+    Control* ctl_h = static_cast<Control*>(ctx->host_buf("eng.ctl", sizeof(Control)));
+    FieldState* st_h = static_cast<FieldState*>(ctx->host_buf("eng.states", sizeof(FieldState) * std::max(1, nf)));
+    if (!image || !ctl_h || !st_h) return TS_E_NOMEM;
+    std::memcpy(image, A.h.data(), A.h.size());
+    *ctl_h = Control{};
 
     Args<Real> args{};
     args.grids = reinterpret_cast<const GridDesc*>(D + o_grids);
     args.fields = reinterpret_cast<const FieldDesc<Real>*>(D + o_fields);
-    args.state = reinterpret_cast<FieldState*>(D + o_state);
     args.seed_tile = reinterpret_cast<const int*>(D + o_seed_tile);
     args.seed_mask = reinterpret_cast<const uint32_t*>(D + o_seed_mask);
     args.plane_tab = reinterpret_cast<const uint16_t*>(D + o_ptab);
@@ -333,11 +319,10 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     args.n_active = int(field_list.size());
     args.worklist = worklist;
     args.worklist_cap = std::max(1, max_items);
-    args.max_rounds_per_launch = 0;
+    args.max_rounds_per_launch = max_rounds;
     args.barrier_timeout_ns = 5000000000LL;
-    args.tol = Real(job.tol);
-    args.wake_rel = Real(job.wake_rel);
-
+    args.tol = Real(tol);
+    args.wake_rel = Real(wake_rel);
     const int smem = engine_smem_bytes<Real, S>(WARPS);
     void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true>
                         : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false>;
@@ -345,38 +330,107 @@ int launch_shape(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     int per_sm = 0;
     TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
     if (per_sm < 1) return ctx->fail(TS_E_CUDA, "engine kernel does not fit on an SM");
-    int blocks = per_sm * ctx->sm_count;
+    const int blocks = per_sm * ctx->sm_count;
     void* params[] = {&args};
-    cudaEvent_t k0, k1;
-    cudaEventCreate(&k0);
-    cudaEventCreate(&k1);
-    cudaEventRecord(k0, s);
-    cudaError_t le = cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s);
-    cudaEventRecord(k1, s);
-    if (le != cudaSuccess) {
-        cudaEventDestroy(k0);
-        cudaEventDestroy(k1);
-        TS_CUDA_TRY(ctx, le);
+    int64_t maxn = 0;
+    for (int f : init_list) {
+        const host::Grid& g = *grids[fl[f]->grid];
+        maxn = std::max(maxn, int64_t(Layout<Real>::pitch(tx[fl[f]->grid], BX)) * g.ny * g.nz);
     }
-    Control ctl{};
-    std::vector<FieldState> st(nf);
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(&ctl, D + o_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(st.data(), D + o_state, sizeof(FieldState) * nf, cudaMemcpyDeviceToHost, s));
+    cudaEvent_t k0 = nullptr, k1 = nullptr;
+    auto enqueue = [&](bool timed) -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(D, image, A.h.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        for (size_t c0 = 0; c0 < init_list.size(); c0 += 65535) {
+            unsigned cnt = unsigned(std::min<size_t>(65535, init_list.size() - c0));
+            dim3 grid(unsigned(std::min<int64_t>((maxn + 255) / 256, 512)), cnt);
+            init_fields_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
+                                                          reinterpret_cast<const GridDesc*>(D + o_grids),
+                                                          reinterpret_cast<const int*>(D + o_init) + c0, S::MW);
+        }
+        int cnt = int(sc_node.size());
+        if (cnt > 0)
+            seed_fields_kernel<Real><<<(cnt + 255) / 256, 256, 0, s>>>(
+                reinterpret_cast<const FieldDesc<Real>*>(D + o_fields), reinterpret_cast<const GridDesc*>(D + o_grids),
+                reinterpret_cast<const int*>(D + o_sc_field), reinterpret_cast<const int32_t*>(D + o_sc_node),
+                reinterpret_cast<const double*>(D + o_sc_t), cnt);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (running > 0) {
+            if (timed) cudaEventRecord(k0, s);
+            e = cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s);
+            if (timed) cudaEventRecord(k1, s);
+            if (e != cudaSuccess) return e;
+        }
+        gather_states_kernel<Real><<<(nf + 127) / 128, 128, 0, s>>>(reinterpret_cast<const FieldDesc<Real>*>(D + o_fields),
+                                                                    nf, reinterpret_cast<FieldState*>(D + o_states));
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(ctl_h, D + o_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        return cudaMemcpyAsync(st_h, D + o_states, sizeof(FieldState) * nf, cudaMemcpyDeviceToHost, s);
+    };
+    bool graphed = false;
+    if (ctx->use_graph && max_rounds <= 0) {
+        // The job's signature: its arena bytes and the device buffers the work touches.
+        unsigned long long sig = 1469598103934665603ULL;
+        auto mix = [&](const void* p, size_t n) {
+            const uint8_t* b = static_cast<const uint8_t*>(p);
+            for (size_t q = 0; q < n; q++) sig = (sig ^ b[q]) * 1099511628211ULL;
+        };
+        mix(A.h.data(), A.h.size());
+        uintptr_t ptrs[4] = {uintptr_t(D), uintptr_t(worklist), uintptr_t(image), uintptr_t(kfn)};
+        mix(ptrs, sizeof ptrs);
+        if (ctx->graph_exec && ctx->graph_sig == sig) {
+            TS_CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph_exec, s));
+            ctx->graph_replays++;
+            graphed = true;
+        } else {
+            ctx->drop_graph();
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                cudaError_t we = enqueue(false);
+                e = cudaStreamEndCapture(s, &graph);
+                if (we != cudaSuccess) e = we;
+            }
+            if (e == cudaSuccess && graph) e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e == cudaSuccess && ctx->graph_exec) {
+                ctx->graph_sig = sig;
+                TS_CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph_exec, s));
+                graphed = true;
+            } else {
+                cudaGetLastError();  // capture unsupported here: run the work directly
+                ctx->drop_graph();
+            }
+        }
+    }
+    if (!graphed) {
+        cudaEventCreate(&k0);
+        cudaEventCreate(&k1);
+        cudaError_t e = enqueue(true);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(k0);
+            cudaEventDestroy(k1);
+            TS_CUDA_TRY(ctx, e);
+        }
+    }
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    for (int f : init_list) fl[f]->initialized = true;
+    const Control ctl = *ctl_h;
     float kms = 0;
-    cudaEventElapsedTime(&kms, k0, k1);
-    cudaEventDestroy(k0);
-    cudaEventDestroy(k1);
-    if (stats) stats->kernel_ms += kms;
-    for (int f = 0; f < nf; f++) {
-        job.fields[f].status = st[f].status;
-        job.fields[f].rounds[0] = st[f].rounds0;
-        job.fields[f].rounds[1] = st[f].rounds1;
-    }
+    if (!graphed && running > 0) cudaEventElapsedTime(&kms, k0, k1);
+    if (k0) cudaEventDestroy(k0);
+    if (k1) cudaEventDestroy(k1);
     if (stats) {
+        stats->kernel_ms += kms;
         stats->node_updates += int64_t(ctl.updates);
         stats->tile_visits += int64_t(ctl.visits);
-        stats->launches += 1;
+        stats->launches += running > 0 ? 1 : 0;
+    }
+    std::vector<FieldState> st(st_h, st_h + nf);
+    for (int f = 0; f < nf; f++) {
+        fl[f]->status = st[f].status;
+        fl[f]->rounds[0] = st[f].rounds0;
+        fl[f]->rounds[1] = st[f].rounds1;
     }
     if (ctl.error == TS_E_CANCELLED) return ctx->fail(TS_E_CANCELLED, "cancelled");
     if (ctl.error) return ctx->fail(ctl.error, "engine: a device-side wait ran out (barrier timeout)");
@@ -419,43 +473,115 @@ int fields_to_dense_host(ts_ctx* ctx, const EngineJob& job, int precision, void*
     return TS_OK;
 }
 
-// Fields of a one-grid job as dense float32 tables on the device (the .qttb rounding).
-int fields_to_dense_f32_device(ts_ctx* ctx, const EngineJob& job, int precision, float* out) {
-    if (job.fields.empty()) return TS_OK;
-    const host::Grid& g = *job.grids[0];
-    const int pitch = job.pitch[0];
+// One field as a dense float32 table on the device (the .qttb rounding).
+int field_to_dense_f32_device(ts_ctx* ctx, const host::Grid& g, const FieldLayout& L, const void* T, int precision,
+                              float* out, cudaStream_t s) {
     const int64_t rows = int64_t(g.ny) * g.nz, n = rows * g.nx;
-    const int64_t stride = int64_t(pitch) * rows;
-    const int nf = int(job.fields.size());
-    int blocks = int(std::min<int64_t>((n + 255) / 256, 1024));
-    for (int f0 = 0; f0 < nf; f0 += 65535) {
-        int cnt = std::min(65535, nf - f0);
-        if (precision == TS_PRECISION_F64)
-            dense_convert_kernel<double, float><<<dim3(blocks, cnt), 256, 0, ctx->stream>>>(
-                static_cast<const double*>(job.fields[f0].T), stride, pitch, job.xoff, g.nx, rows, out + f0 * n);
-        else
-            dense_convert_kernel<float, float><<<dim3(blocks, cnt), 256, 0, ctx->stream>>>(
-                static_cast<const float*>(job.fields[f0].T), stride, pitch, job.xoff, g.nx, rows, out + f0 * n);
-        TS_CUDA_TRY(ctx, cudaGetLastError());
+    int blocks = int(std::min<int64_t>((n + 255) / 256, 2048));
+    if (precision == TS_PRECISION_F64)
+        dense_convert_kernel<double, float><<<dim3(blocks, 1), 256, 0, s>>>(static_cast<const double*>(T), 0, L.pitch,
+                                                                            L.xoff, g.nx, rows, out);
+    else
+        dense_convert_kernel<float, float><<<dim3(blocks, 1), 256, 0, s>>>(static_cast<const float*>(T), 0, L.pitch,
+                                                                           L.xoff, g.nx, rows, out);
+    TS_CUDA_TRY(ctx, cudaGetLastError());
+    return TS_OK;
+}
+
+// Fields of a job as dense float32 tables on the device, one after another.
+int fields_to_dense_f32_device(ts_ctx* ctx, const EngineJob& job, int precision, float* out) {
+    for (const auto& f : job.fields) {
+        const host::Grid& g = *job.grids[f.grid];
+        FieldLayout L = field_layout(g, job.tile, precision);
+        int rc = field_to_dense_f32_device(ctx, g, L, f.T, precision, out, ctx->stream);
+        if (rc) return rc;
+        out += g.count();
     }
     return TS_OK;
 }
 
 template <typename Real>
-int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
-    if (job.fields.empty()) return TS_OK;
+int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
+                 const std::vector<const host::Metric*>& metrics, const std::vector<EngineField*>& fields,
+                 double tol, double wake_rel, int tile, int max_rounds, ts_eik_stats* stats, cudaStream_t s) {
+    if (fields.empty()) return TS_OK;
     // Warps per block sized so that two or three blocks fill an SM's shared memory.
     constexpr bool F64 = sizeof(Real) == 8;
-    switch (job.tile) {
-        case 1: return launch_shape<Real, 16, 8, 4, F64 ? 5 : 8, 2>(ctx, job, stats);
-        case 2: return launch_shape<Real, 8, 8, 4, F64 ? 6 : 8, F64 ? 3 : 2>(ctx, job, stats);
-        case 3: return launch_shape<Real, 8, 4, 4, F64 ? 8 : 8, F64 ? 3 : 3>(ctx, job, stats);
-        default: return launch_shape<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, job, stats);
+    switch (tile) {
+        case 1: return launch_epoch<Real, 16, 8, 4, F64 ? 5 : 8, 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 2: return launch_epoch<Real, 8, 8, 4, F64 ? 6 : 8, F64 ? 3 : 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 3: return launch_epoch<Real, 8, 4, 4, 8, 3>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        default: return launch_epoch<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
     }
+}
+
+FieldLayout field_layout(const host::Grid& g, int tile, int precision) {
+    int bx = 8, by = 8, bz = 8;
+    for (const auto& t : tile_shapes())
+        if (t.id == tile) { bx = t.bx; by = t.by; bz = t.bz; }
+    const int hx = precision == TS_PRECISION_F64 ? 2 : 4;
+    const int tx = (g.nx + bx - 1) / bx, ty = (g.ny + by - 1) / by, tz = (g.nz + bz - 1) / bz;
+    FieldLayout L;
+    L.pitch = hx + tx * bx + hx;
+    L.xoff = hx;
+    L.tiles = tx * ty * tz;
+    L.mask_words = L.tiles * ((bx * by * bz + 31) / 32);
+    L.rows_ = int64_t(g.ny) * g.nz;
+    return L;
+}
+
+int64_t FieldLayout::elems() const { return int64_t(pitch) * rows_; }
+
+static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
+
+int64_t FieldLayout::bytes(int precision) const {
+    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    return int64_t(up256(size_t(elems()) * esz) + up256(size_t(tiles)) + up256(4 * size_t(mask_words)) + 256);
+}
+
+void engine_field_place(EngineField& f, const FieldLayout& L, int precision, void* block) {
+    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    char* p = static_cast<char*>(block);
+    f.T = p;
+    p += up256(size_t(L.elems()) * esz);
+    f.dirty = reinterpret_cast<uint8_t*>(p);
+    p += up256(size_t(L.tiles));
+    f.dmask = reinterpret_cast<uint32_t*>(p);
+    p += up256(4 * size_t(L.mask_words));
+    f.state = p;
+}
+
+template <typename Real>
+int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
+    if (job.fields.empty()) return TS_OK;
+    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    // Every field's buffers from one pooled block of the context.
+    std::vector<FieldLayout> layouts;
+    for (auto* g : job.grids) layouts.push_back(field_layout(*g, job.tile, precision));
+    size_t total = 0;
+    for (auto& f : job.fields) total += size_t(layouts[f.grid].bytes(precision));
+    char* pool = static_cast<char*>(ctx->buf("eng.fields", total));
+    if (!pool) return TS_E_NOMEM;
+    std::vector<EngineField*> fl;
+    for (auto& f : job.fields) {
+        engine_field_place(f, layouts[f.grid], precision, pool);
+        pool += layouts[f.grid].bytes(precision);
+        f.initialized = false;
+        f.status = 0;
+        fl.push_back(&f);
+    }
+    job.pitch.clear();
+    for (auto& L : layouts) job.pitch.push_back(L.pitch);
+    job.xoff = layouts.empty() ? 0 : layouts[0].xoff;
+    return engine_epoch<Real>(ctx, job.grids, job.metrics, fl, job.tol, job.wake_rel, job.tile, 0, stats, ctx->stream);
 }
 
 template int engine_run<float>(ts_ctx*, EngineJob&, ts_eik_stats*);
 template int engine_run<double>(ts_ctx*, EngineJob&, ts_eik_stats*);
+template int engine_epoch<float>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
+                                 const std::vector<EngineField*>&, double, double, int, int, ts_eik_stats*, cudaStream_t);
+template int engine_epoch<double>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
+                                  const std::vector<EngineField*>&, double, double, int, int, ts_eik_stats*, cudaStream_t);
 
 }  // namespace eik
 }  // namespace ts

@@ -265,8 +265,8 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
             EngineField ef;
             ef.grid = 0;
             ef.slowness = slow_d;
-            ef.seed_idx = &sidx[f];
-            ef.seed_t = &st[f];
+            ef.seed_idx = std::move(sidx[f]);
+            ef.seed_t = std::move(st[f]);
             ef.cap = cap;
             job.fields.push_back(ef);
         }

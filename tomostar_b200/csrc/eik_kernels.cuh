@@ -124,6 +124,11 @@ struct Layout {
     TS_HDINL static int pitch(int tiles_x, int bx) { return HX + tiles_x * bx + HX; }
 };
 
+struct FieldState {
+    int phase, round, status, changed;
+    int enter1, rounds0, rounds1, pad;
+};
+
 template <typename Real>
 struct FieldDesc {
     Real* T;              // the field, padded rows (Layout)
@@ -135,11 +140,7 @@ struct FieldDesc {
     int seed_count;
     int cap;              // round cap per phase
     int seed_tile_lo, seed_tile_hi;  // smallest and largest seed tile id (no search outside)
-};
-
-struct FieldState {
-    int phase, round, status, changed;
-    int enter1, rounds0, rounds1, pad;
+    FieldState* state;               // the field's solve state; lives with the field between launches
 };
 
 struct Control {
@@ -170,7 +171,6 @@ template <typename Real>
 struct Args {
     const GridDesc* grids;
     const FieldDesc<Real>* fields;
-    FieldState* state;
     const int* seed_tile;        // tile id of each seed tile
     const uint32_t* seed_mask;   // kMaskWords words per seed tile: the fixed nodes
     const uint16_t* plane_tab;   // canonical tile nodes ordered by plane
@@ -483,7 +483,7 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
         }
     }
     big = __any_sync(0xffffffffu, big);
-    if (lane == 0 && big) atomicExch(&a.state[f].changed, 1);
+    if (lane == 0 && big) atomicExch(&a.fields[f].state->changed, 1);
     __syncwarp();
     return evals;
 }
@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
                         int tx = (dir & 1) ? g.tx - 1 - ca : ca;
                         int ty = (dir & 2) ? g.ty - 1 - cb : cb;
                         int tz = (dir & 4) ? g.tz - 1 - cc : cc;
-                        const FieldState* st = &a.state[fld];
+                        const FieldState* st = a.fields[fld].state;
                         if (*(volatile const int*)&st->status == kRunning) {
                             const FieldDesc<Real>& fd = a.fields[fld];
                             due = __ldcg(&fd.dirty[(tz * g.ty + ty) * g.tx + tx]) != 0;
@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
                         int sx = int(e & 1023u), sy = int((e >> 10) & 1023u), sz = int((e >> 20) & 1023u);
                         const FieldDesc<Real>& fd = a.fields[ff];
                         const GridDesc& g = a.grids[fd.grid];
-                        bool second = *(volatile const int*)&a.state[ff].phase == 1;
+                        bool second = *(volatile const int*)&a.fields[ff].state->phase == 1;
                         int ev;
                         if (VARZ_ANY && g.varz)
                             ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
             if (t == 0) a.ctl->cancelled = (a.cancel && *a.cancel) ? 1 : 0;
             for (int e = t; e < a.n_active; e += nblocks * blockDim.x) {
                 int fld = a.plan.field_list[e];
-                volatile FieldState* st = &a.state[fld];
+                volatile FieldState* st = a.fields[fld].state;
                 if (st->status != kRunning) continue;
                 int cap = a.fields[fld].cap;
                 if (!st->changed) {
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
         // Phase 1 starts with every node due for an update (EikonalOpenCl.cs:235-239).
         for (int e = blockIdx.x; e < a.n_active; e += nblocks) {
             int fld = a.plan.field_list[e];
-            if (!*(volatile int*)&a.state[fld].enter1) continue;
+            if (!*(volatile int*)&a.fields[fld].state->enter1) continue;
             const FieldDesc<Real>& fd = a.fields[fld];
             const GridDesc& g = a.grids[fd.grid];
             int nt = g.tx * g.ty * g.tz;
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
             const int64_t words = int64_t(nt) * ((BX * BY * BZ + 31) / 32);
             for (int64_t q = threadIdx.x; q < words; q += blockDim.x) __stcg(&fd.dmask[q], 0xffffffffu);
             __syncthreads();
-            if (threadIdx.x == 0) a.state[fld].enter1 = 0;
+            if (threadIdx.x == 0) a.fields[fld].state->enter1 = 0;
         }
         rounds_this_launch++;
         if (!grid_barrier(a.ctl, nblocks, a.barrier_timeout_ns)) goto done;

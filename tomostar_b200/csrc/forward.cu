@@ -89,8 +89,8 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
             eik::EngineField ef;
             ef.grid = 0;
             ef.slowness = slow_d + size_t(n) * tables[t].first;
-            ef.seed_idx = &sidx[t];
-            ef.seed_t = &st[t];
+            ef.seed_idx = sidx[t];
+            ef.seed_t = st[t];
             ef.cap = cap;
             job.fields.push_back(ef);
         }

@@ -154,6 +154,78 @@ class EikonalCuda:
             raise L.TsError(rc, self.last_error)
         return output
 
+    def solve_multi(self, grids: Sequence[GridDef], slownesses: Sequence[np.ndarray], field_grid: Sequence[int],
+                    seed_sets, out_dtype=np.float64, mode: int = L.MODE_ENGINE, tol: float = SETTLE_TOLERANCE,
+                    max_rounds: int = 0, precision: int | None = None):
+        """Fields on grids of uneven size in one engine launch (ts_eik_solve_multi): field f lies on
+        grids[field_grid[f]] with seeds seed_sets[f]. Returns one array per field (grid order), or
+        None with out_dtype=None (the fields stay on the device; the timing is in last_stats_struct)."""
+        lib = L.load()
+        prec = self.precision if precision is None else precision
+        ng, nf = len(grids), len(seed_sets)
+        if len(slownesses) != ng or len(field_grid) != nf:
+            raise ValueError("one slowness per grid and one grid index per field")
+        keep = [g.struct() for g in grids]  # depth arrays stay alive through the structs' copies
+        gs = (L.GridStruct * ng)(*keep)
+        sl = [np.ascontiguousarray(s, np.float64).reshape(-1) for s in slownesses]
+        for g, s in zip(grids, sl):
+            if s.size != g.count:
+                raise ValueError("Slowness and grid differ in size.")
+        sp = (C.POINTER(C.c_double) * ng)(*[_ptr(s, C.c_double) for s in sl])
+        fg = np.ascontiguousarray(field_grid, np.int32)
+        off, idx, t = pack_seeds(seed_sets)
+        if out_dtype is None:
+            out, out_type, buf = None, L.OUT_NONE, None
+        else:
+            total = sum(grids[int(q)].count for q in fg)
+            buf = np.empty(total, out_dtype)
+            out_type = L.OUT_F64 if buf.dtype == np.float64 else L.OUT_F32
+            out = buf.ctypes.data_as(C.c_void_p)
+        rc = lib.ts_eik_solve_multi(self._h, ng, gs, sp, nf, _ptr(fg, C.c_int32), _ptr(off, C.c_int32),
+                                    _ptr(idx, C.c_int32), _ptr(t, C.c_double), prec, mode, tol, max_rounds, out,
+                                    out_type, C.byref(self.last_stats_struct))
+        if rc != L.TS_OK:
+            raise L.TsError(rc, self.last_error)
+        if buf is None:
+            return None
+        res, o = [], 0
+        for q in fg:
+            n = grids[int(q)].count
+            res.append(buf[o:o + n])
+            o += n
+        return res
+
+    def set_graph(self, enable: bool) -> None:
+        """Capture one-shot engine solves as CUDA graphs and replay them for repeated jobs."""
+        L.check(L.load().ts_engine_set_graph(self._h, 1 if enable else 0), self)
+
+    @property
+    def graph_replays(self) -> int:
+        return int(L.load().ts_engine_graph_replays(self._h))
+
+    def autotune(self, grids, slownesses, field_grid, seed_sets, mode: int = L.MODE_FAST, repeats: int = 1,
+                 precision: int | None = None):
+        """Times every compiled tile shape on the sample batch and keeps the fastest; returns
+        (best shape id, {shape id: ms})."""
+        lib = L.load()
+        prec = self.precision if precision is None else precision
+        ng = len(grids)
+        keep = [g.struct() for g in grids]
+        gs = (L.GridStruct * ng)(*keep)
+        sl = [np.ascontiguousarray(s, np.float64).reshape(-1) for s in slownesses]
+        sp = (C.POINTER(C.c_double) * ng)(*[_ptr(s, C.c_double) for s in sl])
+        fg = np.ascontiguousarray(field_grid, np.int32)
+        off, idx, t = pack_seeds(seed_sets)
+        shapes = L.engine_shapes()
+        ms = np.full(len(shapes), np.inf)
+        best = C.c_int32(-1)
+        rc = lib.ts_engine_autotune(self._h, ng, gs, sp, len(seed_sets), _ptr(fg, C.c_int32), _ptr(off, C.c_int32),
+                                    _ptr(idx, C.c_int32), _ptr(t, C.c_double), prec, mode, repeats, C.byref(best),
+                                    _ptr(ms, C.c_double), len(ms))
+        if rc != L.TS_OK:
+            raise L.TsError(rc, self.last_error)
+        return int(best.value), {sid: float(v) for (sid, *_), v in zip(shapes, ms)}
+
     def try_solve(self, grid: GridDef, slowness: np.ndarray, seed_sets, output: np.ndarray, **kw) -> tuple[bool, str]:
         """EikonalOpenCl.TrySolve: (True, "") or (False, reason); output is field-major."""
         try:

@@ -176,3 +176,61 @@ def config4(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000
     np.divide(1.0, vp, out=slow[0])
     np.divide(1.0, vs, out=slow[1])
     return Problem("config4", g, g.coarsened(2), slow, stations, events, arrivals, h)
+
+
+@dataclass
+class GridBatch:
+    """Sources each on its own grid: grids[q] with slowness[q] (grid order) and source q."""
+
+    name: str
+    grids: list
+    slowness: list
+    sources: np.ndarray      # (n, 3) lon, lat, depth km
+    h_km: np.ndarray         # horizontal spacing of each grid
+
+
+def smooth3(a: np.ndarray) -> np.ndarray:
+    """Mean over the 3 nearest cells along each axis in turn (edges repeat the end cell)."""
+    for ax in range(a.ndim):
+        p = np.pad(a, [(1, 1) if d == ax else (0, 0) for d in range(a.ndim)], mode="edge")
+        sl = lambda lo, hi: tuple(slice(lo, hi) if d == ax else slice(None) for d in range(a.ndim))
+        a = (p[sl(0, -2)] + p[sl(1, -1)] + p[sl(2, None)]) / 3.0
+    return a
+
+
+def config2(n_sources: int = 200, seed: int = 3, variable_share: float = 0.5,
+            dims_scale: float = 1.0) -> GridBatch:
+    """200 sources, each on its own grid: nx, ny uniform in 48–192, nz in 32–96, spacing h uniform in
+    0.25–1 km. Half the grids (a coin per grid) have depth levels whose spacing grows geometrically
+    by a ratio r uniform in 1.02–1.05 over the same depth extent (nz−1)·h. Vp = 5.0 + 0.03·depth km/s
+    times a lognormal cell factor exp(N(0, 0.04)) smoothed over 3 cells on every axis. One source
+    per grid, horizontally in the middle 80 % and at a depth in the upper half. One generator,
+    seed 3, drawn in that order grid by grid. dims_scale < 1 shrinks every dimension (test sizes)."""
+    rng = np.random.default_rng(seed)
+    grids, slow, src, hs = [], [], [], []
+    for _ in range(n_sources):
+        nx = int(rng.integers(48, 193))
+        ny = int(rng.integers(48, 193))
+        nz = int(rng.integers(32, 97))
+        h = float(rng.uniform(0.25, 1.0))
+        variable = bool(rng.uniform() < variable_share)
+        r = float(rng.uniform(1.02, 1.05))
+        if dims_scale != 1.0:
+            nx, ny, nz = (max(4, int(round(v * dims_scale))) for v in (nx, ny, nz))
+        depth = None
+        if variable:
+            steps = r ** np.arange(nz - 1)
+            depth = np.concatenate([[0.0], np.cumsum(steps)]) * ((nz - 1) * h / steps.sum())
+            depth[-1] = (nz - 1) * h
+        g = regular_grid(nx, ny, nz, h, depth)
+        z = g.depth()
+        pert = np.exp(rng.normal(0.0, 0.04, size=g.shape))
+        vp = (5.0 + 0.03 * z)[:, None, None] * smooth3(pert)
+        fx, fy, fz = rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.0, 0.5)
+        lon = g.min_lon + fx * (g.max_lon - g.min_lon)
+        lat = g.min_lat + fy * (g.max_lat - g.min_lat)
+        grids.append(g)
+        slow.append((1.0 / vp).reshape(-1))
+        src.append((lon, lat, fz * g.max_depth_km))
+        hs.append(h)
+    return GridBatch("config2", grids, slow, np.asarray(src), np.asarray(hs))
