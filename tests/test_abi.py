@@ -61,7 +61,7 @@ def test_engine_shapes():
     assert n >= 1
     shapes = [tuple(buf[4 * q: 4 * q + 4]) for q in range(n)]
     for sid, bx, by, bz in shapes:
-        assert bx * by * bz % 32 == 0 and max(bx, by, bz) <= 32
+        assert bx * by * bz % 32 == 0 and max(by, bz) <= 32 and bx <= 64
 
 
 @pytest.mark.parametrize("src", [(10.37, 42.61, 8.3), (10.0, 42.0, -5.0), (12.0, 44.0, 200.0), (11.13, 43.5, 0.0)])

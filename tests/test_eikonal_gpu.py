@@ -117,6 +117,20 @@ def test_f32_engine_equals_plain_and_oracle(solver):
     assert rel_err(a[0], ref[0]) <= F32_REL_TOL
 
 
+def test_f32_engine_all_tile_shapes_equal_plain(solver):
+    """FP32 arithmetic is the same in every kernel, so each tile shape equals the plain path bitwise."""
+    g, s, seeds = hetero_case(37, 29, 19, seed=13, nsrc=3)
+    plain = solver.solve(g, s, seeds, precision=32, mode=L.MODE_PLAIN)
+    lib = L.load()
+    try:
+        for sid, bx, by, bz in L.engine_shapes():
+            assert lib.ts_engine_set_tile(solver.handle, 32, sid) == 0
+            out = solver.solve(g, s, seeds, precision=32)
+            assert np.array_equal(out, plain), f"shape {bx}x{by}x{bz}"
+    finally:
+        lib.ts_engine_set_tile(solver.handle, 32, 0)
+
+
 def test_f64_tables_config1_subset(solver):
     """Config 1 (121×121×61, 0.5 km): P and S tables of three stations from the FP64 engine, written as
     float32 (.qttb), equal the oracle's tables to the bit — the headline error is float rounding alone."""

@@ -47,6 +47,22 @@ def test_multi_grid_fp64_bitwise(solver, batch, mode):
         assert np.array_equal(fields[q], ref), f"grid {q} {g.nx}x{g.ny}x{g.nz} variable={g.depth_km is not None}"
 
 
+def test_multi_grid_fp64_bitwise_all_tile_shapes(solver, batch):
+    """Every compiled tile shape (cube tiles and pencils) on uneven and variable grids."""
+    b, seeds = batch
+    n = 6
+    refs = [oracle_field(g, s, seeds[q]) for q, (g, s) in enumerate(zip(b.grids[:n], b.slowness[:n]))]
+    lib = L.load()
+    try:
+        for sid, bx, by, bz in L.engine_shapes():
+            L.check(lib.ts_engine_set_tile(solver.handle, 64, sid), solver)
+            fields = solver.solve_multi(b.grids[:n], b.slowness[:n], list(range(n)), seeds[:n], precision=64)
+            for q in range(n):
+                assert np.array_equal(fields[q], refs[q]), f"tile {bx}x{by}x{bz}, grid {q}"
+    finally:
+        lib.ts_engine_set_tile(solver.handle, 64, 0)
+
+
 def test_multi_grid_shared_grids_and_float32_tables(solver, batch):
     """Several fields per grid (field_grid repeats grids), in mixed order; float32 output is the
     float32 rounding of the FP64 field."""

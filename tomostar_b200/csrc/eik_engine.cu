@@ -6,13 +6,15 @@
 #include <vector>
 
 #include "eik_engine.h"
-#include "eik_kernels.cuh"
+#include "eik_engine_kernel.cuh"
 
 namespace ts {
 namespace eik {
 
 const std::vector<TileShapeInfo>& tile_shapes() {
-    static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4}};
+    // 0-3: cube tiles swept by node planes; 4-5: pencils (one lane per row of an 8×4 cross-section).
+    static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4},
+                                                      {4, 32, 8, 4}, {5, 64, 8, 4}};
     return shapes;
 }
 
@@ -78,7 +80,7 @@ __global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_s
     }
 }
 
-template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB>
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool PENCIL = false>
 int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const std::vector<const host::Metric*>& metrics,
                  const std::vector<EngineField*>& fl, double tol, double wake_rel, int max_rounds, ts_eik_stats* stats,
                  cudaStream_t s) {
@@ -176,7 +178,7 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     // Node planes of the canonical tile.
     size_t o_ptab = A.add(sizeof(uint16_t) * S::N);
     size_t o_poff = A.add(sizeof(int) * (S::NPLANES + 1));
-    {
+    if (!PENCIL) {  // cube tiles only: a pencil needs no plane table
         std::vector<int> cnt(S::NPLANES + 1, 0);
         for (int k = 0; k < BZ; k++)
             for (int j = 0; j < BY; j++)
@@ -192,7 +194,7 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     // Wake masks: for each stencil offset, the tile nodes a changed node at that offset reaches
     // without leaving its row, column or plane.
     size_t o_wake = A.add(sizeof(uint32_t) * 12 * S::MW);
-    {
+    if (!PENCIL) {
         uint32_t* wm = A.at<uint32_t>(o_wake);
         for (int d = 0; d < 12; d++) {
             int axis = d >> 2, r = d & 3;
@@ -323,9 +325,9 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     args.barrier_timeout_ns = 5000000000LL;
     args.tol = Real(tol);
     args.wake_rel = Real(wake_rel);
-    const int smem = engine_smem_bytes<Real, S>(WARPS);
-    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true>
-                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false>;
+    const int smem = PENCIL ? WARPS * PencilSmem<Real, BX>::kBytes : engine_smem_bytes<Real, S>(WARPS);
+    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
+                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>;
     TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
     TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
@@ -511,6 +513,8 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
         case 1: return launch_epoch<Real, 16, 8, 4, F64 ? 5 : 8, 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 2: return launch_epoch<Real, 8, 8, 4, F64 ? 6 : 8, F64 ? 3 : 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 3: return launch_epoch<Real, 8, 4, 4, 8, 3>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 4: return launch_epoch<Real, 32, 8, 4, 4, 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 5: return launch_epoch<Real, 64, 8, 4, 4, F64 ? 2 : 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         default: return launch_epoch<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
     }
 }

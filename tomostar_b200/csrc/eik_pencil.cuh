@@ -1,0 +1,277 @@
+// The pencil tile of the engine: BX×8×4 nodes swept by one warp with one lane per (y, z) row.
+//
+// Inside a tile the reference's plane order i'+j'+k' = p (mirrored coordinates) is kept: at step p
+// the lane of canonical row (j', k') evaluates the node i' = p − j' − k', so every plane of the tile
+// is one step of the warp and a step holds up to 32 nodes of the plane. Each lane keeps the five
+// values i'−2..i'+2 of its own row in registers (a window sliding one node per step); the values of
+// the y and z neighbours at i' come from the lanes of the neighbouring rows by warp shuffles — the
+// lane one row back has just evaluated that node (its window offset −1), the lane one row ahead has
+// not yet (offset +1), and likewise two rows away (offsets ∓2). Rows outside the tile (the two-node
+// halo on the y and z faces) are staged in shared memory once per visit. The visiting order is one
+// in which every node follows its axis neighbours of smaller p, so the field is the reference's to
+// the bit, as for the other tile shapes.
+//
+// Due nodes are tracked per node as the reference's dirty flags (EikonalOpenCl.cs:528-532,
+// 608-622): one 64-bit row mask per lane; a changed node wakes its x neighbours in the lane's own
+// mask, and its y and z neighbours through one ballot of the changed lanes per step.
+#pragma once
+
+#include "eik_kernels.cuh"
+
+namespace ts {
+namespace eik {
+
+constexpr int kPencilBY = 8, kPencilBZ = 4;
+
+// Shared memory of one warp: the 48 halo rows of the tile, BX values each in grid x order —
+// 16 y rows (canonical j' = −2, −1, 8, 9 for each k') then 32 z rows (k' = −2, −1, 4, 5 for each j').
+template <typename Real, int BX>
+struct PencilSmem {
+    static constexpr int kRows = 16 + 32;
+    static constexpr int kBytes = kRows * BX * int(sizeof(Real));
+};
+
+// Halo row of canonical row c (< 0 or >= B on its axis): slot 0..3 for c = −2, −1, B, B+1.
+TS_HDINL int halo_slot(int c, int B) { return c < 0 ? c + 2 : c - B + 2; }
+
+template <int BX>
+TS_DEVINL uint64_t row_reverse(uint64_t m) {
+    if (BX == 64) return __brevll(m);
+    return uint64_t(__brev(uint32_t(m)));
+}
+
+template <typename Real, int BX, bool VARZ>
+TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
+                             int tz, int dir, bool second, Real* halo, int lane) {
+    static_assert(BX == 32 || BX == 64, "pencil rows are 32 or 64 nodes");
+    constexpr int BY = kPencilBY, BZ = kPencilBZ, HX = Layout<Real>::HX;
+    constexpr int MWR = BX / 32;           // mask words per row
+    constexpr int MW = BX * BY * BZ / 32;  // mask words per tile
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr uint64_t kRowBits = BX == 64 ? ~0ull : 0xffffffffull;
+    const Real inf = real_inf<Real>();
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int x0 = tx * BX, y0 = ty * BY, z0 = tz * BZ;
+    const int tid = (tz * g.ty + ty) * g.tx + tx;
+    const bool mx = dir & 1, my = (dir & 2) != 0, mz = (dir & 4) != 0;
+    const int jp = lane & 7, kp = lane >> 3;  // canonical row of the lane
+    const int j = my ? BY - 1 - jp : jp, k = mz ? BZ - 1 - kp : kp;
+    const int gy = y0 + j, gz = z0 + k;
+    const bool row_on = gy < ny && gz < nz;
+    const int pitch = g.pitch;
+    const int64_t rowi = int64_t(gz) * ny + gy;
+    Real* __restrict__ row = fd.T + rowi * pitch + HX + x0;  // dereferenced only when row_on
+    const Real* __restrict__ srow = fd.s + rowi * nx + x0;
+
+    // Halo rows → shared memory (16-byte copies in grid x order; +inf for rows off the grid).
+    {
+        constexpr int NCH = BX * int(sizeof(Real)) / 16;
+        constexpr int PER = 16 / int(sizeof(Real));
+        for (int q = lane; q < 48 * NCH; q += 32) {
+            const int h = q / NCH, ch = q - h * NCH;
+            int hj, hk;  // canonical row of halo row h
+            if (h < 16) {
+                const int slot = h >> 2;
+                hj = slot < 2 ? slot - 2 : slot - 2 + BY;
+                hk = h & 3;
+            } else {
+                const int slot = (h - 16) >> 3;
+                hk = slot < 2 ? slot - 2 : slot - 2 + BZ;
+                hj = (h - 16) & 7;
+            }
+            const int ay = y0 + (my ? BY - 1 - hj : hj), az = z0 + (mz ? BZ - 1 - hk : hk);
+            Real* dst = halo + h * BX + ch * PER;
+            if (ay >= 0 && ay < ny && az >= 0 && az < nz) {
+                cp_async16_cg(dst, fd.T + (int64_t(az) * ny + ay) * pitch + HX + x0 + ch * PER);
+            } else {
+#pragma unroll
+                for (int e = 0; e < PER; e++) dst[e] = inf;
+            }
+        }
+    }
+    // Shared-memory rows of the eight neighbour directions that leave the tile (−1: a lane's shuffle).
+    auto yhalo = [&](int c) { return (c < 0 || c >= BY) ? (halo_slot(c, BY) * 4 + kp) * BX : -1; };
+    auto zhalo = [&](int c) { return (c < 0 || c >= BZ) ? (16 + halo_slot(c, BZ) * 8 + jp) * BX : -1; };
+    const int hy_m1 = yhalo(jp - 1), hy_p1 = yhalo(jp + 1), hy_m2 = yhalo(jp - 2), hy_p2 = yhalo(jp + 2);
+    const int hz_m1 = zhalo(kp - 1), hz_p1 = zhalo(kp + 1), hz_m2 = zhalo(kp - 2), hz_p2 = zhalo(kp + 2);
+
+    // The lane's row: weights, fixed (seed or off-grid) and due nodes, in canonical x order.
+    const Real* wxp = static_cast<const Real*>(g.wx);
+    const Real* wyp = static_cast<const Real*>(g.wy);
+    Real wx1 = Real(1), wx2 = Real(1), wy1 = Real(1), wy2 = Real(1);
+    if (row_on) {
+        wx1 = __ldg(&wxp[2 * rowi]);
+        wx2 = __ldg(&wxp[2 * rowi + 1]);
+        wy1 = __ldg(&wyp[2 * gz]);
+        wy2 = __ldg(&wyp[2 * gz + 1]);
+    }
+    const Real wz1 = Real(g.wz1), wz2 = Real(g.wz2);
+    const Real* zc = VARZ ? static_cast<const Real*>(g.zc) + kZCoef * (row_on ? gz : 0) : nullptr;
+    const int r = k * BY + j;
+    uint64_t fixed = 0, due = 0;
+    {
+        const bool in_range = tid >= fd.seed_tile_lo && tid <= fd.seed_tile_hi;
+        int lo = 0, hi = in_range ? fd.seed_count : 0;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (__ldg(&a.seed_tile[fd.seed_begin + mid]) < tid) lo = mid + 1;
+            else hi = mid;
+        }
+        const bool has = in_range && lo < fd.seed_count && __ldg(&a.seed_tile[fd.seed_begin + lo]) == tid;
+        uint64_t fx = 0, dm = 0;
+#pragma unroll
+        for (int w = 0; w < MWR; w++) {
+            if (has) fx |= uint64_t(__ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * MW + r * MWR + w])) << (32 * w);
+            dm |= uint64_t(__ldcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w])) << (32 * w);
+        }
+        if (!row_on) fx = kRowBits;
+        else if (x0 + BX > nx) fx |= kRowBits & ~((1ull << (nx - x0)) - 1ull);  // x off the grid
+        fixed = mx ? row_reverse<BX>(fx) : fx;
+        due = (mx ? row_reverse<BX>(dm) : dm) & ~fixed;
+    }
+    if (lane == 0) __stcg(&fd.dirty[tid], (uint8_t)0);
+
+    // Window and prefetch rings. Canonical x c ↦ grid x offset ax(c); the row's pads (and the
+    // tile's nodes beyond nx) hold +inf, so x needs no check inside [−2, BX+1].
+    auto ax = [&](int c) { return mx ? BX - 1 - c : c; };
+    auto ldT = [&](int c) -> Real { return (row_on && c >= -2 && c <= BX + 1) ? ld_cg(row + ax(c)) : inf; };
+    auto ldS = [&](int c) -> Real {
+        return (row_on && c >= 0 && c < BX && x0 + ax(c) < nx) ? __ldg(srow + ax(c)) : Real(0);
+    };
+    const int ip0 = -jp - kp;
+    Real W0 = ldT(ip0 - 2), W1 = ldT(ip0 - 1), W2 = ldT(ip0), W3 = ldT(ip0 + 1), W4 = ldT(ip0 + 2);
+    Real tr[4], sr[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        tr[u] = ldT(ip0 + 3 + u);
+        sr[u] = ldS(ip0 + u);
+    }
+    cp_async_wait_all();
+    __syncwarp();
+
+    const Real tol = a.tol, wake_rel = a.wake_rel;
+    auto bit = [](int c) -> uint64_t { return (unsigned)c < unsigned(BX) ? (1ull << c) : 0ull; };
+    uint64_t changed_all = 0;
+    bool big = false;
+    int evals = 0;
+    constexpr int NSTEPS = (BX + BY + BZ - 2 + 3) / 4 * 4;
+    for (int p0 = 0; p0 < NSTEPS; p0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int ip = p0 + u + ip0;
+            const bool is_due = (due >> (ip & 63)) & (unsigned(ip) < unsigned(BX));
+            if (__any_sync(FULL, is_due)) {
+                // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
+                // ahead has not (offset +1); two rows away likewise at offsets ∓2.
+                Real yb1 = __shfl_up_sync(FULL, W1, 1), ya1 = __shfl_down_sync(FULL, W3, 1);
+                Real yb2 = __shfl_up_sync(FULL, W0, 2), ya2 = __shfl_down_sync(FULL, W4, 2);
+                Real zb1 = __shfl_up_sync(FULL, W1, 8), za1 = __shfl_down_sync(FULL, W3, 8);
+                Real zb2 = __shfl_up_sync(FULL, W0, 16), za2 = __shfl_down_sync(FULL, W4, 16);
+                bool chg = false;
+                if (is_due) {
+                    const int x = ax(ip);
+                    if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
+                    if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
+                    if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                    if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
+                    if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
+                    if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
+                    if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                    if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
+                    due &= ~(1ull << ip);
+                    evals++;
+                    // Canonical → grid orientation (minus = smaller grid index).
+                    const Real xm = mx ? W3 : W1, xp = mx ? W1 : W3, xm2 = mx ? W4 : W0, xp2 = mx ? W0 : W4;
+                    const Real ym = my ? ya1 : yb1, yp = my ? yb1 : ya1, ym2 = my ? ya2 : yb2, yp2 = my ? yb2 : ya2;
+                    const Real zm = mz ? za1 : zb1, zp = mz ? zb1 : za1, zm2 = mz ? za2 : zb2, zp2 = mz ? zb2 : za2;
+                    const Real cand = Update<Real, VARZ>::eval(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
+                                                               zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
+                    if (cand < W2) {
+                        if (counts_as_change<Real>(W2, cand, tol)) big = true;
+                        chg = wakes<Real>(W2, cand, wake_rel);
+                        W2 = cand;
+                        st_cg(row + x, cand);
+                    }
+                }
+                const unsigned cb = __ballot_sync(FULL, chg);
+                if (cb) {
+                    // Nodes of this row woken by this step's changes: the lane's own x neighbours,
+                    // and x = i'±1, i'±2 for a change one or two rows back or ahead in y or z.
+                    uint64_t wk = 0;
+                    if (chg) {
+                        wk = bit(ip - 2) | bit(ip - 1) | bit(ip + 1) | bit(ip + 2);
+                        changed_all |= 1ull << ip;
+                    }
+                    const bool back1 = (jp >= 1 && ((cb >> (lane - 1)) & 1u)) || (kp >= 1 && ((cb >> (lane - 8)) & 1u));
+                    const bool ahead1 = (jp <= BY - 2 && ((cb >> (lane + 1)) & 1u)) ||
+                                        (kp <= BZ - 2 && ((cb >> (lane + 8)) & 1u));
+                    const bool back2 = (jp >= 2 && ((cb >> (lane - 2)) & 1u)) || (kp >= 2 && ((cb >> (lane - 16)) & 1u));
+                    const bool ahead2 = (jp <= BY - 3 && ((cb >> (lane + 2)) & 1u)) ||
+                                        (kp <= BZ - 3 && ((cb >> (lane + 16)) & 1u));
+                    if (back1) wk |= bit(ip + 1);
+                    if (ahead1) wk |= bit(ip - 1);
+                    if (back2) wk |= bit(ip + 2);
+                    if (ahead2) wk |= bit(ip - 2);
+                    due |= wk & ~fixed;
+                }
+            }
+            // Slide the window one node and refill the rings four nodes ahead.
+            W0 = W1;
+            W1 = W2;
+            W2 = W3;
+            W3 = W4;
+            W4 = tr[u];
+            tr[u] = ldT(ip + 7);
+            sr[u] = ldS(ip + 4);
+        }
+    }
+
+    // Hand the due nodes back; wake the nodes of the neighbour tiles within two nodes of a change.
+    const uint64_t due_g = mx ? row_reverse<BX>(due & ~fixed) : (due & ~fixed);
+#pragma unroll
+    for (int w = 0; w < MWR; w++) __stcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w], uint32_t(due_g >> (32 * w)));
+    if (__any_sync(FULL, due_g != 0) && lane == 0) __stcg(&fd.dirty[tid], (uint8_t)1);
+    const uint64_t ca = mx ? row_reverse<BX>(changed_all) : changed_all;
+    if (ca) {
+        auto wake_row = [&](int ntid, int nr, uint64_t bits) {
+#pragma unroll
+            for (int w = 0; w < MWR; w++) {
+                const uint32_t m = uint32_t(bits >> (32 * w));
+                if (m) atomicOr(&fd.dmask[int64_t(ntid) * MW + nr * MWR + w], m);
+            }
+            __stcg(&fd.dirty[ntid], (uint8_t)1);
+        };
+        const uint64_t top = 1ull << (BX - 1), top2 = 1ull << (BX - 2);
+        if (tx > 0 && (ca & 3ull)) wake_row(tid - 1, r, ((ca & 1ull) ? (top | top2) : 0ull) | ((ca & 2ull) ? top : 0ull));
+        if (tx + 1 < g.tx && (ca & (top | top2)))
+            wake_row(tid + 1, r, ((ca & top) ? 3ull : 0ull) | ((ca & top2) ? 1ull : 0ull));
+        // Rows j = 0, 1 reach row BY − 1 of the tile behind (j − 1, resp. j − 2); row 0 also BY − 2.
+        if (j <= 1 && ty > 0) {
+            const int nt = tid - g.tx;
+            wake_row(nt, k * BY + BY - 1, ca);
+            if (j == 0) wake_row(nt, k * BY + BY - 2, ca);
+        }
+        if (j >= BY - 2 && ty + 1 < g.ty) {
+            const int nt = tid + g.tx;
+            wake_row(nt, k * BY, ca);
+            if (j == BY - 1) wake_row(nt, k * BY + 1, ca);
+        }
+        if (k <= 1 && tz > 0) {
+            const int nt = tid - g.tx * g.ty;
+            wake_row(nt, (BZ - 1) * BY + j, ca);
+            if (k == 0) wake_row(nt, (BZ - 2) * BY + j, ca);
+        }
+        if (k >= BZ - 2 && tz + 1 < g.tz) {
+            const int nt = tid + g.tx * g.ty;
+            wake_row(nt, j, ca);
+            if (k == BZ - 1) wake_row(nt, BY + j, ca);
+        }
+    }
+    big = __any_sync(FULL, big);
+    if (lane == 0 && big) atomicExch(&a.fields[f].state->changed, 1);
+    __syncwarp();
+    return evals;
+}
+
+}  // namespace eik
+}  // namespace ts
