@@ -332,7 +332,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--tile", type=int, default=2)
+    ap.add_argument("--tile", type=int, default=5)
     ap.add_argument("--mode", type=int, default=2, help="0 engine (bitwise), 2 fast (wake threshold 1e-13)")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")

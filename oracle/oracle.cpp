@@ -885,11 +885,13 @@ extern "C" {
 
 // The reference's sweeping with node-level due flags (EikonalOpenCl.cs:528-532, 608-622), where a
 // node wakes its 12 stencil neighbours only when it dropped by more than wake_rel of its new value
-// (wake_rel = 0: every drop wakes, the reference's rule, identical to or_relax). Used to bound the
-// effect of not propagating last-digit changes. evals_out receives the node evaluations made.
+// (wake_rel = 0: every drop wakes, the reference's rule, identical to or_relax). With `causal`, a
+// drop to t wakes only the neighbours holding more than t: an upwind update uses only neighbours
+// smaller than its result, so a neighbour at or below t cannot be lowered by it (the engine's fast
+// mode). Used to bound the effect of both rules. evals_out receives the node evaluations made.
 int32_t or_relax_wake(const or_grid_def* d, const double* slowness, int32_t n_seeds, const int32_t* seed_idx,
-                      const double* seed_t, double tol, double wake_rel, double* out, int32_t* rounds_out,
-                      int64_t* evals_out) {
+                      const double* seed_t, double tol, double wake_rel, int32_t causal, double* out,
+                      int32_t* rounds_out, int64_t* evals_out) {
     Grid g(*d);
     Metric m(g);
     int n = g.count();
@@ -931,13 +933,16 @@ int32_t or_relax_wake(const or_grid_def* d, const double* slowness, int32_t n_se
                             out[idx] = cand;
                             if (!std::isfinite(cur) || cur - cand > tol) changed = true;
                             if (std::isfinite(cur) && cur - cand <= wake_rel * cand) continue;
+                            auto wake = [&](int nb) {
+                                if (!causal || cand < out[nb]) due[nb] = 1;
+                            };
                             for (int s = 1; s <= 2; s++) {
-                                if (i >= s) due[idx - s] = 1;
-                                if (i + s < nx) due[idx + s] = 1;
-                                if (j >= s) due[idx - s * nx] = 1;
-                                if (j + s < ny) due[idx + s * nx] = 1;
-                                if (k >= s) due[idx - s * nxy] = 1;
-                                if (k + s < nz) due[idx + s * nxy] = 1;
+                                if (i >= s) wake(idx - s);
+                                if (i + s < nx) wake(idx + s);
+                                if (j >= s) wake(idx - s * nx);
+                                if (j + s < ny) wake(idx + s * nx);
+                                if (k >= s) wake(idx - s * nxy);
+                                if (k + s < nz) wake(idx + s * nxy);
                             }
                         }
                 }

@@ -69,7 +69,7 @@ def lib():
             "or_kernel": (i32, [g, dp, i32, ip, dp, i32]),
             "or_ray_row": (i32, [g, fp, d, d, d, g, d, d, d, d, ip, fp, i32, dp]),
             "or_ray_rows_many": (None, [g, fp, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32]),
-            "or_relax_wake": (i32, [g, dp, i32, ip, dp, d, d, dp, ip, P(C.c_int64)]),
+            "or_relax_wake": (i32, [g, dp, i32, ip, dp, d, d, i32, dp, ip, P(C.c_int64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -170,9 +170,11 @@ def relax(g: Grid, slowness, seed_idx, seed_t, tol=1e-7, max_rounds=0):
     return out, bool(ok), rounds
 
 
-def relax_wake(g: Grid, slowness, seed_idx, seed_t, wake_rel, tol=1e-7):
+def relax_wake(g: Grid, slowness, seed_idx, seed_t, wake_rel, tol=1e-7, causal=False):
     """Relax with node-level due flags where a drop wakes the neighbours only above wake_rel of the
-    new time (wake_rel = 0 is the reference's rule). Returns (field, settled, rounds[2], evaluations)."""
+    new time (wake_rel = 0 is the reference's rule) and, with causal, only the neighbours holding
+    more than the new time (the engine's fast mode uses both). Returns (field, settled, rounds[2],
+    evaluations)."""
     s = np.ascontiguousarray(slowness, np.float64)
     si = np.ascontiguousarray(seed_idx, np.int32)
     st = np.ascontiguousarray(seed_t, np.float64)
@@ -180,7 +182,7 @@ def relax_wake(g: Grid, slowness, seed_idx, seed_t, wake_rel, tol=1e-7):
     rounds = np.zeros(2, np.int32)
     ev = C.c_int64()
     ok = lib().or_relax_wake(g.ref, _p(s, C.c_double), len(si), _p(si, C.c_int32), _p(st, C.c_double), tol, wake_rel,
-                             _p(out, C.c_double), _p(rounds, C.c_int32), C.byref(ev))
+                             1 if causal else 0, _p(out, C.c_double), _p(rounds, C.c_int32), C.byref(ev))
     return out, bool(ok), rounds, ev.value
 
 

@@ -252,13 +252,13 @@ WAKE = 1e-13
 
 @pytest.mark.parametrize("shape", [(23, 19, 13), (33, 17, 21), (40, 40, 20)])
 def test_fast_mode_equals_wake_oracle(solver, shape):
-    """TS_MODE_FAST is the reference scheme with the wake threshold: equal to the oracle's
-    relax_wake to the bit, and within 1e-10 relative of the reference (Relax)."""
+    """TS_MODE_FAST is the reference scheme with the wake threshold and the causal wake rule: equal
+    to the oracle's relax_wake to the bit, and within 1e-10 relative of the reference (Relax)."""
     g, s, seeds = hetero_case(*shape, seed=3 * sum(shape))
     og = O.Grid.of(g)
     out = solver.solve(g, s, seeds, precision=64, mode=L.MODE_FAST)
     for f, (si, st) in enumerate(seeds):
-        w, ok, _, _ = O.relax_wake(og, s, si, st, WAKE)
+        w, ok, _, _ = O.relax_wake(og, s, si, st, WAKE, causal=True)
         ref = O.relax(og, s, si, st)[0]
         assert ok and np.array_equal(out[f], w)
         assert rel_err(out[f], ref) <= 1e-10
@@ -280,7 +280,7 @@ def test_fast_mode_all_tile_shapes(solver):
     buf = (C.c_int32 * 64)()
     n = lib.ts_engine_shapes(buf, 16)
     og = O.Grid.of(g)
-    want = np.stack([O.relax_wake(og, s, si, st, WAKE)[0] for si, st in seeds])
+    want = np.stack([O.relax_wake(og, s, si, st, WAKE, causal=True)[0] for si, st in seeds])
     try:
         for q in range(n):
             assert lib.ts_engine_set_tile(solver.handle, 64, buf[4 * q]) == 0

@@ -28,7 +28,7 @@ def oracle_field(g, s, seed, wake_rel=None):
     og = O.Grid.of(g)
     if wake_rel is None:
         return O.relax(og, s, seed[0], seed[1])[0]
-    return O.relax_wake(og, s, seed[0], seed[1], wake_rel)[0]
+    return O.relax_wake(og, s, seed[0], seed[1], wake_rel, causal=True)[0]
 
 
 def test_batch_has_variable_and_uneven_grids(batch):

@@ -169,3 +169,20 @@ def test_relax_wake_threshold_bound():
     fin = np.isfinite(b)
     assert ok and ok2 and np.array_equal(fin, np.isfinite(a))
     assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(b[fin], 1e-9)) < 1e-10
+
+
+def test_relax_wake_causal_rule_bound():
+    """Waking only the neighbours above the new time (the engine's fast mode) skips evaluations that
+    cannot lower a node: the field stays within 1e-10 relative of Relax with fewer evaluations."""
+    g = O.Grid(10, 11, 42, 43, 0, 30, 31, 29, 17)
+    rng = np.random.default_rng(23)
+    s = (1 / (5 + 0.04 * np.repeat(np.linspace(0, 30, 17), 31 * 29))) * (1 + 0.05 * rng.standard_normal(g.count))
+    si, st = O.point_source(g, s, 10.6, 42.5, 9)
+    b, ok, _ = O.relax(g, s, si, st)
+    _, _, _, ev_ref = O.relax_wake(g, s, si, st, 0.0)
+    for wake in (0.0, 1e-13):
+        a, ok2, _, ev = O.relax_wake(g, s, si, st, wake, causal=True)
+        fin = np.isfinite(b)
+        assert ok and ok2 and np.array_equal(fin, np.isfinite(a))
+        assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(b[fin], 1e-9)) < 1e-10
+        assert ev < ev_ref

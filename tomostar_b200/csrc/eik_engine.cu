@@ -325,6 +325,7 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     args.barrier_timeout_ns = 5000000000LL;
     args.tol = Real(tol);
     args.wake_rel = Real(wake_rel);
+    args.causal = wake_rel > 0 ? 1 : 0;  // fast mode: threshold and causal wakes together
     const int smem = PENCIL ? WARPS * PencilSmem<Real, BX>::kBytes : engine_smem_bytes<Real, S>(WARPS);
     void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
                         : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>;

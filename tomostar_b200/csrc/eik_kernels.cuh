@@ -186,6 +186,7 @@ struct Args {
     long long barrier_timeout_ns;
     Real tol;
     Real wake_rel;               // a drop wakes the neighbours when it exceeds wake_rel × the new time
+    int causal;                  // a drop to t wakes only the neighbours holding more than t
 };
 
 TS_DEVINL unsigned long long global_ns() {
@@ -410,8 +411,41 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
                     modified = true;
                     if (counts_as_change<Real>(cur, cand, tol)) big = true;
                     if (wakes<Real>(cur, cand, a.wake_rel)) {
-                        atomicOr(&chg[L >> 5], 1u << (L & 31));
-                        changed_here = true;
+                        if (a.causal) {
+                            // Wake each stencil neighbour holding more than cand, now: in this tile
+                            // through its due mask, in a neighbour tile (whose values are the
+                            // cube's halo, fixed in this visit) through the tile's global mask.
+                            const int pos[3] = {i, j, k};
+                            const int B[3] = {S::BX, S::BY, S::BZ};
+                            const int cstep[3] = {1, S::CX, S::CX * S::CY};
+                            const int nstep[3] = {1, S::BX, S::BX * S::BY};
+                            const int tpos[3] = {tx, ty, tz};
+                            const int tcnt[3] = {g.tx, g.ty, g.tz};
+                            const int tstep[3] = {1, g.tx, g.tx * g.ty};
+#pragma unroll
+                            for (int ax = 0; ax < 3; ax++) {
+#pragma unroll
+                                for (int dd = -2; dd <= 2; dd++) {
+                                    if (dd == 0) continue;
+                                    if (!(cand < cube[c + dd * cstep[ax]])) continue;
+                                    const int np = pos[ax] + dd;
+                                    if (np >= 0 && np < B[ax]) {
+                                        const int nL = L + dd * nstep[ax];
+                                        if (!((fixedm[nL >> 5] >> (nL & 31)) & 1u)) atomicOr(&dm[nL >> 5], 1u << (nL & 31));
+                                    } else {
+                                        const int nt = np < 0 ? tpos[ax] - 1 : tpos[ax] + 1;
+                                        if (nt < 0 || nt >= tcnt[ax]) continue;
+                                        const int nL = L + ((np < 0 ? np + B[ax] : np - B[ax]) - pos[ax]) * nstep[ax];
+                                        const int ntid = tid + (nt - tpos[ax]) * tstep[ax];
+                                        atomicOr(&fd.dmask[int64_t(ntid) * S::MW + (nL >> 5)], 1u << (nL & 31));
+                                        __stcg(&fd.dirty[ntid], (uint8_t)1);
+                                    }
+                                }
+                            }
+                        } else {
+                            atomicOr(&chg[L >> 5], 1u << (L & 31));
+                            changed_here = true;
+                        }
                     }
                 }
             }
@@ -483,7 +517,7 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
         }
     }
     big = __any_sync(0xffffffffu, big);
-    if (lane == 0 && big) atomicExch(&a.fields[f].state->changed, 1);
+    if (lane == 0 && big) __stcg(&a.fields[f].state->changed, 1);  // every writer writes 1
     __syncwarp();
     return evals;
 }

@@ -150,8 +150,12 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     __syncwarp();
 
     const Real tol = a.tol, wake_rel = a.wake_rel;
+    const bool causal = a.causal != 0;
     auto bit = [](int c) -> uint64_t { return (unsigned)c < unsigned(BX) ? (1ull << c) : 0ull; };
-    uint64_t changed_all = 0;
+    // Woken nodes of the neighbour tiles, as row masks in canonical x: the rows one and two beyond
+    // the lane's own y and z faces (a lane has at most one such side per axis), and the x halo.
+    uint64_t wky1 = 0, wky2 = 0, wkz1 = 0, wkz2 = 0;
+    unsigned wxh = 0;  // bits 0..3: canonical x = −1, −2, BX, BX+1
     bool big = false;
     int evals = 0;
     constexpr int NSTEPS = (BX + BY + BZ - 2 + 3) / 4 * 4;
@@ -195,24 +199,41 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                 }
                 const unsigned cb = __ballot_sync(FULL, chg);
                 if (cb) {
-                    // Nodes of this row woken by this step's changes: the lane's own x neighbours,
-                    // and x = i'±1, i'±2 for a change one or two rows back or ahead in y or z.
+                    // A changed node wakes its 12 stencil neighbours (with the causal rule, those
+                    // holding more than its new value W2). The y and z neighbours are woken through
+                    // one ballot per direction: a change one row back wakes x = i'+1 of this row,
+                    // one row ahead x = i'−1, and two rows back or ahead x = i'±2.
+                    auto wk_if = [&](Real v) { return chg && (!causal || W2 < v); };
                     uint64_t wk = 0;
-                    if (chg) {
-                        wk = bit(ip - 2) | bit(ip - 1) | bit(ip + 1) | bit(ip + 2);
-                        changed_all |= 1ull << ip;
-                    }
-                    const bool back1 = (jp >= 1 && ((cb >> (lane - 1)) & 1u)) || (kp >= 1 && ((cb >> (lane - 8)) & 1u));
-                    const bool ahead1 = (jp <= BY - 2 && ((cb >> (lane + 1)) & 1u)) ||
-                                        (kp <= BZ - 2 && ((cb >> (lane + 8)) & 1u));
-                    const bool back2 = (jp >= 2 && ((cb >> (lane - 2)) & 1u)) || (kp >= 2 && ((cb >> (lane - 16)) & 1u));
-                    const bool ahead2 = (jp <= BY - 3 && ((cb >> (lane + 2)) & 1u)) ||
-                                        (kp <= BZ - 3 && ((cb >> (lane + 16)) & 1u));
-                    if (back1) wk |= bit(ip + 1);
-                    if (ahead1) wk |= bit(ip - 1);
-                    if (back2) wk |= bit(ip + 2);
-                    if (ahead2) wk |= bit(ip - 2);
+                    if (wk_if(W1)) wk |= bit(ip - 1);
+                    if (wk_if(W3)) wk |= bit(ip + 1);
+                    if (wk_if(W0)) wk |= bit(ip - 2);
+                    if (wk_if(W4)) wk |= bit(ip + 2);
+                    const unsigned Byb1 = __ballot_sync(FULL, wk_if(yb1)), Bya1 = __ballot_sync(FULL, wk_if(ya1));
+                    const unsigned Byb2 = __ballot_sync(FULL, wk_if(yb2)), Bya2 = __ballot_sync(FULL, wk_if(ya2));
+                    const unsigned Bzb1 = __ballot_sync(FULL, wk_if(zb1)), Bza1 = __ballot_sync(FULL, wk_if(za1));
+                    const unsigned Bzb2 = __ballot_sync(FULL, wk_if(zb2)), Bza2 = __ballot_sync(FULL, wk_if(za2));
+                    if ((jp >= 1 && ((Bya1 >> (lane - 1)) & 1u)) || (kp >= 1 && ((Bza1 >> (lane - 8)) & 1u)))
+                        wk |= bit(ip + 1);
+                    if ((jp <= BY - 2 && ((Byb1 >> (lane + 1)) & 1u)) || (kp <= BZ - 2 && ((Bzb1 >> (lane + 8)) & 1u)))
+                        wk |= bit(ip - 1);
+                    if ((jp >= 2 && ((Bya2 >> (lane - 2)) & 1u)) || (kp >= 2 && ((Bza2 >> (lane - 16)) & 1u)))
+                        wk |= bit(ip + 2);
+                    if ((jp <= BY - 3 && ((Byb2 >> (lane + 2)) & 1u)) || (kp <= BZ - 3 && ((Bzb2 >> (lane + 16)) & 1u)))
+                        wk |= bit(ip - 2);
                     due |= wk & ~fixed;
+                    if (chg) {
+                        // Neighbours in other tiles (their values are the halo's, fixed in this visit).
+                        const uint64_t b = 1ull << ip;
+                        if ((hy_m1 >= 0 && wk_if(yb1)) || (hy_p1 >= 0 && wk_if(ya1))) wky1 |= b;
+                        if ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2))) wky2 |= b;
+                        if ((hz_m1 >= 0 && wk_if(zb1)) || (hz_p1 >= 0 && wk_if(za1))) wkz1 |= b;
+                        if ((hz_m2 >= 0 && wk_if(zb2)) || (hz_p2 >= 0 && wk_if(za2))) wkz2 |= b;
+                        if (ip == 0 && wk_if(W1)) wxh |= 1u;
+                        if (ip <= 1 && wk_if(W0)) wxh |= ip == 0 ? 2u : 1u;
+                        if (ip == BX - 1 && wk_if(W3)) wxh |= 4u;
+                        if (ip >= BX - 2 && wk_if(W4)) wxh |= ip == BX - 1 ? 8u : 4u;
+                    }
                 }
             }
             // Slide the window one node and refill the rings four nodes ahead.
@@ -231,44 +252,46 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
 #pragma unroll
     for (int w = 0; w < MWR; w++) __stcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w], uint32_t(due_g >> (32 * w)));
     if (__any_sync(FULL, due_g != 0) && lane == 0) __stcg(&fd.dirty[tid], (uint8_t)1);
-    const uint64_t ca = mx ? row_reverse<BX>(changed_all) : changed_all;
-    if (ca) {
-        auto wake_row = [&](int ntid, int nr, uint64_t bits) {
+    auto wake_row = [&](int ntid, int nr, uint64_t canon_bits) {
+        const uint64_t bits = mx ? row_reverse<BX>(canon_bits) : canon_bits;
 #pragma unroll
-            for (int w = 0; w < MWR; w++) {
-                const uint32_t m = uint32_t(bits >> (32 * w));
-                if (m) atomicOr(&fd.dmask[int64_t(ntid) * MW + nr * MWR + w], m);
-            }
-            __stcg(&fd.dirty[ntid], (uint8_t)1);
-        };
+        for (int w = 0; w < MWR; w++) {
+            const uint32_t m = uint32_t(bits >> (32 * w));
+            if (m) atomicOr(&fd.dmask[int64_t(ntid) * MW + nr * MWR + w], m);
+        }
+        __stcg(&fd.dirty[ntid], (uint8_t)1);
+    };
+    // Rows beyond the y and z faces: canonical row c outside the tile → the neighbour tile and its row.
+    auto wake_y = [&](int c, uint64_t bits) {
+        if (!bits) return;
+        int ay = my ? BY - 1 - c : c;  // tile-local actual row, outside [0, BY)
+        int nty = ay < 0 ? ty - 1 : ty + 1;
+        if (nty < 0 || nty >= g.ty) return;
+        wake_row(tid + (nty - ty) * g.tx, k * BY + (ay < 0 ? ay + BY : ay - BY), bits);
+    };
+    auto wake_z = [&](int c, uint64_t bits) {
+        if (!bits) return;
+        int az = mz ? BZ - 1 - c : c;
+        int ntz = az < 0 ? tz - 1 : tz + 1;
+        if (ntz < 0 || ntz >= g.tz) return;
+        wake_row(tid + (ntz - tz) * g.tx * g.ty, (az < 0 ? az + BZ : az - BZ) * BY + j, bits);
+    };
+    wake_y(jp == 0 ? -1 : BY, wky1);                      // one row beyond (lanes j' = 0, BY − 1)
+    wake_y(jp <= 1 ? jp - 2 : jp + 2, wky2);              // two rows beyond (j' = 0, 1, BY − 2, BY − 1)
+    wake_z(kp == 0 ? -1 : BZ, wkz1);
+    wake_z(kp <= 1 ? kp - 2 : kp + 2, wkz2);
+    if (wxh) {
+        // Canonical x −1, −2 lie in the tile before along the sweep, BX, BX+1 in the one after.
+        const int back = mx ? tx + 1 : tx - 1, ahead = mx ? tx - 1 : tx + 1;
         const uint64_t top = 1ull << (BX - 1), top2 = 1ull << (BX - 2);
-        if (tx > 0 && (ca & 3ull)) wake_row(tid - 1, r, ((ca & 1ull) ? (top | top2) : 0ull) | ((ca & 2ull) ? top : 0ull));
-        if (tx + 1 < g.tx && (ca & (top | top2)))
-            wake_row(tid + 1, r, ((ca & top) ? 3ull : 0ull) | ((ca & top2) ? 1ull : 0ull));
-        // Rows j = 0, 1 reach row BY − 1 of the tile behind (j − 1, resp. j − 2); row 0 also BY − 2.
-        if (j <= 1 && ty > 0) {
-            const int nt = tid - g.tx;
-            wake_row(nt, k * BY + BY - 1, ca);
-            if (j == 0) wake_row(nt, k * BY + BY - 2, ca);
-        }
-        if (j >= BY - 2 && ty + 1 < g.ty) {
-            const int nt = tid + g.tx;
-            wake_row(nt, k * BY, ca);
-            if (j == BY - 1) wake_row(nt, k * BY + 1, ca);
-        }
-        if (k <= 1 && tz > 0) {
-            const int nt = tid - g.tx * g.ty;
-            wake_row(nt, (BZ - 1) * BY + j, ca);
-            if (k == 0) wake_row(nt, (BZ - 2) * BY + j, ca);
-        }
-        if (k >= BZ - 2 && tz + 1 < g.tz) {
-            const int nt = tid + g.tx * g.ty;
-            wake_row(nt, j, ca);
-            if (k == BZ - 1) wake_row(nt, BY + j, ca);
-        }
+        // In the neighbour tile's canonical x, −1 ↦ BX−1, −2 ↦ BX−2, BX ↦ 0, BX+1 ↦ 1.
+        if ((wxh & 3u) && back >= 0 && back < g.tx)
+            wake_row(tid + (back - tx), r, ((wxh & 1u) ? top : 0ull) | ((wxh & 2u) ? top2 : 0ull));
+        if ((wxh & 12u) && ahead >= 0 && ahead < g.tx)
+            wake_row(tid + (ahead - tx), r, ((wxh & 4u) ? 1ull : 0ull) | ((wxh & 8u) ? 2ull : 0ull));
     }
     big = __any_sync(FULL, big);
-    if (lane == 0 && big) atomicExch(&a.fields[f].state->changed, 1);
+    if (lane == 0 && big) __stcg(&a.fields[f].state->changed, 1);  // every writer writes 1
     __syncwarp();
     return evals;
 }
