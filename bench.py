@@ -304,7 +304,9 @@ def run_ours(args, problem_fn):
             "config": {"workload": f"config4: 401x401x121 nodes at 0.25 km (19.46 M), {n_st} surface stations x P,S "
                                    f"= {2 * n_st} fields per GPU, Vp 1-D gradient + 3 ellipsoids +-8 % (seed 5)",
                        "global_fields": 2 * n_st * world, "tile": args.tile,
-                       "mode": {0: "engine (bitwise with the reference)", 2: "fast (wake 1e-13; <= 1e-11 of bitwise)"}[args.mode],
+                       "mode": {0: "engine (bitwise with the reference)",
+                                2: "fast (a drop wakes only neighbours above the new time, and only when above "
+                                   "1e-13 of it; within 1e-10 rel of bitwise)"}[args.mode],
                        "l2": "inputs larger than L2 (fields 2 x 65 GB per step)",
                        "rounds_last": list(rounds)},
             # Per solve call: the init, seed, engine and state-gather kernels.

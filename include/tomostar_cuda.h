@@ -177,6 +177,59 @@ int ts_engine_autotune(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const
                        const double* seed_time, int32_t precision, int32_t mode, int32_t repeats, int32_t* best_tile,
                        double* ms_per_shape, int32_t cap);
 
+/* ---- serving: a resident request loop with continuous batching (no reference counterpart) ----
+ * A server owns its own context on `device` and one loop thread. Models are put once and stay on
+ * the device. Requests (fields on one model and phase, optionally rays traced on those fields) are
+ * queued in arrival order, admitted while their device footprint (engine buffers and float32
+ * tables of their fields) fits in hbm_budget_bytes, and solved by the engine in epochs of
+ * rounds_per_epoch sweep rounds over every field in flight, so requests that arrive while others
+ * run join the next epoch. A field's result does not depend on the requests it ran with. Rows of
+ * a finished request belong to the caller (ts_rows_free) and must be freed before
+ * ts_serve_destroy. All calls are thread-safe. */
+typedef struct ts_server ts_server;
+typedef struct ts_rows ts_rows;  /* ray rows, see below */
+typedef struct ts_serve_request {
+    int32_t model_id;             /* from ts_serve_model_put */
+    int32_t phase;
+    int32_t n_fields;
+    int32_t n_rays;
+    const int32_t* seed_offsets;  /* n_fields + 1, into seed_index / seed_time (copied at submit) */
+    const int32_t* seed_index;
+    const double* seed_time;
+    const double* field_origin;   /* 3 per field (lon, lat, depth km): where rays of the field end */
+    const int32_t* ray_field;     /* n_rays: the field each ray is traced on */
+    const double* ray_event;      /* 3 per ray: the ray's start (the event) */
+    const ts_grid* inv;           /* grid of the rows' columns; NULL: the forward grid coarsened by 2 */
+    double step_km;               /* <= 0: the RayKernels step (RayKernels.cs:62) */
+    float* tables_out;            /* NULL, or n_fields * nx*ny*nz floats, filled before completion */
+} ts_serve_request;
+typedef struct ts_serve_result {
+    int32_t status;               /* TS_OK or the request's error code */
+    int32_t n_fields;
+    int32_t rounds[2];            /* sweep rounds per phase, the largest over its fields */
+    double queue_ms;              /* submit → admission */
+    double latency_ms;            /* submit → completion (tables and rays done) */
+    ts_rows* rows;                /* the rays' rows (NULL without rays); the caller frees them */
+    char error[160];
+} ts_serve_result;
+typedef struct ts_serve_stats_t {
+    int64_t epochs, fields_done, requests_done, node_updates;
+    double device_ms;             /* engine kernel time */
+    double bytes_in_use, peak_bytes;
+    int32_t queued, in_flight;
+} ts_serve_stats_t;
+int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, double hbm_budget_bytes,
+                    int32_t rounds_per_epoch, ts_server** out);
+void ts_serve_destroy(ts_server* server);
+const char* ts_serve_last_error(ts_server* server);
+int ts_serve_model_put(ts_server* server, const ts_grid* grid, const double* slowness, int32_t n_phases,
+                       int32_t* model_id);
+int ts_serve_submit(ts_server* server, const ts_serve_request* request, int64_t* request_id);
+/* Waits up to timeout_s (< 0: for ever) for a request; TS_E_TIMEOUT if it is not done yet. A
+ * request can be waited for once: its result (and rows) then pass to the caller. */
+int ts_serve_wait(ts_server* server, int64_t request_id, double timeout_s, ts_serve_result* result);
+int ts_serve_stats(ts_server* server, ts_serve_stats_t* stats);
+
 /* ---- rays and Jacobian rows (RayKernels.Compute's per-arrival body) ---------------------------- */
 
 typedef struct ts_rows ts_rows;

@@ -288,3 +288,17 @@ def test_fast_mode_all_tile_shapes(solver):
             assert np.array_equal(out, want)
     finally:
         lib.ts_engine_set_tile(solver.handle, 64, 0)
+
+
+def test_fast_mode_full_size_field_within_1e10(solver):
+    """One field of the 401×401×121 forward step: fast mode against the bitwise engine (which equals
+    the reference's Relax to the bit) within 1e-10 relative; float32 tables within 2e-5 (their
+    rounding)."""
+    p = syn.config4(n_stations=2, n_events=10, n_rays=10)
+    seeds = [point_source(p.grid, p.slowness[1], *p.stations[0])]
+    exact = solver.solve(p.grid, p.slowness[1], seeds, precision=64, mode=L.MODE_ENGINE)
+    fast = solver.solve(p.grid, p.slowness[1], seeds, precision=64, mode=L.MODE_FAST)
+    assert rel_err(fast[0], exact[0]) <= 1e-10
+    t32 = solver.solve(p.grid, p.slowness[1], seeds, mode=L.MODE_FAST,
+                       output=np.empty((1, p.grid.count), np.float32), precision=64)
+    assert rel_err(t32[0].astype(np.float64), exact[0]) <= 2e-5

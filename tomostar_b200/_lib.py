@@ -56,8 +56,46 @@ class EikStats(C.Structure):
 _P = C.POINTER
 _vp, _i32, _i64, _d = C.c_void_p, C.c_int32, C.c_int64, C.c_double
 _ip, _dp, _fp, _u8p = _P(C.c_int32), _P(C.c_double), _P(C.c_float), _P(C.c_uint8)
+class ServeRequest(C.Structure):
+    """ts_serve_request."""
+
+    _fields_ = [
+        ("model_id", C.c_int32), ("phase", C.c_int32), ("n_fields", C.c_int32), ("n_rays", C.c_int32),
+        ("seed_offsets", C.POINTER(C.c_int32)), ("seed_index", C.POINTER(C.c_int32)),
+        ("seed_time", C.POINTER(C.c_double)), ("field_origin", C.POINTER(C.c_double)),
+        ("ray_field", C.POINTER(C.c_int32)), ("ray_event", C.POINTER(C.c_double)),
+        ("inv", C.POINTER(GridStruct)), ("step_km", C.c_double), ("tables_out", C.POINTER(C.c_float)),
+    ]
+
+
+class ServeResult(C.Structure):
+    """ts_serve_result."""
+
+    _fields_ = [
+        ("status", C.c_int32), ("n_fields", C.c_int32), ("rounds", C.c_int32 * 2), ("queue_ms", C.c_double),
+        ("latency_ms", C.c_double), ("rows", C.c_void_p), ("error", C.c_char * 160),
+    ]
+
+
+class ServeStats(C.Structure):
+    """ts_serve_stats_t."""
+
+    _fields_ = [
+        ("epochs", C.c_int64), ("fields_done", C.c_int64), ("requests_done", C.c_int64),
+        ("node_updates", C.c_int64), ("device_ms", C.c_double), ("bytes_in_use", C.c_double),
+        ("peak_bytes", C.c_double), ("queued", C.c_int32), ("in_flight", C.c_int32),
+    ]
+
+
 _gp = _P(GridStruct)
 SIGNATURES = {
+    "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
+    "ts_serve_destroy": (None, [_vp]),
+    "ts_serve_last_error": (C.c_char_p, [_vp]),
+    "ts_serve_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _ip]),
+    "ts_serve_submit": (C.c_int, [_vp, _P(ServeRequest), _P(C.c_int64)]),
+    "ts_serve_wait": (C.c_int, [_vp, C.c_int64, _d, _P(ServeResult)]),
+    "ts_serve_stats": (C.c_int, [_vp, _P(ServeStats)]),
     "ts_cuda_create": (C.c_int, [_i32, _P(_vp)]),
     "ts_cuda_destroy": (None, [_vp]),
     "ts_last_error": (C.c_char_p, [_vp]),

@@ -234,3 +234,108 @@ def config2(n_sources: int = 200, seed: int = 3, variable_share: float = 0.5,
         src.append((lon, lat, fz * g.max_depth_km))
         hs.append(h)
     return GridBatch("config2", grids, slow, np.asarray(src), np.asarray(hs))
+
+
+@dataclass
+class ServeModel:
+    """A resident model of the serving load: grid, slowness (phases, n) and node spacing."""
+
+    name: str
+    grid: GridDef
+    slowness: np.ndarray
+    h_km: float
+
+
+@dataclass
+class ServeRequestSpec:
+    """One request of the serving load: arrival time (s), kind, model, phase, the stations its
+    fields are seeded at (n_fields, 3) and its rays: events (n_rays, 3) and the field of each."""
+
+    t: float
+    kind: str
+    model: str
+    phase: int
+    stations: np.ndarray
+    events: np.ndarray
+    ray_field: np.ndarray
+
+
+def _surface_points(g: GridDef, h: float, n: int, rng) -> np.ndarray:
+    span_x, span_y = (g.nx - 1) * h, (g.ny - 1) * h
+    xy = rng.uniform(0, 1, size=(n, 2)) * [span_x, span_y]
+    lon, lat = km_to_geo(g, xy[:, 0], xy[:, 1], h)
+    return np.stack([lon, lat, np.zeros(n)], axis=1)
+
+
+def _volume_points(g: GridDef, h: float, n: int, zmin: float, zmax: float, rng) -> np.ndarray:
+    span_x, span_y = (g.nx - 1) * h, (g.ny - 1) * h
+    x, y, z = rng.uniform(0, span_x, n), rng.uniform(0, span_y, n), rng.uniform(zmin, zmax, n)
+    lon, lat = km_to_geo(g, x, y, h)
+    return np.stack([lon, lat, z], axis=1)
+
+
+def spikes(grid: GridDef, h_km: float, cell_km: float, amplitude_percent: float, n: int, rng) -> np.ndarray:
+    """Spike-test perturbation (ResolutionTests.cs:62-82 spike branch in spirit): n isolated cubes
+    of cell_km at random cell positions, alternately +/− amplitude, fractional, grid order."""
+    x = np.arange(grid.nx) * h_km
+    y = np.arange(grid.ny) * h_km
+    z = grid.depth() - grid.min_depth_km
+    out = np.zeros(grid.shape)
+    for q in range(n):
+        cx, cy, cz = (rng.integers(0, max(1, int(v // cell_km))) * cell_km for v in (x[-1], y[-1], z[-1]))
+        sign = 1 if q % 2 == 0 else -1
+        mz = (z >= cz) & (z < cz + cell_km)
+        my = (y >= cy) & (y < cy + cell_km)
+        mx = (x >= cx) & (x < cx + cell_km)
+        out[np.ix_(mz, my, mx)] = sign * amplitude_percent / 100
+    return out.reshape(-1)
+
+
+def config3_models() -> dict:
+    """Resident models of the serving load: the 121×121×61 forward model of the inversion step
+    (config 1, P and S); two 81×81×41 resolution-test models at 1 km (Vp(z) times a ±5 %
+    checkerboard and ±5 % spikes of 8 km cells); a 161×161×81 relocation model at 0.5 km (Vp(z),
+    Vs = Vp/1.73)."""
+    p1 = config1()
+    models = {"forward121": ServeModel("forward121", p1.grid, p1.slowness, 0.5)}
+    g81 = regular_grid(81, 81, 41, 1.0)
+    v81 = vp_linear(g81)
+    models["checker81"] = ServeModel("checker81", g81, (1 / (v81 * (1 + checkerboard(g81, 8, 8, 5))))[None, :], 1.0)
+    rng = np.random.default_rng(4)
+    models["spike81"] = ServeModel("spike81", g81, (1 / (v81 * (1 + spikes(g81, 1.0, 8, 5, 12, rng))))[None, :], 1.0)
+    g161 = regular_grid(161, 161, 81, 0.5)
+    v161 = vp_linear(g161)
+    models["reloc161"] = ServeModel("reloc161", g161, np.stack([1 / v161, 1.73 / v161]), 0.5)
+    return models
+
+
+def config3_stream(models: dict, rate: float = 200.0, duration: float = 60.0, seed: int = 4) -> list:
+    """The serving load: Poisson arrivals at `rate` per second for `duration` seconds, mixed 60 %
+    single-station eikonal-plus-rays requests on forward121 (P or S, 20–150 rays from events at
+    2–20 km), 25 % resolution-test batches of 25 fields on checker81 or spike81 (no rays), 15 %
+    relocation requests on reloc161 (one station field, 10–40 rays from events at 2–25 km). One
+    generator, stream seed 4."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        u = rng.uniform()
+        if u < 0.60:
+            m = models["forward121"]
+            nr = int(rng.integers(20, 151))
+            out.append(ServeRequestSpec(t, "eikonal+rays", m.name, int(rng.integers(0, 2)),
+                                        _surface_points(m.grid, m.h_km, 1, rng),
+                                        _volume_points(m.grid, m.h_km, nr, 2, 20, rng), np.zeros(nr, np.int32)))
+        elif u < 0.85:
+            m = models["checker81" if rng.uniform() < 0.5 else "spike81"]
+            out.append(ServeRequestSpec(t, "resolution", m.name, 0, _surface_points(m.grid, m.h_km, 25, rng),
+                                        np.zeros((0, 3)), np.zeros(0, np.int32)))
+        else:
+            m = models["reloc161"]
+            nr = int(rng.integers(10, 41))
+            out.append(ServeRequestSpec(t, "relocation", m.name, int(rng.integers(0, 2)),
+                                        _surface_points(m.grid, m.h_km, 1, rng),
+                                        _volume_points(m.grid, m.h_km, nr, 2, 25, rng), np.zeros(nr, np.int32)))
+    return out
