@@ -215,6 +215,8 @@ typedef struct ts_serve_result {
 typedef struct ts_serve_stats_t {
     int64_t epochs, fields_done, requests_done, node_updates;
     double device_ms;             /* engine kernel time */
+    double epoch_ms;              /* wall time of the epochs (kernel, its set-up and read-back) */
+    double complete_ms;           /* wall time of finishing requests (tables, rays, copies) */
     double bytes_in_use, peak_bytes;
     int32_t queued, in_flight;
 } ts_serve_stats_t;

@@ -17,7 +17,7 @@ STRUCTS = {
     "ts_eik_stats": (L.EikStats, ["node_updates", "kernel_ms"]),
     "ts_serve_request": (L.ServeRequest, ["n_rays", "seed_offsets", "inv", "step_km", "tables_out"]),
     "ts_serve_result": (L.ServeResult, ["queue_ms", "rows", "error"]),
-    "ts_serve_stats_t": (L.ServeStats, ["device_ms", "queued", "in_flight"]),
+    "ts_serve_stats_t": (L.ServeStats, ["device_ms", "complete_ms", "queued", "in_flight"]),
 }
 
 

@@ -82,7 +82,8 @@ class ServeStats(C.Structure):
 
     _fields_ = [
         ("epochs", C.c_int64), ("fields_done", C.c_int64), ("requests_done", C.c_int64),
-        ("node_updates", C.c_int64), ("device_ms", C.c_double), ("bytes_in_use", C.c_double),
+        ("node_updates", C.c_int64), ("device_ms", C.c_double), ("epoch_ms", C.c_double),
+        ("complete_ms", C.c_double), ("bytes_in_use", C.c_double),
         ("peak_bytes", C.c_double), ("queued", C.c_int32), ("in_flight", C.c_int32),
     ]
 

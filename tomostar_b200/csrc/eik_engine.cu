@@ -134,34 +134,44 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     std::vector<int> sc_field, init_list;
     std::vector<int32_t> sc_node;
     std::vector<double> sc_t;
+    constexpr int kShape = BX | (BY << 8) | (BZ << 16);
     for (int f = 0; f < nf; f++) {
-        const EngineField& ef = *fl[f];
+        EngineField& ef = *fl[f];
         const host::Grid& g = *grids[ef.grid];
         const int gi = ef.grid;
-        if (!ef.initialized) init_list.push_back(f);
-        std::vector<std::pair<int, int>> tl;  // (tile, local)
-        for (size_t q = 0; q < ef.seed_idx.size(); q++) {
-            int node = ef.seed_idx[q];
-            int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
-            int tid = ((k / BZ) * ty[gi] + j / BY) * tx[gi] + i / BX;
-            int loc = ((k % BZ) * BY + j % BY) * BX + i % BX;
-            tl.push_back({tid, loc});
-            if (!ef.initialized) {
+        if (!ef.initialized) {
+            init_list.push_back(f);
+            for (size_t q = 0; q < ef.seed_idx.size(); q++) {
                 sc_field.push_back(f);
-                sc_node.push_back(node);
+                sc_node.push_back(ef.seed_idx[q]);
                 sc_t.push_back(ef.seed_t[q]);
             }
         }
-        std::sort(tl.begin(), tl.end());
-        seed_begin[f] = int(st_tile.size());
-        for (size_t q = 0; q < tl.size(); q++) {
-            if (q == 0 || tl[q].first != tl[q - 1].first) {
-                st_tile.push_back(tl[q].first);
-                st_mask.resize(st_mask.size() + S::MW, 0u);
+        if (ef.seed_shape != kShape) {
+            std::vector<std::pair<int, int>> tl;  // (tile, local)
+            for (size_t q = 0; q < ef.seed_idx.size(); q++) {
+                int node = ef.seed_idx[q];
+                int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+                int tid = ((k / BZ) * ty[gi] + j / BY) * tx[gi] + i / BX;
+                int loc = ((k % BZ) * BY + j % BY) * BX + i % BX;
+                tl.push_back({tid, loc});
             }
-            st_mask[(st_tile.size() - 1) * S::MW + tl[q].second / 32] |= 1u << (tl[q].second % 32);
+            std::sort(tl.begin(), tl.end());
+            ef.seed_tiles.clear();
+            ef.seed_masks.clear();
+            for (size_t q = 0; q < tl.size(); q++) {
+                if (q == 0 || tl[q].first != tl[q - 1].first) {
+                    ef.seed_tiles.push_back(tl[q].first);
+                    ef.seed_masks.resize(ef.seed_masks.size() + S::MW, 0u);
+                }
+                ef.seed_masks[(ef.seed_tiles.size() - 1) * S::MW + tl[q].second / 32] |= 1u << (tl[q].second % 32);
+            }
+            ef.seed_shape = kShape;
         }
-        seed_count[f] = int(st_tile.size()) - seed_begin[f];
+        seed_begin[f] = int(st_tile.size());
+        st_tile.insert(st_tile.end(), ef.seed_tiles.begin(), ef.seed_tiles.end());
+        st_mask.insert(st_mask.end(), ef.seed_masks.begin(), ef.seed_masks.end());
+        seed_count[f] = int(ef.seed_tiles.size());
     }
     size_t o_seed_tile = A.add(sizeof(int) * std::max<size_t>(1, st_tile.size()));
     std::copy(st_tile.begin(), st_tile.end(), A.at<int>(o_seed_tile));

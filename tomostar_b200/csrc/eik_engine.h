@@ -27,6 +27,11 @@ struct EngineField {
     void* state = nullptr;              // its FieldState
     void* block = nullptr;              // its own allocation (serving), freed by engine_field_free
     bool initialized = false;           // +inf, all due and seeds written
+    // Its seed tiles (ascending tile id) with their fixed-node masks, for the tile shape `seed_shape`
+    // (BX | BY << 8 | BZ << 16); kept between epochs.
+    int seed_shape = -1;
+    std::vector<int> seed_tiles;
+    std::vector<uint32_t> seed_masks;
     // results
     int status = 0;                     // 1 settled, 2 refused at the cap, 0 running
     int rounds[2] = {0, 0};

@@ -34,6 +34,7 @@ struct TraceArgs {
     RGrid fwd, inv;
     const float* tables;
     int64_t table_n;
+    const float* const* table_ptr;  // when set: table t at table_ptr[t] (tables in separate buffers)
     const double* table_station;  // 3 per table
     const int* table_of;          // per ray
     const double* events;         // 3 per ray
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     if (r >= a.nrays) return;
     const int ray = a.ray0 + r;
     const int tab = a.table_of[ray];
-    const float* tb = a.tables + int64_t(tab) * a.table_n;
+    const float* tb = a.table_ptr ? a.table_ptr[tab] : a.tables + int64_t(tab) * a.table_n;
     const RGrid& g = a.fwd;
     const double st_lon = a.table_station[3 * tab], st_lat = a.table_station[3 * tab + 1];
     const double st_dep = fmin(fmax(a.table_station[3 * tab + 2], g.min_dep), g.dep_last);
@@ -330,21 +331,22 @@ struct ts_rows {
     float* len = nullptr;
     double* tcg = nullptr;    // device, 4 per row
     uint8_t* ok = nullptr;
+    // Stream-ordered frees: no device-wide synchronisation while other work runs (serving).
     ~ts_rows() {
-        cudaFree(row_ptr);
-        cudaFree(col);
-        cudaFree(len);
-        cudaFree(tcg);
-        cudaFree(ok);
+        cudaStream_t s = ctx ? ctx->stream : nullptr;
+        for (void* p : {static_cast<void*>(row_ptr), static_cast<void*>(col), static_cast<void*>(len),
+                        static_cast<void*>(tcg), static_cast<void*>(ok)})
+            if (p) cudaFreeAsync(p, s);
     }
 };
 
 namespace ts {
 namespace rays {
 
-int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
-                    const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
-                    const double* events_host, double step_km, ts_rows** out, RayStats* st) {
+static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, const float* const* table_ptrs_host,
+                      int n_tables, const double* table_station_host, const host::Grid& inv, int n_rays,
+                      const int32_t* table_of_host, const double* events_host, double step_km, ts_rows** out,
+                      RayStats* st) {
     cudaStream_t s = ctx->stream;
     const int64_t n = fwd.count();
     for (int a = 0; a < n_rays; a++)
@@ -358,9 +360,9 @@ int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev,
         delete rows;
         return code;
     };
-    if (cudaMalloc(&rows->row_ptr, sizeof(int) * (n_rays + 1)) != cudaSuccess ||
-        cudaMalloc(&rows->tcg, sizeof(double) * 4 * std::max(1, n_rays)) != cudaSuccess ||
-        cudaMalloc(&rows->ok, std::max(1, n_rays)) != cudaSuccess) {
+    if (cudaMallocAsync(reinterpret_cast<void**>(&rows->row_ptr), sizeof(int) * (n_rays + 1), s) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&rows->tcg), sizeof(double) * 4 * std::max(1, n_rays), s) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&rows->ok), std::max(1, n_rays), s) != cudaSuccess) {
         cudaGetLastError();
         ctx->fail(TS_E_NOMEM, "row buffers");
         return bail(TS_E_NOMEM);
@@ -377,6 +379,13 @@ int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev,
     a.inv = make_rgrid(inv);
     a.tables = tables_dev;
     a.table_n = n;
+    a.table_ptr = nullptr;
+    if (table_ptrs_host) {
+        TS_BUF(ctx, d_ptrs, const float*, "rays.table_ptrs", std::max(1, n_tables));
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ptrs, table_ptrs_host, sizeof(const float*) * n_tables,
+                                         cudaMemcpyHostToDevice, s));
+        a.table_ptr = d_ptrs;
+    }
     a.table_station = d_station;
     a.table_of = d_table_of;
     a.events = d_events;
@@ -452,19 +461,18 @@ int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev,
                 want = std::max<int64_t>(want, 1024);
                 int* ncol = nullptr;
                 float* nlen = nullptr;
-                if (cudaMalloc(&ncol, sizeof(int) * want) != cudaSuccess ||
-                    cudaMalloc(&nlen, sizeof(float) * want) != cudaSuccess) {
+                if (cudaMallocAsync(reinterpret_cast<void**>(&ncol), sizeof(int) * want, s) != cudaSuccess ||
+                    cudaMallocAsync(reinterpret_cast<void**>(&nlen), sizeof(float) * want, s) != cudaSuccess) {
                     cudaGetLastError();
-                    cudaFree(ncol);
+                    if (ncol) cudaFreeAsync(ncol, s);
                     return bail(ctx->fail(TS_E_NOMEM, "CSR arrays"));
                 }
                 if (total > 0) {
                     cudaMemcpyAsync(ncol, rows->col, sizeof(int) * total, cudaMemcpyDeviceToDevice, s);
                     cudaMemcpyAsync(nlen, rows->len, sizeof(float) * total, cudaMemcpyDeviceToDevice, s);
-                    cudaStreamSynchronize(s);
                 }
-                cudaFree(rows->col);
-                cudaFree(rows->len);
+                if (rows->col) cudaFreeAsync(rows->col, s);
+                if (rows->len) cudaFreeAsync(rows->len, s);
                 rows->col = ncol;
                 rows->len = nlen;
                 csr_cap = want;
@@ -489,6 +497,74 @@ int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev,
     *out = rows;
     return TS_OK;
 }
+
+}  // namespace rays
+}  // namespace ts
+
+namespace ts {
+namespace rays {
+
+int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
+                    const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st) {
+    return trace_impl(ctx, fwd, tables_dev, nullptr, n_tables, table_station_host, inv, n_rays, table_of_host,
+                      events_host, step_km, out, st);
+}
+
+int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const std::vector<const float*>& tables, const double* table_station_host,
+                    const host::Grid& inv, int n_rays, const int32_t* table_of_host, const double* events_host,
+                    double step_km, ts_rows** out, RayStats* st) {
+    return trace_impl(ctx, fwd, nullptr, tables.data(), int(tables.size()), table_station_host, inv, n_rays,
+                      table_of_host, events_host, step_km, out, st);
+}
+
+int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begin, std::vector<ts_rows*>& parts) {
+    cudaStream_t s = ctx->stream;
+    std::vector<int> rp(all->n_rows + 1);
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(rp.data(), all->row_ptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost, s));
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    parts.assign(row_begin.size() - 1, nullptr);
+    for (size_t k = 0; k + 1 < row_begin.size(); k++) {
+        const int r0 = row_begin[k], r1 = row_begin[k + 1], n = r1 - r0;
+        const int64_t z0 = rp[r0], nnz = int64_t(rp[r1]) - rp[r0];
+        auto* p = new ts_rows();
+        p->ctx = ctx;
+        p->n_rows = n;
+        p->nnz = nnz;
+        std::vector<int> local(n + 1);
+        for (int q = 0; q <= n; q++) local[q] = int(rp[r0 + q] - z0);
+        auto fail = [&]() {
+            cudaGetLastError();
+            delete p;
+            for (auto*& q : parts) {
+                delete q;
+                q = nullptr;
+            }
+            return ctx->fail(TS_E_NOMEM, "row buffers");
+        };
+        if (cudaMallocAsync(reinterpret_cast<void**>(&p->row_ptr), sizeof(int) * (n + 1), s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&p->tcg), sizeof(double) * 4 * std::max(1, n), s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&p->ok), std::max(1, n), s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&p->col), sizeof(int) * std::max<int64_t>(1, nnz), s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&p->len), sizeof(float) * std::max<int64_t>(1, nnz), s) != cudaSuccess)
+            return fail();
+        // From pageable memory the copy has taken the source when the call returns.
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->row_ptr, local.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+        if (n) {
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->tcg, all->tcg + 4 * int64_t(r0), sizeof(double) * 4 * n,
+                                             cudaMemcpyDeviceToDevice, s));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->ok, all->ok + r0, size_t(n), cudaMemcpyDeviceToDevice, s));
+        }
+        if (nnz) {
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->col, all->col + z0, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->len, all->len + z0, sizeof(float) * nnz, cudaMemcpyDeviceToDevice, s));
+        }
+        parts[k] = p;
+    }
+    return TS_OK;
+}
+
+void free_rows(ts_rows* rows) { delete rows; }
 
 }  // namespace rays
 }  // namespace ts
@@ -540,10 +616,8 @@ int ts_rows_copy(ts_rows* rows, int32_t* row_ptr, int32_t* col, float* len, doub
 
 void ts_rows_free(ts_rows* rows) {
     if (!rows) return;
-    {
-        std::lock_guard<std::recursive_mutex> lk(rows->ctx->mu);
-        cudaSetDevice(rows->ctx->device);
-    }
+    std::lock_guard<std::recursive_mutex> lk(rows->ctx->mu);
+    cudaSetDevice(rows->ctx->device);
     delete rows;
 }
 

@@ -4,6 +4,8 @@
 #include "ctx.h"
 #include "host_geo.h"
 
+#include <vector>
+
 namespace ts {
 namespace rays {
 
@@ -17,6 +19,16 @@ struct RayStats {
 int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
                     const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
                     const double* events_host, double step_km, ts_rows** out, RayStats* st);
+
+// The same with each table in a buffer of its own (tables[t] on the device).
+int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const std::vector<const float*>& tables,
+                    const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st);
+
+// Cuts a result into consecutive row ranges [row_begin[k], row_begin[k+1]), each a result of its
+// own (stream-ordered copies on the context's stream).
+int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begin, std::vector<ts_rows*>& parts);
+void free_rows(ts_rows* rows);
 
 }  // namespace rays
 }  // namespace ts

@@ -81,15 +81,26 @@ struct ts_server {
     std::thread loop;
     bool stop = false;
     int64_t next_id = 1;
+    // What submit checks a request against, kept here so that submitting never waits for an epoch.
+    struct ModelInfo {
+        int n_phases;
+        int64_t count;
+        bool variable;
+    };
+    std::map<int, ModelInfo> model_info;
     // statistics
     int64_t epochs = 0, fields_done = 0, requests_done = 0, node_updates = 0;
-    double device_ms = 0;
+    double device_ms = 0, epoch_ms = 0, complete_ms = 0;
     std::string err;
 };
 
 namespace {
 
 using ts::eik::EngineField;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
 
 ts_grid coarsened(const ts_grid& g) {
     ts_grid c = g;
@@ -169,38 +180,115 @@ void admit(ts_server* sv) {
     }
 }
 
-// Tables, rays and copies of a request whose fields have all settled; frees its device block.
-int complete(ts_server* sv, ServeRequest* r) {
+// Tables, rays and copies of the requests whose fields have all stopped, as one batch: the tables
+// of every field, then the rays of all requests on one model traced together and cut into each
+// request's rows, then the copies the callers asked for, then one synchronisation. codes/errors
+// receive each request's outcome.
+void complete_batch(ts_server* sv, const std::vector<ServeRequest*>& reqs, std::vector<int>& codes,
+                    std::vector<std::string>& errors) {
     ts_ctx* ctx = sv->ctx;
-    const ts_ctx::Model& m = *ctx->models.at(r->model_id);
-    const ts::eik::FieldLayout L = ts::eik::field_layout(*m.grid, sv->tile, sv->precision);
-    const int64_t n = m.grid->count();
-    for (auto& ef : r->fields) {
-        r->rounds[0] = std::max(r->rounds[0], ef.rounds[0]);
-        r->rounds[1] = std::max(r->rounds[1], ef.rounds[1]);
-        if (ef.status != 1) return ctx->fail(TS_E_UNSETTLED, "sweeping not settled within the round cap");
+    codes.assign(reqs.size(), TS_OK);
+    errors.assign(reqs.size(), std::string());
+    auto fail = [&](size_t k, int rc) {
+        codes[k] = rc;
+        errors[k] = ctx->err;
+    };
+    for (size_t k = 0; k < reqs.size(); k++) {
+        ServeRequest* r = reqs[k];
+        const ts_ctx::Model& m = *ctx->models.at(r->model_id);
+        const ts::eik::FieldLayout L = ts::eik::field_layout(*m.grid, sv->tile, sv->precision);
+        bool settled = true;
+        for (auto& ef : r->fields) {
+            r->rounds[0] = std::max(r->rounds[0], ef.rounds[0]);
+            r->rounds[1] = std::max(r->rounds[1], ef.rounds[1]);
+            settled = settled && ef.status == 1;
+        }
+        if (!settled) {
+            fail(k, ctx->fail(TS_E_UNSETTLED, "sweeping not settled within the round cap"));
+            continue;
+        }
+        for (int f = 0; f < r->n_fields && codes[k] == TS_OK; f++) {
+            int rc = ts::eik::field_to_dense_f32_device(ctx, *m.grid, L, r->fields[f].T, sv->precision,
+                                                        r->tables_dev + size_t(f) * m.grid->count(), ctx->stream);
+            if (rc) fail(k, rc);
+        }
     }
-    for (int f = 0; f < r->n_fields; f++) {
-        int rc = ts::eik::field_to_dense_f32_device(ctx, *m.grid, L, r->fields[f].T, sv->precision,
-                                                    r->tables_dev + size_t(f) * n, ctx->stream);
-        if (rc) return rc;
+    // Rays: requests on one model with the default inversion grid and step form one trace.
+    std::map<int, std::vector<size_t>> groups;
+    std::vector<size_t> singles;
+    for (size_t k = 0; k < reqs.size(); k++) {
+        if (codes[k] != TS_OK || reqs[k]->n_rays == 0) continue;
+        if (!reqs[k]->has_inv && !(reqs[k]->step_km > 0)) groups[reqs[k]->model_id].push_back(k);
+        else singles.push_back(k);
     }
-    if (r->n_rays > 0) {
+    for (auto& grp : groups) {
+        const ts_ctx::Model& m = *ctx->models.at(grp.first);
+        const int64_t n = m.grid->count();
+        std::vector<const float*> tables;
+        std::vector<double> origin, events;
+        std::vector<int32_t> table_of;
+        std::vector<int> row_begin{0};
+        for (size_t k : grp.second) {
+            ServeRequest* r = reqs[k];
+            const int base = int(tables.size());
+            for (int f = 0; f < r->n_fields; f++) tables.push_back(r->tables_dev + size_t(f) * n);
+            origin.insert(origin.end(), r->origin.begin(), r->origin.end());
+            for (int a = 0; a < r->n_rays; a++) table_of.push_back(base + r->ray_field[a]);
+            events.insert(events.end(), r->ray_event.begin(), r->ray_event.end());
+            row_begin.push_back(row_begin.back() + r->n_rays);
+        }
+        ts_grid invdef = coarsened(m.def);
+        ts::host::Grid inv(invdef);
+        const double step = 0.5 * std::min(m.grid->min_spacing_km(), inv.min_spacing_km());  // RayKernels.cs:62
+        ts_rows* all = nullptr;
+        ts::rays::RayStats rst;
+        int rc = ts::rays::trace_on_device(ctx, *m.grid, tables, origin.data(), inv, int(table_of.size()),
+                                           table_of.data(), events.data(), step, &all, &rst);
+        std::vector<ts_rows*> parts;
+        if (rc == TS_OK) rc = ts::rays::split_rows(ctx, all, row_begin, parts);
+        if (all) ts::rays::free_rows(all);
+        for (size_t q = 0; q < grp.second.size(); q++) {
+            if (rc) fail(grp.second[q], rc);
+            else reqs[grp.second[q]]->rows = parts[q];
+        }
+    }
+    for (size_t k : singles) {
+        ServeRequest* r = reqs[k];
+        const ts_ctx::Model& m = *ctx->models.at(r->model_id);
         ts_grid invdef = r->has_inv ? r->inv : coarsened(m.def);
         if (r->has_inv && !r->inv_depth.empty()) invdef.depth_km = r->inv_depth.data();
-        if (const char* bad = ts::host::Grid::validate(invdef)) return ctx->fail(TS_E_ARG, bad);
+        if (const char* bad = ts::host::Grid::validate(invdef)) {
+            fail(k, ctx->fail(TS_E_ARG, bad));
+            continue;
+        }
         ts::host::Grid inv(invdef);
         double step = r->step_km > 0 ? r->step_km : 0.5 * std::min(m.grid->min_spacing_km(), inv.min_spacing_km());
         ts::rays::RayStats rst;
         int rc = ts::rays::trace_on_device(ctx, *m.grid, r->tables_dev, r->n_fields, r->origin.data(), inv, r->n_rays,
                                            r->ray_field.data(), r->ray_event.data(), step, &r->rows, &rst);
-        if (rc) return rc;
+        if (rc) fail(k, rc);
     }
-    if (r->tables_out)
-        TS_CUDA_TRY(ctx, cudaMemcpyAsync(r->tables_out, r->tables_dev, sizeof(float) * size_t(n) * r->n_fields,
-                                         cudaMemcpyDeviceToHost, ctx->stream));
-    TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    return TS_OK;
+    for (size_t k = 0; k < reqs.size(); k++) {
+        ServeRequest* r = reqs[k];
+        if (codes[k] != TS_OK || !r->tables_out) continue;
+        const int64_t n = ctx->models.at(r->model_id)->grid->count();
+        cudaError_t e = cudaMemcpyAsync(r->tables_out, r->tables_dev, sizeof(float) * size_t(n) * r->n_fields,
+                                        cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            codes[k] = TS_E_CUDA;
+            errors[k] = cudaGetErrorString(e);
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        for (size_t k = 0; k < reqs.size(); k++)
+            if (codes[k] == TS_OK) {
+                codes[k] = TS_E_CUDA;
+                errors[k] = cudaGetErrorString(e);
+            }
+    }
 }
 
 void release(ts_server* sv, ServeRequest* r) {
@@ -255,6 +343,7 @@ void serve_loop(ts_server* sv) {
         }
         ts_eik_stats st{};
         int rc = TS_OK;
+        const auto te0 = Clock::now();
         if (!fl.empty()) {
             rc = sv->precision == TS_PRECISION_F64
                      ? ts::eik::engine_epoch<double>(ctx, grids, metrics, fl, ts::kSettleTolerance, wake_rel, sv->tile,
@@ -262,32 +351,37 @@ void serve_loop(ts_server* sv) {
                      : ts::eik::engine_epoch<float>(ctx, grids, metrics, fl, ts::kSettleTolerance, wake_rel, sv->tile,
                                                     sv->rounds_per_epoch, &st, ctx->stream);
         }
-        std::vector<ServeRequest*> still;
-        std::vector<std::pair<ServeRequest*, std::pair<int, std::string>>> done;
+        const auto te1 = Clock::now();
+        std::vector<ServeRequest*> still, finished;
         for (ServeRequest* r : sv->running) {
-            bool settled = true;
-            for (auto& ef : r->fields) settled = settled && ef.status != 0;
-            if (rc != TS_OK) {
-                done.push_back({r, {rc, ctx->err}});
-            } else if (settled) {
-                int c = complete(sv, r);
-                done.push_back({r, {c, c ? ctx->err : std::string()}});
-            } else {
-                still.push_back(r);
-            }
+            bool stopped = true;
+            for (auto& ef : r->fields) stopped = stopped && ef.status != 0;
+            if (rc != TS_OK || stopped) finished.push_back(r);
+            else still.push_back(r);
         }
+        std::vector<int> codes;
+        std::vector<std::string> errors;
+        if (rc != TS_OK) {
+            codes.assign(finished.size(), rc);
+            errors.assign(finished.size(), ctx->err);
+        } else {
+            complete_batch(sv, finished, codes, errors);
+        }
+        const auto te2 = Clock::now();
         std::lock_guard<std::mutex> lk(sv->mu);
         sv->epochs++;
         sv->device_ms += st.kernel_ms;
+        sv->epoch_ms += ms_between(te0, te1);
+        sv->complete_ms += ms_between(te1, te2);
         sv->node_updates += st.node_updates;
         sv->running.swap(still);
-        for (auto& d : done) {
-            release(sv, d.first);
-            finish(sv, d.first, d.second.first, d.second.second);
-            sv->fields_done += d.first->n_fields;
+        for (size_t k = 0; k < finished.size(); k++) {
+            release(sv, finished[k]);
+            finish(sv, finished[k], codes[k], errors[k]);
+            sv->fields_done += finished[k]->n_fields;
             sv->requests_done++;
         }
-        if (!done.empty()) sv->cv_done.notify_all();
+        if (!finished.empty()) sv->cv_done.notify_all();
     }
     // Shutdown: every request still queued or in flight ends with an error.
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -301,10 +395,6 @@ void serve_loop(ts_server* sv) {
     sv->pending.clear();
     cudaStreamSynchronize(ctx->stream);
     sv->cv_done.notify_all();
-}
-
-double ms_between(Clock::time_point a, Clock::time_point b) {
-    return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
 }  // namespace
@@ -367,8 +457,15 @@ int ts_serve_model_put(ts_server* sv, const ts_grid* grid, const double* slownes
     std::lock_guard<std::recursive_mutex> cl(sv->ctx->mu);
     cudaSetDevice(sv->ctx->device);
     int rc = ts::eik::model_put(sv->ctx, grid, slowness, n_phases, sv->precision, model_id);
-    if (rc) sv->err = sv->ctx->err;
-    return rc;
+    if (rc) {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->err = sv->ctx->err;
+        return rc;
+    }
+    const ts_ctx::Model& m = *sv->ctx->models.at(*model_id);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->model_info[*model_id] = ts_server::ModelInfo{m.n_phases, m.grid->count(), m.grid->variable};
+    return TS_OK;
 }
 
 int ts_serve_submit(ts_server* sv, const ts_serve_request* q, int64_t* request_id) {
@@ -381,23 +478,24 @@ int ts_serve_submit(ts_server* sv, const ts_serve_request* q, int64_t* request_i
     r->phase = q->phase;
     r->n_fields = q->n_fields;
     r->n_rays = q->n_rays;
+    const auto t_submit = Clock::now();
     int64_t n = 0;
     {
-        std::lock_guard<std::recursive_mutex> cl(sv->ctx->mu);
-        auto it = sv->ctx->models.find(q->model_id);
-        if (it == sv->ctx->models.end()) {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        auto it = sv->model_info.find(q->model_id);
+        if (it == sv->model_info.end()) {
             sv->err = "unknown model";
             return TS_E_ARG;
         }
-        if (q->phase < 0 || q->phase >= it->second->n_phases) {
+        if (q->phase < 0 || q->phase >= it->second.n_phases) {
             sv->err = "phase out of range";
             return TS_E_ARG;
         }
-        if (q->n_rays > 0 && it->second->grid->variable) {
+        if (q->n_rays > 0 && it->second.variable) {
             sv->err = "rays need uniform grids";
             return TS_E_ARG;
         }
-        n = it->second->grid->count();
+        n = it->second.count;
     }
     for (int f = 0; f < q->n_fields; f++) {
         std::map<int32_t, double> merged;  // as TrySolve takes seed sets (EikonalOpenCl.cs:147-163)
@@ -407,6 +505,7 @@ int ts_serve_submit(ts_server* sv, const ts_serve_request* q, int64_t* request_i
             if (it == merged.end() || q->seed_time[s] < it->second) merged[q->seed_index[s]] = q->seed_time[s];
         }
         if (merged.empty()) {
+            std::lock_guard<std::mutex> lk(sv->mu);
             sv->err = "no seed nodes for field " + std::to_string(f);
             return TS_E_NOSEEDS;
         }
@@ -423,6 +522,7 @@ int ts_serve_submit(ts_server* sv, const ts_serve_request* q, int64_t* request_i
     if (q->n_rays > 0) {
         for (int a = 0; a < q->n_rays; a++)
             if (q->ray_field[a] < 0 || q->ray_field[a] >= q->n_fields) {
+                std::lock_guard<std::mutex> lk(sv->mu);
                 sv->err = "ray_field out of range";
                 return TS_E_ARG;
             }
@@ -439,7 +539,7 @@ int ts_serve_submit(ts_server* sv, const ts_serve_request* q, int64_t* request_i
     }
     r->step_km = q->step_km;
     r->tables_out = q->tables_out;
-    r->t_submit = Clock::now();
+    r->t_submit = t_submit;
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->stop) return TS_E_CANCELLED;
     r->id = sv->next_id++;
@@ -482,6 +582,8 @@ int ts_serve_stats(ts_server* sv, ts_serve_stats_t* out) {
     out->requests_done = sv->requests_done;
     out->node_updates = sv->node_updates;
     out->device_ms = sv->device_ms;
+    out->epoch_ms = sv->epoch_ms;
+    out->complete_ms = sv->complete_ms;
     out->bytes_in_use = double(sv->in_use);
     out->peak_bytes = double(sv->peak_use);
     out->queued = int32_t(sv->pending.size());
