@@ -8,8 +8,12 @@ S fields). `value` is fields/s with the velocity model resident in HBM and the f
 device; `e2e` is the same job through the C-ABI entry point a host calls (ts_eik_solve: slowness and
 seeds from host memory, float32 tables read back into pinned host memory). Under torchrun every rank
 solves its own job of 800 fields (different stations; weak scaling, no collective on the data path);
-rank 0 prints one JSON line with the max-over-ranks time. `--impl reference` times the reference's
-CPU solver (fast marching, restated in oracle/) on the host cores on a bounded sample of the job.
+rank 0 prints one JSON line with the max-over-ranks time. At N = 1 the line also carries the
+serving load (`serving`: Poisson arrivals at 200 requests/s of mixed eikonal, ray and resolution
+requests on three grid sizes, p50/p99 latency and fields/s). `--impl reference` times the
+reference's CPU solver (fast marching, restated in oracle/) on the host cores on a bounded sample of
+the job. Fields are computed in FP64 (fast mode: within 1e-10 relative of the reference's sweeping)
+and delivered as float32 tables (the .qttb rounding, within 6e-8 relative).
 """
 from __future__ import annotations
 
@@ -27,7 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "travel-time fields/s (FP64 sweeping, float32 tables; err vs FP64 oracle <= 1e-10 rel)"
+METRIC = "travel-time fields/s + p99 solve latency, batched vs plain GPU, err\u22642e-5 rel"
 UNIT = "fields/s"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -113,13 +117,29 @@ def barrier(dist):
 
 
 def max_over_ranks(dist, local, x: float) -> float:
+    """The largest x over the ranks (a device tensor over NCCL, a host one over gloo)."""
     if dist is None:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_problem(rank: int):
+    """Weak scaling with no collective on the data path: rank r solves its own job of the same shape
+    (the workload generated with seed 5 + r: its own stations, events and velocity bodies)."""
+    from tomostar_b200 import synthetic as syn
+
+    return syn.config4(seed=5 + rank)
+
+
+def job_throughput(dist, local, world: int, fields_per_rank_step: int, steps: int, dev_ms: float):
+    """Whole-job fields/s: every rank's fields over the slowest rank's device time."""
+    dev_max = max_over_ranks(dist, local, dev_ms)
+    return fields_per_rank_step * world * steps / (dev_max / 1e3), dev_max
 
 
 def cpu_fmm_sample(problem, n_fields: int, threads: int):
@@ -229,9 +249,7 @@ def run_ours(args, problem_fn):
     t_wall = time.perf_counter() - t_wall
     clk = clocks.stop()
     barrier(dist)
-    dev_max = max_over_ranks(dist, local, dev)
-    fields_total = 2 * n_st * world * args.steps
-    value = fields_total / (dev_max / 1e3)
+    value, dev_max = job_throughput(dist, local, world, 2 * n_st, args.steps, dev)
 
     # Roofline of the sweeping kernel: algorithmic bytes per node update (FP64: the node's time read
     # and written, its slowness read = 24 B) over the kernel's event time.
@@ -296,6 +314,16 @@ def run_ours(args, problem_fn):
         cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{threads} of 800 fields, fast marching one field per thread (oracle/oracle.cpp)"}
 
+    # The serving load (Poisson stream of mixed requests) on one GPU, after the batch job's buffers
+    # are released; at N = 1 only (the scaling runs measure the batch job).
+    solver.close()
+    serving = None
+    if world == 1 and not args.no_serving:
+        from tomostar_b200.serve_load import run as serve_run
+
+        serving = serve_run(seconds=args.serve_seconds, rate=200.0, tile=args.serve_tile,
+                            rounds_per_epoch=args.serve_rounds, budget_bytes=120e9, device=local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -318,11 +346,11 @@ def run_ours(args, problem_fn):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "plain_gpu": plain,
+            "serving": serving,
             "node_updates_per_step": updates // args.steps,
             "wall_s_timed": t_wall,
         }
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -341,15 +369,15 @@ def main():
     ap.add_argument("--no-baselines", action="store_true")
     ap.add_argument("--fields", type=int, default=0, help="stations per step (default all 400; fewer = a small case)")
     ap.add_argument("--verbose", action="store_true", help="per-launch statistics on stderr")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-load measurement")
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-tile", type=int, default=2)
+    ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
     args = ap.parse_args()
-    from tomostar_b200 import synthetic as syn
-
-    def problem(rank):
-        return syn.config4(seed=5 + rank)
 
     if args.impl == "reference":
-        return run_reference(args, problem)
-    return run_ours(args, problem)
+        return run_reference(args, rank_problem)
+    return run_ours(args, rank_problem)
 
 
 if __name__ == "__main__":
