@@ -154,6 +154,10 @@ int ts_cuda_selftest(ts_ctx* ctx, int32_t precision, double* rel_err, char* msg,
  * shapes and returns how many exist. No reference counterpart (the OpenCL kernel is untiled). */
 int32_t ts_engine_shapes(int32_t* shapes, int32_t cap);
 /* Selects the engine's tile shape for one precision on this context (the autotuner's knob). */
+/* Engine scheduler: 0 = all fields step through the tile diagonals together (one grid-wide barrier
+ * per diagonal); 1 = flow: each field advances on its own through a shared tile queue (no barrier).
+ * Both give the same fields. No reference counterpart. */
+int ts_engine_set_scheduler(ts_ctx* ctx, int32_t scheduler);
 int ts_engine_set_tile(ts_ctx* ctx, int32_t precision, int32_t shape_id);
 
 /* Many fields on grids of uneven size in one engine launch (the reference batches only fields of one
@@ -220,8 +224,8 @@ typedef struct ts_serve_stats_t {
     double bytes_in_use, peak_bytes;
     int32_t queued, in_flight;
 } ts_serve_stats_t;
-int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, double hbm_budget_bytes,
-                    int32_t rounds_per_epoch, ts_server** out);
+int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, int32_t scheduler,
+                    double hbm_budget_bytes, int32_t rounds_per_epoch, ts_server** out);
 void ts_serve_destroy(ts_server* server);
 const char* ts_serve_last_error(ts_server* server);
 int ts_serve_model_put(ts_server* server, const ts_grid* grid, const double* slowness, int32_t n_phases,

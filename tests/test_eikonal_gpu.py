@@ -302,3 +302,40 @@ def test_fast_mode_full_size_field_within_1e10(solver):
     t32 = solver.solve(p.grid, p.slowness[1], seeds, mode=L.MODE_FAST,
                        output=np.empty((1, p.grid.count), np.float32), precision=64)
     assert rel_err(t32[0].astype(np.float64), exact[0]) <= 2e-5
+
+
+@pytest.mark.parametrize("mode", [L.MODE_ENGINE, L.MODE_FAST])
+def test_flow_scheduler_all_tile_shapes(solver, mode):
+    """The flow scheduler (fields advance on their own through a shared tile queue, no grid-wide
+    barrier) gives the same fields as the lockstep one: bitwise vs Relax (exact mode) or vs the
+    oracle's fast-mode rule, for every tile shape, several fields of one grid at once."""
+    g, s, seeds = hetero_case(37, 29, 19, seed=14, nsrc=4)
+    og = O.Grid.of(g)
+    if mode == L.MODE_ENGINE:
+        want = np.stack([O.relax(og, s, si, st)[0] for si, st in seeds])
+    else:
+        want = np.stack([O.relax_wake(og, s, si, st, WAKE, causal=True)[0] for si, st in seeds])
+    lib = L.load()
+    try:
+        assert lib.ts_engine_set_scheduler(solver.handle, 1) == 0
+        for sid, bx, by, bz in L.engine_shapes():
+            assert lib.ts_engine_set_tile(solver.handle, 64, sid) == 0
+            out = solver.solve(g, s, seeds, precision=64, mode=mode)
+            assert np.array_equal(out, want), f"shape {bx}x{by}x{bz}"
+    finally:
+        lib.ts_engine_set_scheduler(solver.handle, 0)
+        lib.ts_engine_set_tile(solver.handle, 64, 0)
+
+
+def test_flow_scheduler_config1_batch(solver):
+    """A batch of config-1 fields (P and S) under the flow scheduler equals the lockstep one."""
+    p = syn.config1()
+    seeds = [point_source(p.grid, p.slowness[0], *p.stations[q]) for q in range(6)]
+    lib = L.load()
+    a = solver.solve(p.grid, p.slowness[0], seeds, precision=64, mode=L.MODE_FAST)
+    try:
+        assert lib.ts_engine_set_scheduler(solver.handle, 1) == 0
+        b = solver.solve(p.grid, p.slowness[0], seeds, precision=64, mode=L.MODE_FAST)
+    finally:
+        lib.ts_engine_set_scheduler(solver.handle, 0)
+    assert np.array_equal(a, b)

@@ -63,6 +63,21 @@ def test_multi_grid_fp64_bitwise_all_tile_shapes(solver, batch):
         lib.ts_engine_set_tile(solver.handle, 64, 0)
 
 
+@pytest.mark.parametrize("mode", [L.MODE_ENGINE, L.MODE_FAST])
+def test_multi_grid_flow_scheduler(solver, batch, mode):
+    """Uneven and variable grids under the flow scheduler: each field advances on its own."""
+    b, seeds = batch
+    lib = L.load()
+    try:
+        L.check(lib.ts_engine_set_scheduler(solver.handle, 1), solver)
+        fields = solver.solve_multi(b.grids, b.slowness, list(range(len(b.grids))), seeds, mode=mode, precision=64)
+    finally:
+        lib.ts_engine_set_scheduler(solver.handle, 0)
+    wake = None if mode == L.MODE_ENGINE else L.WAKE_REL
+    for q, (g, s) in enumerate(zip(b.grids, b.slowness)):
+        assert np.array_equal(fields[q], oracle_field(g, s, seeds[q], wake)), f"grid {q}"
+
+
 def test_multi_grid_shared_grids_and_float32_tables(solver, batch):
     """Several fields per grid (field_grid repeats grids), in mixed order; float32 output is the
     float32 rounding of the FP64 field."""

@@ -90,7 +90,7 @@ class ServeStats(C.Structure):
 
 _gp = _P(GridStruct)
 SIGNATURES = {
-    "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
+    "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
     "ts_serve_destroy": (None, [_vp]),
     "ts_serve_last_error": (C.c_char_p, [_vp]),
     "ts_serve_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _ip]),
@@ -106,6 +106,7 @@ SIGNATURES = {
     "ts_eik_suggest_batch": (_i32, [_vp, _i64, _i32]),
     "ts_engine_shapes": (_i32, [_ip, _i32]),
     "ts_engine_set_tile": (C.c_int, [_vp, _i32, _i32]),
+    "ts_engine_set_scheduler": (C.c_int, [_vp, _i32]),
     "ts_eik_solve_multi": (C.c_int, [_vp, _i32, _gp, _P(_dp), _i32, _ip, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32,
                                      _P(EikStats)]),
     "ts_engine_set_graph": (C.c_int, [_vp, _i32]),

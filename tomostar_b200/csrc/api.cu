@@ -129,6 +129,15 @@ int32_t ts_engine_shapes(int32_t* shapes, int32_t cap) {
     return int32_t(all.size());
 }
 
+int ts_engine_set_scheduler(ts_ctx* ctx, int32_t scheduler) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (scheduler != 0 && scheduler != 1) return ctx->fail(TS_E_ARG, "scheduler must be 0 (lockstep) or 1 (flow)");
+    ctx->scheduler = scheduler;
+    ctx->drop_graph();
+    return TS_OK;
+}
+
 int ts_engine_set_tile(ts_ctx* ctx, int32_t precision, int32_t shape_id) {
     if (!ctx) return TS_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);

@@ -257,6 +257,20 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
         pre[G] = int(acc);
         max_items = std::max(max_items, int(acc));
     }
+    // Flow scheduler queue: room for twice the tiles all fields can have outstanding at once (each
+    // field has one diagonal in flight).
+    size_t qcap = 1024;
+    if (ctx->scheduler == 1) {
+        size_t need = 0;
+        for (int f = 0; f < nf; f++) {
+            const int gi = fl[f]->grid;
+            const int* doff = A.at<int>(o_diag_off[gi]);
+            int mx = 0;
+            for (int q = 0; q < ndiag[gi]; q++) mx = std::max(mx, doff[q + 1] - doff[q]);
+            need += size_t(mx);
+        }
+        while (qcap < 2 * need) qcap *= 2;
+    }
     // Fields, control, state copies.
     size_t o_fields = A.add(sizeof(FieldDesc<Real>) * nf);
     size_t o_ctl = A.add(sizeof(Control));
@@ -266,6 +280,14 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     if (!D) return TS_E_NOMEM;
     auto* worklist = static_cast<unsigned long long*>(ctx->buf("eng.worklist", 16 * size_t(std::max(1, max_items))));
     if (!worklist) return TS_E_NOMEM;
+    const bool flow = ctx->scheduler == 1;
+    unsigned long long* q_items = nullptr;
+    unsigned long long* q_seq = nullptr;
+    if (flow) {
+        q_items = static_cast<unsigned long long*>(ctx->buf("eng.q_items", 8 * qcap));
+        q_seq = static_cast<unsigned long long*>(ctx->buf("eng.q_seq", 8 * qcap));
+        if (!q_items || !q_seq) return TS_E_NOMEM;
+    }
     for (int gi = 0; gi < ng; gi++) {
         GridDesc gd{};
         const host::Grid& g = *grids[gi];
@@ -333,12 +355,17 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     args.worklist_cap = std::max(1, max_items);
     args.max_rounds_per_launch = max_rounds;
     args.barrier_timeout_ns = 5000000000LL;
+    args.q_items = q_items;
+    args.q_seq = q_seq;
+    args.q_mask = qcap - 1;
     args.tol = Real(tol);
     args.wake_rel = Real(wake_rel);
     args.causal = wake_rel > 0 ? 1 : 0;  // fast mode: threshold and causal wakes together
     const int smem = PENCIL ? WARPS * PencilSmem<Real, BX>::kBytes : engine_smem_bytes<Real, S>(WARPS);
-    void* kfn = any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
-                        : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>;
+    void* kfn = flow ? (any_var ? (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
+                               : (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>)
+                     : (any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
+                                : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>);
     TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
     TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
@@ -368,6 +395,10 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
                 reinterpret_cast<const int*>(D + o_sc_field), reinterpret_cast<const int32_t*>(D + o_sc_node),
                 reinterpret_cast<const double*>(D + o_sc_t), cnt);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (running > 0 && flow) {
+            flow_queue_init<<<int(std::min<size_t>((qcap + 255) / 256, 1024)), 256, 0, s>>>(q_seq, qcap);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         if (running > 0) {
             if (timed) cudaEventRecord(k0, s);
             e = cudaLaunchCooperativeKernel(kfn, dim3(blocks), dim3(WARPS * 32), params, smem, s);

@@ -127,6 +127,10 @@ struct Layout {
 struct FieldState {
     int phase, round, status, changed;
     int enter1, rounds0, rounds1, pad;
+    // Flow scheduler: the sweep ordering and diagonal in progress, its tiles still outstanding, and
+    // the rounds run in the current launch.
+    int dir, q, pending, launch_rounds;
+    int pad2[4];
 };
 
 template <typename Real>
@@ -156,6 +160,11 @@ struct Control {
     unsigned long long visits;
     int produced[2];   // due tiles listed in the step's worklist (by step parity)
     int consumed[2];   // worklist entries taken
+    // Flow scheduler: the tile queue's tickets (consumers take from head, producers reserve at tail)
+    // and the end of the launch (every field stopped).
+    unsigned long long q_head, q_tail;
+    int done;
+    int pad3[3];
 };
 
 struct Plan {
@@ -184,6 +193,12 @@ struct Args {
     int worklist_cap;
     int max_rounds_per_launch;   // rounds this launch may run (<= 0: until every field is done)
     long long barrier_timeout_ns;
+    // Flow scheduler queue (a bounded multi-producer multi-consumer ring): items[slot] =
+    // field << 32 | tx | ty << 10 | tz << 20. seq[slot] starts at slot; the producer of ticket t waits
+    // for seq == t, writes, and sets t + 1; its consumer waits for t + 1, reads, and sets t + capacity.
+    unsigned long long* q_items;
+    unsigned long long* q_seq;
+    unsigned long long q_mask;
     Real tol;
     Real wake_rel;               // a drop wakes the neighbours when it exceeds wake_rel × the new time
     int causal;                  // a drop to t wakes only the neighbours holding more than t

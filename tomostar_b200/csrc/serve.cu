@@ -401,8 +401,8 @@ void serve_loop(ts_server* sv) {
 
 extern "C" {
 
-int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, double hbm_budget_bytes,
-                    int32_t rounds_per_epoch, ts_server** out) {
+int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, int32_t scheduler,
+                    double hbm_budget_bytes, int32_t rounds_per_epoch, ts_server** out) {
     if (!out) return TS_E_ARG;
     *out = nullptr;
     if (precision != TS_PRECISION_F64 && precision != TS_PRECISION_F32) return TS_E_ARG;
@@ -411,9 +411,11 @@ int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t til
     bool known = false;
     for (const auto& t : ts::eik::tile_shapes()) known |= t.id == tile;
     if (!known) return TS_E_ARG;
+    if (scheduler != 0 && scheduler != 1) return TS_E_ARG;
     ts_ctx* ctx = nullptr;
     int rc = ts_cuda_create(device, &ctx);
     if (rc) return rc;
+    ctx->scheduler = scheduler;
     // Memory freed by finished requests stays with the stream-ordered pool for the next ones.
     cudaMemPool_t pool = nullptr;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
