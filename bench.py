@@ -201,6 +201,7 @@ def run_ours(args, problem_fn):
     if not (rel <= 1e-6):
         raise SystemExit(f"self-test failed: {msg}")
     lib.ts_engine_set_tile(solver.handle, 64, args.tile)
+    lib.ts_engine_set_scheduler(solver.handle, args.scheduler)
     # Seeds of every (station, phase) field, on the host before timing (PointSource, C ABI).
     seeds = {ph: [point_source(g, p.slowness[ph], *p.stations[q]) for q in range(n_st)] for ph in (0, 1)}
     packed = {ph: pack_seeds(seeds[ph]) for ph in (0, 1)}
@@ -314,15 +315,37 @@ def run_ours(args, problem_fn):
         cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{threads} of 800 fields, fast marching one field per thread (oracle/oracle.cpp)"}
 
+    solver.close()
+    # The whole forward step through RayKernels.Compute's drop-in (ts_forward): the 800 tables, then
+    # every arrival back-traced into its Jacobian row, rows copied to the host.
+    forward = None
+    if not args.no_forward:
+        from tomostar_b200.rays import RayKernels
+
+        fsolver = EikonalCuda.create(local, 64)
+        lib.ts_engine_set_tile(fsolver.handle, 64, args.tile)
+        rk = RayKernels(p.inv, g, fsolver)
+        t0 = time.perf_counter()
+        rows = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64)
+        wall = time.perf_counter() - t0
+        fields_s = rk.last_stats.device_ms / 1e3
+        n_rows = int(rows.n_rows)
+        forward = {"arrivals": n_rows, "tables": 2 * len(p.stations), "wall_s": wall,
+                   "rows_per_s": n_rows / wall, "tables_s": fields_s, "rays_and_copy_s": wall - fields_s,
+                   "rays_rows_per_s": n_rows / max(1e-9, wall - fields_s), "nnz": int(rows.nnz),
+                   "nnz_per_row": rows.nnz / max(1, int(rows.ok.sum())), "kept_rows": int(rows.ok.sum()),
+                   "mode": "engine (bitwise) tables, float32, rays FP64"}
+        del rows
+        fsolver.close()
     # The serving load (Poisson stream of mixed requests) on one GPU, after the batch job's buffers
     # are released; at N = 1 only (the scaling runs measure the batch job).
-    solver.close()
     serving = None
     if world == 1 and not args.no_serving:
         from tomostar_b200.serve_load import run as serve_run
 
         serving = serve_run(seconds=args.serve_seconds, rate=200.0, tile=args.serve_tile,
-                            rounds_per_epoch=args.serve_rounds, budget_bytes=120e9, device=local)
+                            rounds_per_epoch=args.serve_rounds, budget_bytes=120e9, device=local,
+                            scheduler=args.serve_scheduler)
 
     if rank == 0:
         line = {
@@ -332,6 +355,7 @@ def run_ours(args, problem_fn):
             "config": {"workload": f"config4: 401x401x121 nodes at 0.25 km (19.46 M), {n_st} surface stations x P,S "
                                    f"= {2 * n_st} fields per GPU, Vp 1-D gradient + 3 ellipsoids +-8 % (seed 5)",
                        "global_fields": 2 * n_st * world, "tile": args.tile,
+                       "scheduler": {0: "lockstep diagonals", 1: "flow (per-field diagonals, tile queue)"}[args.scheduler],
                        "mode": {0: "engine (bitwise with the reference)",
                                 2: "fast (a drop wakes only neighbours above the new time, and only when above "
                                    "1e-13 of it; within 1e-10 rel of bitwise)"}[args.mode],
@@ -346,6 +370,7 @@ def run_ours(args, problem_fn):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "plain_gpu": plain,
+            "forward_step": forward,
             "serving": serving,
             "node_updates_per_step": updates // args.steps,
             "wall_s_timed": t_wall,
@@ -369,9 +394,12 @@ def main():
     ap.add_argument("--no-baselines", action="store_true")
     ap.add_argument("--fields", type=int, default=0, help="stations per step (default all 400; fewer = a small case)")
     ap.add_argument("--verbose", action="store_true", help="per-launch statistics on stderr")
+    ap.add_argument("--scheduler", type=int, default=0, help="0 lockstep diagonals, 1 flow (per field)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-load measurement")
+    ap.add_argument("--no-forward", action="store_true", help="skip the forward step (tables + rays)")
+    ap.add_argument("--serve-scheduler", type=int, default=1)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
-    ap.add_argument("--serve-tile", type=int, default=2)
+    ap.add_argument("--serve-tile", type=int, default=4)
     ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
     args = ap.parse_args()
 

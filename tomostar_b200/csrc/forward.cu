@@ -74,18 +74,33 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
         table_station[3 * t + 1] = sp[1];
         table_station[3 * t + 2] = sp[2];
     }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, ctx->stream);
-    eik::EngineJob job;
+    // Tables in batches that fit next to the tables themselves: each batch solved by the engine and
+    // rounded to float32 into its slots (TravelTimeTable.Write's rounding).
+    float* tab = nullptr;
     if (nt > 0) {
+        tab = static_cast<float*>(ctx->buf("fwd.tables", sizeof(float) * size_t(n) * nt));
+        if (!tab) return TS_E_NOMEM;
+    }
+    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    const int tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
+    const size_t per_field = size_t(eik::field_layout(g, tile, precision).bytes(precision));
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    cudaGetLastError();
+    free_b += ctx->bufs.count("eng.fields") ? ctx->bufs["eng.fields"].n : 0;  // reused by the batches
+    const size_t room = free_b > (size_t(4) << 30) ? free_b - (size_t(4) << 30) : free_b / 2;
+    const int batch = int(std::max<size_t>(1, std::min<size_t>(size_t(std::max(1, nt)), room / per_field)));
+    const int cap = std::max(32, (g.nx + g.ny + g.nz) / 4);
+    int r0 = 0, r1 = 0;
+    double field_ms = 0;
+    for (int t0 = 0; t0 < nt; t0 += batch) {
+        const int t1 = std::min(nt, t0 + batch);
+        eik::EngineJob job;
         job.grids.push_back(&g);
         job.metrics.push_back(&m);
         job.tol = 1e-7;  // SphericalEikonal.SettleTolerance
-        job.tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
-        const int cap = std::max(32, (g.nx + g.ny + g.nz) / 4);
-        for (int t = 0; t < nt; t++) {
+        job.tile = tile;
+        for (int t = t0; t < t1; t++) {
             eik::EngineField ef;
             ef.grid = 0;
             ef.slowness = slow_d + size_t(n) * tables[t].first;
@@ -94,36 +109,44 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
             ef.cap = cap;
             job.fields.push_back(ef);
         }
-        rc = eik::engine_run<Real>(ctx, job, stats);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, ctx->stream);
+        ts_eik_stats bst{};
+        rc = eik::engine_run<Real>(ctx, job, &bst);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        field_ms += ms;
+        if (stats) {
+            stats->node_updates += bst.node_updates;
+            stats->tile_visits += bst.tile_visits;
+            stats->launches += bst.launches;
+            stats->kernel_ms += bst.kernel_ms;
+        }
         if (rc) return rc;
-        int r0 = 0, r1 = 0;
         for (auto& ef : job.fields) {
             if (ef.status != 1)
                 return ctx->fail(TS_E_UNSETTLED, "sweeping not settled after " + std::to_string(cap) + " rounds");
             r0 = std::max(r0, ef.rounds[0]);
             r1 = std::max(r1, ef.rounds[1]);
         }
-        if (stats) {
-            stats->rounds[0] = r0;
-            stats->rounds[1] = r1;
-        }
-        ctx->stats = std::to_string(r0) + "+" + std::to_string(r1) + " rounds of 8 sweeps";
-    }
-    cudaEventRecord(e1, ctx->stream);
-    cudaEventSynchronize(e1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (stats) stats->device_ms = ms;
-    // Dense float32 tables (TravelTimeTable.Write's rounding).
-    float* tab = nullptr;
-    if (nt > 0) {
-        tab = static_cast<float*>(ctx->buf("fwd.tables", sizeof(float) * size_t(n) * nt));
-        if (!tab) return TS_E_NOMEM;
-        rc = eik::fields_to_dense_f32_device(ctx, job, sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32, tab);
+        rc = eik::fields_to_dense_f32_device(ctx, job, precision, tab + size_t(t0) * n);
         if (rc) return rc;
     }
+    if (stats) {
+        stats->rounds[0] = r0;
+        stats->rounds[1] = r1;
+        stats->device_ms = field_ms;
+    }
+    ctx->stats = std::to_string(r0) + "+" + std::to_string(r1) + " rounds of 8 sweeps";
+    // The engine's field buffers are not needed by the rays: give their memory to the rows.
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->release("eng.fields");
     // Arrivals → rays.
     std::vector<int32_t> table_of(std::max(1, n_arr));
     std::vector<double> ev(3 * std::max(1, n_arr));
