@@ -227,6 +227,10 @@ typedef struct ts_serve_stats_t {
 int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t tile, int32_t scheduler,
                     double hbm_budget_bytes, int32_t rounds_per_epoch, ts_server** out);
 void ts_serve_destroy(ts_server* server);
+/* Flow scheduler only: an epoch ends once `ms` have passed, each field pausing at its next round
+ * end (and at rounds_per_epoch rounds at the latest), so that fields of small grids keep the device
+ * busy while larger ones finish their rounds. 0: rounds only. */
+int ts_serve_set_epoch_ms(ts_server* server, double ms);
 const char* ts_serve_last_error(ts_server* server);
 int ts_serve_model_put(ts_server* server, const ts_grid* grid, const double* slowness, int32_t n_phases,
                        int32_t* model_id);

@@ -100,3 +100,21 @@ def test_request_beyond_budget_is_refused(models):
         seeds = [point_source(m.grid, m.slowness[0], m.grid.min_lon + 0.1, m.grid.min_lat + 0.1, 0.0)]
         res = server.wait(server.submit(mid, 0, seeds))
         assert res.status == L.TS_E_CAPACITY and "budget" in res.error
+
+
+def test_flow_scheduler_time_budgeted_epochs(models, solver):
+    """Flow scheduler with epochs that end on time (fields pausing at a round end after 5 ms): every
+    request still gets the one-shot engine's bits."""
+    stream = syn.config3_stream(models, rate=200, duration=0.1, seed=4)
+    with Server(tile=4, budget_bytes=16e9, rounds_per_epoch=8, scheduler=1, epoch_ms=5.0) as server:
+        ids = {name: server.model_put(m.grid, m.slowness) for name, m in models.items()}
+        rid = [submit_spec(server, ids, models, r) for r in stream]
+        results = [server.wait(q) for q in rid]
+        assert server.stats()["epochs"] > 1
+    for r, res in zip(stream, results):
+        assert res.status == L.TS_OK, res.error
+        m = models[r.model]
+        seeds = [point_source(m.grid, m.slowness[r.phase], *st) for st in r.stations]
+        one = solver.solve(m.grid, m.slowness[r.phase], seeds, mode=L.MODE_FAST, precision=64,
+                           output=np.empty((len(seeds), m.grid.count), np.float32))
+        assert np.array_equal(res.tables, one)

@@ -92,6 +92,7 @@ _gp = _P(GridStruct)
 SIGNATURES = {
     "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
     "ts_serve_destroy": (None, [_vp]),
+    "ts_serve_set_epoch_ms": (C.c_int, [_vp, _d]),
     "ts_serve_last_error": (C.c_char_p, [_vp]),
     "ts_serve_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _ip]),
     "ts_serve_submit": (C.c_int, [_vp, _P(ServeRequest), _P(C.c_int64)]),

@@ -25,6 +25,7 @@ struct ts_ctx {
     int* cancel_dev = nullptr;
     int tile_f64 = 0, tile_f32 = 0;       // engine tile shape per precision
     int scheduler = 0;                    // engine scheduler: 0 lockstep diagonals, 1 flow (per field)
+    double epoch_budget_ms = 0;           // flow epochs: fields pause at the first round end after this
     // CUDA-graph replay of one-shot engine solves: the last captured solve and its signature.
     bool use_graph = false;
     unsigned long long graph_sig = 0;

@@ -354,6 +354,7 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     args.worklist = worklist;
     args.worklist_cap = std::max(1, max_items);
     args.max_rounds_per_launch = max_rounds;
+    args.epoch_budget_ns = (flow && max_rounds > 0) ? (long long)(ctx->epoch_budget_ms * 1e6) : 0;
     args.barrier_timeout_ns = 5000000000LL;
     args.q_items = q_items;
     args.q_seq = q_seq;

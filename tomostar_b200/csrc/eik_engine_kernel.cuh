@@ -249,6 +249,9 @@ TS_DEVINL bool flow_round_end(const Args<Real>& a, int f, int lane) {
         st->changed = 0;
         st->launch_rounds = st->launch_rounds + 1;
         if (!stop && a.max_rounds_per_launch > 0 && st->launch_rounds >= a.max_rounds_per_launch) stop = true;
+        if (!stop && a.epoch_budget_ns > 0 &&
+            (long long)(global_ns() - *(volatile unsigned long long*)&a.ctl->t_start) > a.epoch_budget_ns)
+            stop = true;
         if (!stop && a.cancel && *a.cancel) {
             atomicCAS(&a.ctl->error, 0, TS_E_CANCELLED);
             stop = true;
@@ -400,6 +403,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) flow_kernel(Args<Real> a) {
     const int nwarps = gridDim.x * WARPS;
     unsigned long long my_updates = 0, my_visits = 0;
 
+    if (lane == 0) atomicCAS(&a.ctl->t_start, 0ull, global_ns());
+    __syncwarp();
     // Every running field starts its launch at the first diagonal of a round.
     for (int e = gwarp; e < a.n_active; e += nwarps) {
         const int f = a.plan.field_list[e];

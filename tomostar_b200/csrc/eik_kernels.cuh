@@ -163,6 +163,7 @@ struct Control {
     // Flow scheduler: the tile queue's tickets (consumers take from head, producers reserve at tail)
     // and the end of the launch (every field stopped).
     unsigned long long q_head, q_tail;
+    unsigned long long t_start;  // globaltimer at the launch's start (first warp to arrive)
     int done;
     int pad3[3];
 };
@@ -192,6 +193,7 @@ struct Args {
     unsigned long long* worklist;  // 2 x worklist_cap due tiles: field << 32 | tx | ty << 10 | tz << 20
     int worklist_cap;
     int max_rounds_per_launch;   // rounds this launch may run (<= 0: until every field is done)
+    long long epoch_budget_ns;   // flow scheduler: after this long, each field pauses at its next round end
     long long barrier_timeout_ns;
     // Flow scheduler queue (a bounded multi-producer multi-consumer ring): items[slot] =
     // field << 32 | tx | ty << 10 | tz << 20. seq[slot] starts at slot; the producer of ticket t waits

@@ -454,6 +454,13 @@ void ts_serve_destroy(ts_server* sv) {
 
 const char* ts_serve_last_error(ts_server* sv) { return sv ? sv->err.c_str() : ""; }
 
+int ts_serve_set_epoch_ms(ts_server* sv, double ms) {
+    if (!sv || !(ms >= 0)) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> cl(sv->ctx->mu);
+    sv->ctx->epoch_budget_ms = ms;
+    return TS_OK;
+}
+
 int ts_serve_model_put(ts_server* sv, const ts_grid* grid, const double* slowness, int32_t n_phases, int32_t* model_id) {
     if (!sv || !grid || !slowness || !model_id || n_phases < 1) return TS_E_ARG;
     std::lock_guard<std::recursive_mutex> cl(sv->ctx->mu);

@@ -17,7 +17,8 @@ from .serving import Server
 
 
 def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 2, rounds_per_epoch: int = 1,
-        budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 0) -> dict:
+        budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 0,
+        epoch_ms: float = 0.0) -> dict:
     models = syn.config3_models()
     stream = syn.config3_stream(models, rate=rate, duration=seconds, seed=seed)
     # Seeds of every field on the host before the clock starts (PointSource, ts_point_source).
@@ -26,7 +27,7 @@ def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 2, rounds_per_ep
         m = models[r.model]
         prepared.append([point_source(m.grid, m.slowness[r.phase], *st) for st in r.stations])
     server = Server(device=device, tile=tile, budget_bytes=budget_bytes, rounds_per_epoch=rounds_per_epoch,
-                    scheduler=scheduler)
+                    scheduler=scheduler, epoch_ms=epoch_ms)
     try:
         ids = {name: server.model_put(m.grid, m.slowness) for name, m in models.items()}
 
@@ -87,7 +88,7 @@ def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 2, rounds_per_ep
         "complete_wall_s": (st["complete_ms"] - base["complete_ms"]) / 1e3,
         "node_updates": st["node_updates"] - base["node_updates"], "peak_hbm_gb": st["peak_bytes"] / 1e9,
         "budget_gb": budget_bytes / 1e9, "tile": tile, "rounds_per_epoch": rounds_per_epoch,
-        "scheduler": {0: "lockstep", 1: "flow"}[scheduler],
+        "scheduler": {0: "lockstep", 1: "flow"}[scheduler], "epoch_ms": epoch_ms,
         "errors": sorted({res.error for res in results if res.status != L.TS_OK})[:3],
     }
 
@@ -100,8 +101,10 @@ def main():
     ap.add_argument("--rounds-per-epoch", type=int, default=1)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--scheduler", type=int, default=0)
+    ap.add_argument("--epoch-ms", type=float, default=0.0)
     a = ap.parse_args()
-    print(json.dumps(run(a.seconds, a.rate, a.tile, a.rounds_per_epoch, a.budget_gb * 1e9, scheduler=a.scheduler)))
+    print(json.dumps(run(a.seconds, a.rate, a.tile, a.rounds_per_epoch, a.budget_gb * 1e9, scheduler=a.scheduler,
+                         epoch_ms=a.epoch_ms)))
 
 
 if __name__ == "__main__":

@@ -38,7 +38,8 @@ class Server:
     """One serving loop on one GPU (ts_serve_create)."""
 
     def __init__(self, device: int = 0, precision: int = 64, mode: int = L.MODE_FAST, tile: int = 2,
-                 budget_bytes: float = 120e9, rounds_per_epoch: int = 1, scheduler: int = 0):
+                 budget_bytes: float = 120e9, rounds_per_epoch: int = 1, scheduler: int = 0,
+                 epoch_ms: float = 0.0):
         lib = L.load()
         h = C.c_void_p()
         rc = lib.ts_serve_create(device, precision, mode, tile, scheduler, float(budget_bytes), rounds_per_epoch,
@@ -46,6 +47,8 @@ class Server:
         if rc != L.TS_OK:
             raise L.TsError(rc, "ts_serve_create")
         self._h = h
+        if epoch_ms > 0:
+            L.check(lib.ts_serve_set_epoch_ms(h, float(epoch_ms)))
         self._models: dict[int, GridDef] = {}
         self._keep: dict[int, tuple] = {}
 
