@@ -319,7 +319,7 @@ def run_ours(args, problem_fn):
     # The whole forward step through RayKernels.Compute's drop-in (ts_forward): the 800 tables, then
     # every arrival back-traced into its Jacobian row, rows copied to the host.
     forward = None
-    if not args.no_forward:
+    if world == 1 and not args.no_forward:
         from tomostar_b200.rays import RayKernels
 
         fsolver = EikonalCuda.create(local, 64)
