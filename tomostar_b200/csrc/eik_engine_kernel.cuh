@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
                         if constexpr (PENCIL) {
                             Real* halo = reinterpret_cast<Real*>(mine);
                             if (VARZ_ANY && g.varz)
-                                ev = process_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                             else
-                                ev = process_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                         } else {
                             if (VARZ_ANY && g.varz)
                                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
@@ -464,8 +464,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) flow_kernel(Args<Real> a) {
         int ev;
         if constexpr (PENCIL) {
             Real* halo = reinterpret_cast<Real*>(mine);
-            if (VARZ_ANY && g.varz) ev = process_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
-            else ev = process_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            if (VARZ_ANY && g.varz) ev = visit_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            else ev = visit_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
         } else {
             if (VARZ_ANY && g.varz)
                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx, mwy, mzc,
