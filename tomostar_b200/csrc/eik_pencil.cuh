@@ -40,26 +40,32 @@ TS_DEVINL uint64_t row_reverse(uint64_t m) {
     return uint64_t(__brev(uint32_t(m)));
 }
 
-template <typename Real, int BX, bool VARZ, int MXMODE>
+template <typename Real, int BX, bool VARZ, int SDIR>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane);
 
-// The pencil visit with the x mirroring specialised where that pays (64-wide pencils).
+// The pencil visit with the sweep ordering specialised where that pays (64-wide FP64 pencils).
 template <typename Real, int BX, bool VARZ>
 TS_DEVINL int visit_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                            int tz, int dir, bool second, Real* halo, int lane) {
-    if constexpr (BX == 64) {
-        if (dir & 1) return process_pencil<Real, BX, VARZ, 2>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
-        return process_pencil<Real, BX, VARZ, 1>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
+    if constexpr (BX == 64 && sizeof(Real) == 8) {
+        switch (dir) {
+#define TS_PENCIL_DIR(d) \
+    case d: return process_pencil<Real, BX, VARZ, d>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
+            TS_PENCIL_DIR(0) TS_PENCIL_DIR(1) TS_PENCIL_DIR(2) TS_PENCIL_DIR(3)
+            TS_PENCIL_DIR(4) TS_PENCIL_DIR(5) TS_PENCIL_DIR(6) TS_PENCIL_DIR(7)
+#undef TS_PENCIL_DIR
+        }
+        return 0;
     } else {
-        return process_pencil<Real, BX, VARZ, 0>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
+        return process_pencil<Real, BX, VARZ, -1>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
     }
 }
 
-// MXMODE 1 / 2: the sweep runs with / against x, fixed at compile time so that the x mirroring
-// costs nothing in the step loop (used for 64-wide pencils); 0: read from dir at run time (32-wide
-// pencils, where the specialised code needs more registers than the 128 their occupancy allows).
-template <typename Real, int BX, bool VARZ, int MXMODE>
+// SDIR 0..7: the sweep ordering fixed at compile time, so that the mirroring costs nothing in the
+// step loop (used for 64-wide FP64 pencils); −1: read from dir at run time (32-wide pencils, where
+// the specialised code needs more registers than the 128 their occupancy allows, and FP32).
+template <typename Real, int BX, bool VARZ, int SDIR>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane) {
     static_assert(BX == 32 || BX == 64, "pencil rows are 32 or 64 nodes");
@@ -72,8 +78,8 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int x0 = tx * BX, y0 = ty * BY, z0 = tz * BZ;
     const int tid = (tz * g.ty + ty) * g.tx + tx;
-    const bool mx = MXMODE == 0 ? (dir & 1) != 0 : MXMODE == 2;
-    const bool my = (dir & 2) != 0, mz = (dir & 4) != 0;
+    const int sd = SDIR < 0 ? dir : SDIR;
+    const bool mx = (sd & 1) != 0, my = (sd & 2) != 0, mz = (sd & 4) != 0;
     const int jp = lane & 7, kp = lane >> 3;  // canonical row of the lane
     const int j = my ? BY - 1 - jp : jp, k = mz ? BZ - 1 - kp : kp;
     const int gy = y0 + j, gz = z0 + k;
@@ -158,11 +164,11 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     auto ax = [&](int c) { return mx ? BX - 1 - c : c; };
     [[maybe_unused]] const int xlast = min(BX, nx - x0) - 1;  // last on-grid x offset of the tile
     auto ldT = [&](int c) -> Real {
-        if constexpr (MXMODE != 0) return row_on ? ld_cg(row + ax(max(-2, min(c, BX + 1)))) : inf;
+        if constexpr (SDIR >= 0) return row_on ? ld_cg(row + ax(max(-2, min(c, BX + 1)))) : inf;
         else return (row_on && c >= -2 && c <= BX + 1) ? ld_cg(row + ax(c)) : inf;
     };
     auto ldS = [&](int c) -> Real {
-        if constexpr (MXMODE != 0) return row_on ? __ldg(srow + max(0, min(ax(c), xlast))) : Real(0);
+        if constexpr (SDIR >= 0) return row_on ? __ldg(srow + max(0, min(ax(c), xlast))) : Real(0);
         else return (row_on && c >= 0 && c < BX && x0 + ax(c) < nx) ? __ldg(srow + ax(c)) : Real(0);
     };
     const int ip0 = -jp - kp;
