@@ -173,13 +173,14 @@ int ts_eik_solve_multi(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const
  * grids, fields and seeds on the same buffers) is solved again. No reference counterpart. */
 int ts_engine_set_graph(ts_ctx* ctx, int32_t enable);
 int32_t ts_engine_graph_replays(ts_ctx* ctx);
-/* Times every tile shape on a sample batch (ts_eik_solve_multi arguments, best of `repeats`), selects
- * the fastest for `precision` on this context and returns it; ms_per_shape[q] receives shape q's
- * time (up to cap entries). No reference counterpart. */
+/* Times every tile shape under both schedulers on a sample batch (ts_eik_solve_multi arguments, best
+ * of `repeats`), selects the fastest pair for `precision` on this context and returns it;
+ * ms_per_shape[2q + s] receives shape q's time under scheduler s (up to cap entries). No reference
+ * counterpart. */
 int ts_engine_autotune(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const double* const* slowness,
                        int32_t n_fields, const int32_t* field_grid, const int32_t* seed_offsets, const int32_t* seed_index,
                        const double* seed_time, int32_t precision, int32_t mode, int32_t repeats, int32_t* best_tile,
-                       double* ms_per_shape, int32_t cap);
+                       int32_t* best_scheduler, double* ms_per_shape, int32_t cap);
 
 /* ---- serving: a resident request loop with continuous batching (no reference counterpart) ----
  * A server owns its own context on `device` and one loop thread. Models are put once and stay on

@@ -137,8 +137,16 @@ def test_graph_replay_repeats_the_job(solver, batch):
 def test_autotune_selects_a_compiled_shape(solver, batch):
     b, seeds = batch
     n = 3
-    best, ms = solver.autotune(b.grids[:n], b.slowness[:n], list(range(n)), seeds[:n], precision=64)
-    assert best in ms and all(np.isfinite(v) and v > 0 for v in ms.values())
-    assert ms[best] == min(ms.values())
-    # The selection stays on the context; restore the default shape afterwards.
-    L.check(L.load().ts_engine_set_tile(solver.handle, 64, 0), solver)
+    best, sched, ms = solver.autotune(b.grids[:n], b.slowness[:n], list(range(n)), seeds[:n], precision=64)
+    assert (best, sched) in ms and all(np.isfinite(v) and v > 0 for v in ms.values())
+    assert ms[(best, sched)] == min(ms.values())
+    # The selection stays on the context and gives the same fields; restore the defaults afterwards.
+    lib = L.load()
+    try:
+        fields = solver.solve_multi(b.grids[:n], b.slowness[:n], list(range(n)), seeds[:n], mode=L.MODE_FAST,
+                                    precision=64)
+        for q in range(n):
+            assert np.array_equal(fields[q], oracle_field(b.grids[q], b.slowness[q], seeds[q], L.WAKE_REL))
+    finally:
+        L.check(lib.ts_engine_set_tile(solver.handle, 64, 0), solver)
+        L.check(lib.ts_engine_set_scheduler(solver.handle, 0), solver)

@@ -112,8 +112,8 @@ SIGNATURES = {
                                      _P(EikStats)]),
     "ts_engine_set_graph": (C.c_int, [_vp, _i32]),
     "ts_engine_graph_replays": (_i32, [_vp]),
-    "ts_engine_autotune": (C.c_int, [_vp, _i32, _gp, _P(_dp), _i32, _ip, _ip, _ip, _dp, _i32, _i32, _i32, _ip, _dp,
-                                     _i32]),
+    "ts_engine_autotune": (C.c_int, [_vp, _i32, _gp, _P(_dp), _i32, _ip, _ip, _ip, _dp, _i32, _i32, _i32, _ip, _ip,
+                                     _dp, _i32]),
     "ts_point_source": (_i32, [_gp, _dp, _d, _d, _d, _d, _d, _ip, _dp, _i32]),
     "ts_eik_solve": (C.c_int, [_vp, _gp, _dp, _i32, _ip, _ip, _dp, _i32, _i32, _d, _i32, _vp, _i32, _P(EikStats)]),
     "ts_model_put": (C.c_int, [_vp, _gp, _dp, _i32, _i32, _ip]),

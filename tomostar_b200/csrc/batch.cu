@@ -148,43 +148,54 @@ int32_t ts_engine_graph_replays(ts_ctx* ctx) { return ctx ? ctx->graph_replays :
 int ts_engine_autotune(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const double* const* slowness,
                        int32_t n_fields, const int32_t* field_grid, const int32_t* seed_offsets, const int32_t* seed_index,
                        const double* seed_time, int32_t precision, int32_t mode, int32_t repeats, int32_t* best_tile,
-                       double* ms_per_shape, int32_t cap) {
+                       int32_t* best_scheduler, double* ms_per_shape, int32_t cap) {
     if (!ctx || !best_tile) return TS_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     const auto& shapes = ts::eik::tile_shapes();
-    int best = -1;
+    int best = -1, best_sched = 0;
     double best_ms = INFINITY;
-    const int keep64 = ctx->tile_f64, keep32 = ctx->tile_f32;
+    const int keep64 = ctx->tile_f64, keep32 = ctx->tile_f32, keep_sched = ctx->scheduler;
     const bool keep_graph = ctx->use_graph;
     ctx->use_graph = false;
+    auto restore = [&]() {
+        ctx->tile_f64 = keep64;
+        ctx->tile_f32 = keep32;
+        ctx->scheduler = keep_sched;
+        ctx->use_graph = keep_graph;
+    };
+    // Every (shape, scheduler) pair; entry 2·q + scheduler of ms_per_shape.
     for (size_t q = 0; q < shapes.size(); q++) {
-        if (precision == TS_PRECISION_F64) ctx->tile_f64 = shapes[q].id;
-        else ctx->tile_f32 = shapes[q].id;
-        double ms = INFINITY;
-        for (int r = 0; r < std::max(1, repeats); r++) {
-            ts_eik_stats st{};
-            int rc = ts_eik_solve_multi(ctx, n_grids, grids, slowness, n_fields, field_grid, seed_offsets, seed_index,
-                                        seed_time, precision, mode, 1e-7, 0, nullptr, TS_OUT_NONE, &st);
-            if (rc) {
-                ctx->tile_f64 = keep64;
-                ctx->tile_f32 = keep32;
-                ctx->use_graph = keep_graph;
-                return rc;
+        for (int sched = 0; sched < 2; sched++) {
+            if (precision == TS_PRECISION_F64) ctx->tile_f64 = shapes[q].id;
+            else ctx->tile_f32 = shapes[q].id;
+            ctx->scheduler = sched;
+            double ms = INFINITY;
+            for (int r = 0; r < std::max(1, repeats); r++) {
+                ts_eik_stats st{};
+                int rc = ts_eik_solve_multi(ctx, n_grids, grids, slowness, n_fields, field_grid, seed_offsets,
+                                            seed_index, seed_time, precision, mode, 1e-7, 0, nullptr, TS_OUT_NONE, &st);
+                if (rc) {
+                    restore();
+                    return rc;
+                }
+                ms = std::min(ms, st.device_ms);
             }
-            ms = std::min(ms, st.device_ms);
-        }
-        if (ms_per_shape && int32_t(q) < cap) ms_per_shape[q] = ms;
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = shapes[q].id;
+            const int32_t slot = int32_t(2 * q + sched);
+            if (ms_per_shape && slot < cap) ms_per_shape[slot] = ms;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = shapes[q].id;
+                best_sched = sched;
+            }
         }
     }
-    ctx->tile_f64 = keep64;
-    ctx->tile_f32 = keep32;
+    restore();
     if (precision == TS_PRECISION_F64) ctx->tile_f64 = best;
     else ctx->tile_f32 = best;
-    ctx->use_graph = keep_graph;
+    ctx->scheduler = best_sched;
+    ctx->drop_graph();
     *best_tile = best;
+    if (best_scheduler) *best_scheduler = best_sched;
     return TS_OK;
 }
 

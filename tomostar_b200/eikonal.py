@@ -205,8 +205,8 @@ class EikonalCuda:
 
     def autotune(self, grids, slownesses, field_grid, seed_sets, mode: int = L.MODE_FAST, repeats: int = 1,
                  precision: int | None = None):
-        """Times every compiled tile shape on the sample batch and keeps the fastest; returns
-        (best shape id, {shape id: ms})."""
+        """Times every compiled tile shape under both schedulers on the sample batch and keeps the
+        fastest pair; returns (best shape id, best scheduler, {(shape id, scheduler): ms})."""
         lib = L.load()
         prec = self.precision if precision is None else precision
         ng = len(grids)
@@ -217,14 +217,15 @@ class EikonalCuda:
         fg = np.ascontiguousarray(field_grid, np.int32)
         off, idx, t = pack_seeds(seed_sets)
         shapes = L.engine_shapes()
-        ms = np.full(len(shapes), np.inf)
-        best = C.c_int32(-1)
+        ms = np.full(2 * len(shapes), np.inf)
+        best, sched = C.c_int32(-1), C.c_int32(0)
         rc = lib.ts_engine_autotune(self._h, ng, gs, sp, len(seed_sets), _ptr(fg, C.c_int32), _ptr(off, C.c_int32),
                                     _ptr(idx, C.c_int32), _ptr(t, C.c_double), prec, mode, repeats, C.byref(best),
-                                    _ptr(ms, C.c_double), len(ms))
+                                    C.byref(sched), _ptr(ms, C.c_double), len(ms))
         if rc != L.TS_OK:
             raise L.TsError(rc, self.last_error)
-        return int(best.value), {sid: float(v) for (sid, *_), v in zip(shapes, ms)}
+        table = {(sid, sc): float(ms[2 * q + sc]) for q, (sid, *_) in enumerate(shapes) for sc in (0, 1)}
+        return int(best.value), int(sched.value), table
 
     def try_solve(self, grid: GridDef, slowness: np.ndarray, seed_sets, output: np.ndarray, **kw) -> tuple[bool, str]:
         """EikonalOpenCl.TrySolve: (True, "") or (False, reason); output is field-major."""
