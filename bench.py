@@ -399,7 +399,7 @@ def main():
     ap.add_argument("--no-forward", action="store_true", help="skip the forward step (tables + rays)")
     ap.add_argument("--serve-scheduler", type=int, default=1)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
-    ap.add_argument("--serve-tile", type=int, default=4)
+    ap.add_argument("--serve-tile", type=int, default=2)
     ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
     args = ap.parse_args()
 

@@ -12,9 +12,11 @@ namespace ts {
 namespace eik {
 
 const std::vector<TileShapeInfo>& tile_shapes() {
-    // 0-3: cube tiles swept by node planes; 4-5: pencils (one lane per row of an 8×4 cross-section).
+    // 0-3: cube tiles swept by node planes; 4-6: pencils (one lane per row of an 8×4 cross-section;
+    // 6 is 4 with room for 170 registers instead of 128: 12 warps per SM and the FP64 sweep
+    // orderings specialised).
     static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4},
-                                                      {4, 32, 8, 4}, {5, 64, 8, 4}};
+                                                      {4, 32, 8, 4}, {5, 64, 8, 4}, {6, 32, 8, 4}};
     return shapes;
 }
 
@@ -558,6 +560,7 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
         case 3: return launch_epoch<Real, 8, 4, 4, 8, 3>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 4: return launch_epoch<Real, 32, 8, 4, 4, 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 5: return launch_epoch<Real, 64, 8, 4, 4, F64 ? 2 : 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 6: return launch_epoch<Real, 32, 8, 4, 4, F64 ? 3 : 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         default: return launch_epoch<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
     }
 }

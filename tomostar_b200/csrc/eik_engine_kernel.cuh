@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
                         if constexpr (PENCIL) {
                             Real* halo = reinterpret_cast<Real*>(mine);
                             if (VARZ_ANY && g.varz)
-                                ev = visit_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, true, (BX == 64 || MINB <= 3)>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                             else
-                                ev = visit_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, false, (BX == 64 || MINB <= 3)>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                         } else {
                             if (VARZ_ANY && g.varz)
                                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
@@ -463,9 +463,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) flow_kernel(Args<Real> a) {
         const bool second = st->phase == 1;
         int ev;
         if constexpr (PENCIL) {
+            // No per-ordering specialisation here: warps of one launch work on fields at different
+            // orderings, and eight copies of the visit would not share the instruction cache.
             Real* halo = reinterpret_cast<Real*>(mine);
-            if (VARZ_ANY && g.varz) ev = visit_pencil<Real, BX, true>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
-            else ev = visit_pencil<Real, BX, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            if (VARZ_ANY && g.varz) ev = visit_pencil<Real, BX, true, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            else ev = visit_pencil<Real, BX, false, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
         } else {
             if (VARZ_ANY && g.varz)
                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx, mwy, mzc,

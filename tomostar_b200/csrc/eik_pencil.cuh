@@ -44,11 +44,13 @@ template <typename Real, int BX, bool VARZ, int SDIR>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane);
 
-// The pencil visit with the sweep ordering specialised where that pays (64-wide FP64 pencils).
-template <typename Real, int BX, bool VARZ>
+// The pencil visit with the sweep ordering specialised where that pays (SPEC): FP64 pencils whose
+// launch leaves room for the extra registers (64-wide pencils, and 32-wide ones at 12 warps per SM),
+// under the lockstep scheduler, where every warp of a step runs the same ordering.
+template <typename Real, int BX, bool VARZ, bool SPEC>
 TS_DEVINL int visit_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                            int tz, int dir, bool second, Real* halo, int lane) {
-    if constexpr (BX == 64 && sizeof(Real) == 8) {
+    if constexpr (SPEC && sizeof(Real) == 8) {
         switch (dir) {
 #define TS_PENCIL_DIR(d) \
     case d: return process_pencil<Real, BX, VARZ, d>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
