@@ -23,6 +23,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -54,7 +55,7 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.out = os.path.join(tempfile.gettempdir(), f"tomostar_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -133,7 +134,7 @@ def rank_problem(rank: int):
     (the workload generated with seed 5 + r: its own stations, events and velocity bodies)."""
     from tomostar_b200 import synthetic as syn
 
-    return syn.config4(seed=5 + rank)
+    return syn.regional_401(seed=5 + rank)
 
 
 def job_throughput(dist, local, world: int, fields_per_rank_step: int, steps: int, dev_ms: float):
@@ -176,7 +177,7 @@ def run_reference(args, problem_fn):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "config4: 401x401x121 at 0.25 km, 800 P+S fields (400 stations)",
+        "config": {"workload": "regional forward step: 401x401x121 at 0.25 km, 800 P+S fields (400 stations)",
                    "sample": f"{n} fields per step"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n} of 800 fields per step, fast marching (oracle/oracle.cpp or_fmm_many)"},
@@ -352,7 +353,7 @@ def run_ours(args, problem_fn):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"config4: 401x401x121 nodes at 0.25 km (19.46 M), {n_st} surface stations x P,S "
+            "config": {"workload": f"regional forward step: 401x401x121 nodes at 0.25 km (19.46 M), {n_st} surface stations x P,S "
                                    f"= {2 * n_st} fields per GPU, Vp 1-D gradient + 3 ellipsoids +-8 % (seed 5)",
                        "global_fields": 2 * n_st * world, "tile": args.tile,
                        "scheduler": {0: "lockstep diagonals", 1: "flow (per-field diagonals, tile queue)"}[args.scheduler],

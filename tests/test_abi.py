@@ -73,8 +73,8 @@ def test_point_source_matches_oracle_bitwise(src):
     assert np.array_equal(a_idx, b_idx) and np.array_equal(a_t, b_t)
 
 
-def test_point_source_config0_matches_oracle():
-    p = syn.config0()
+def test_point_source_single_source_61_matches_oracle():
+    p = syn.single_source_61()
     a = point_source(p.grid, p.slowness[0], *p.stations[0])
     b = O.point_source(O.Grid.of(p.grid), p.slowness[0], *p.stations[0])
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])

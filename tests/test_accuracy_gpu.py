@@ -52,29 +52,29 @@ def check(solver, name, cases):
     assert r["fp32 arithmetic"][1] <= 2e-5 and r["fp32 arithmetic"][0] <= 2e-4
 
 
-def test_accuracy_config0(solver):
-    p = syn.config0()
+def test_accuracy_single_source_61(solver):
+    p = syn.single_source_61()
     check(solver, "61x61x31 at 1 km (one source)",
           [(p.grid, p.slowness[0], point_source(p.grid, p.slowness[0], *p.stations[0]))])
 
 
-def test_accuracy_config1(solver):
-    p = syn.config1()
+def test_accuracy_inversion_step_121(solver):
+    p = syn.inversion_step_121()
     cases = [(p.grid, p.slowness[ph], point_source(p.grid, p.slowness[ph], *p.stations[q]))
              for ph in (0, 1) for q in (0, 7)]
     check(solver, "121x121x61 at 0.5 km (P and S, 2 stations)", cases)
 
 
-def test_accuracy_config2_reduced(solver):
-    b = syn.config2(n_sources=6, seed=3, dims_scale=0.35)
+def test_accuracy_uneven_grids_reduced(solver):
+    b = syn.uneven_grids(n_sources=6, seed=3, dims_scale=0.35)
     cases = [(g, s, point_source(g, s, *src)) for g, s, src in zip(b.grids, b.slowness, b.sources)]
     check(solver, "uneven grids, half with geometric depth spacing (6 grids at 35 % size)", cases)
 
 
-def test_accuracy_config4_one_field(solver):
+def test_accuracy_regional_401_one_field(solver):
     """The 401x401x121 workload against the bitwise FP64 engine (equal to Relax to the bit by the
     tests above; the oracle itself would take minutes here)."""
-    p = syn.config4(n_stations=2, n_events=10, n_rays=10)
+    p = syn.regional_401(n_stations=2, n_events=10, n_rays=10)
     seeds = point_source(p.grid, p.slowness[0], *p.stations[1])
     ref = solver.solve(p.grid, p.slowness[0], [seeds], precision=64, mode=L.MODE_ENGINE)[0]
     tables = solver.solve(p.grid, p.slowness[0], [seeds], precision=64, mode=L.MODE_FAST,

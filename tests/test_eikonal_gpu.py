@@ -58,8 +58,8 @@ def test_try_create_passes_gate():
 
 
 @pytest.mark.parametrize("mode", [L.MODE_ENGINE, L.MODE_PLAIN])
-def test_f64_bitwise_config0(solver, mode):
-    p = syn.config0()
+def test_f64_bitwise_single_source_61(solver, mode):
+    p = syn.single_source_61()
     seeds = [point_source(p.grid, p.slowness[0], *p.stations[0])]
     ref = oracle_fields(p.grid, p.slowness[0], seeds)
     out = solver.solve(p.grid, p.slowness[0], seeds, mode=mode, precision=64)
@@ -108,7 +108,7 @@ def test_f64_batch_equals_solo(solver):
 
 
 def test_f32_engine_equals_plain_and_oracle(solver):
-    p = syn.config0()
+    p = syn.single_source_61()
     seeds = [point_source(p.grid, p.slowness[0], *p.stations[0])]
     ref = oracle_fields(p.grid, p.slowness[0], seeds)
     a = solver.solve(p.grid, p.slowness[0], seeds, precision=32)
@@ -131,10 +131,10 @@ def test_f32_engine_all_tile_shapes_equal_plain(solver):
         lib.ts_engine_set_tile(solver.handle, 32, 0)
 
 
-def test_f64_tables_config1_subset(solver):
-    """Config 1 (121×121×61, 0.5 km): P and S tables of three stations from the FP64 engine, written as
+def test_f64_tables_inversion_step_121_subset(solver):
+    """121×121×61 at 0.5 km: P and S tables of three stations from the FP64 engine, written as
     float32 (.qttb), equal the oracle's tables to the bit — the headline error is float rounding alone."""
-    p = syn.config1()
+    p = syn.inversion_step_121()
     for ph in (0, 1):
         seeds = [point_source(p.grid, p.slowness[ph], *p.stations[q]) for q in (0, 7, 19)]
         ref = oracle_fields(p.grid, p.slowness[ph], seeds)
@@ -144,12 +144,12 @@ def test_f64_tables_config1_subset(solver):
             assert rel_err(out[f].astype(np.float64), ref[f]) <= 6e-8
 
 
-def test_f32_compute_error_profile_config1(solver):
+def test_f32_compute_error_profile_inversion_step_121(solver):
     """FP32 arithmetic and float32 storage: the error against the FP64 oracle is float rounding
     (p99 under 2e-6) except along the lines of nodes where two neighbour times differ by about one
     float ulp and the reference's second-order promotion test (t2 <= first, SphericalEikonal.cs:391)
     flips; those reach a few 1e-5 relative. This mode is the fast option, not the headline."""
-    p = syn.config1()
+    p = syn.inversion_step_121()
     for ph in (0, 1):
         seeds = [point_source(p.grid, p.slowness[ph], *p.stations[q]) for q in (0, 7, 19)]
         ref = oracle_fields(p.grid, p.slowness[ph], seeds)
@@ -264,8 +264,8 @@ def test_fast_mode_equals_wake_oracle(solver, shape):
         assert rel_err(out[f], ref) <= 1e-10
 
 
-def test_fast_mode_config1_within_1e10(solver):
-    p = syn.config1()
+def test_fast_mode_inversion_step_121_within_1e10(solver):
+    p = syn.inversion_step_121()
     for ph in (0, 1):
         seeds = [point_source(p.grid, p.slowness[ph], *p.stations[q]) for q in (2, 13)]
         ref = oracle_fields(p.grid, p.slowness[ph], seeds)
@@ -294,7 +294,7 @@ def test_fast_mode_full_size_field_within_1e10(solver):
     """One field of the 401×401×121 forward step: fast mode against the bitwise engine (which equals
     the reference's Relax to the bit) within 1e-10 relative; float32 tables within 2e-5 (their
     rounding)."""
-    p = syn.config4(n_stations=2, n_events=10, n_rays=10)
+    p = syn.regional_401(n_stations=2, n_events=10, n_rays=10)
     seeds = [point_source(p.grid, p.slowness[1], *p.stations[0])]
     exact = solver.solve(p.grid, p.slowness[1], seeds, precision=64, mode=L.MODE_ENGINE)
     fast = solver.solve(p.grid, p.slowness[1], seeds, precision=64, mode=L.MODE_FAST)
@@ -327,9 +327,9 @@ def test_flow_scheduler_all_tile_shapes(solver, mode):
         lib.ts_engine_set_tile(solver.handle, 64, 0)
 
 
-def test_flow_scheduler_config1_batch(solver):
+def test_flow_scheduler_inversion_step_121_batch(solver):
     """A batch of config-1 fields (P and S) under the flow scheduler equals the lockstep one."""
-    p = syn.config1()
+    p = syn.inversion_step_121()
     seeds = [point_source(p.grid, p.slowness[0], *p.stations[q]) for q in range(6)]
     lib = L.load()
     a = solver.solve(p.grid, p.slowness[0], seeds, precision=64, mode=L.MODE_FAST)

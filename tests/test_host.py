@@ -37,8 +37,8 @@ def test_interpolate_and_resample_match_oracle():
     assert abs(res[q] - O.interpolate(og, field, lon[7], lat[5], dep[3])) < 1e-12
 
 
-def test_config0_inputs():
-    p = syn.config0()
+def test_single_source_61_inputs():
+    p = syn.single_source_61()
     assert (p.grid.nx, p.grid.ny, p.grid.nz) == (61, 61, 31)
     assert (p.inv.nx, p.inv.ny, p.inv.nz) == (31, 31, 16)
     assert p.slowness.shape == (1, p.grid.count)
@@ -49,8 +49,8 @@ def test_config0_inputs():
     assert abs(p.grid.min_spacing_km() - 1.0) < 0.01
 
 
-def test_config1_inputs():
-    p = syn.config1()
+def test_inversion_step_121_inputs():
+    p = syn.inversion_step_121()
     assert (p.grid.nx, p.grid.ny, p.grid.nz) == (121, 121, 61)
     assert p.slowness.shape == (2, p.grid.count)
     assert len(p.stations) == 25 and len(p.events) == 150 and len(p.arrivals) == 7500

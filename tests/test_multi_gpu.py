@@ -19,7 +19,7 @@ F32_REL_TOL = 2e-5
 
 @pytest.fixture(scope="module")
 def batch():
-    b = syn.config2(n_sources=10, seed=3, dims_scale=0.22)
+    b = syn.uneven_grids(n_sources=10, seed=3, dims_scale=0.22)
     seeds = [point_source(g, s, *src) for g, s, src in zip(b.grids, b.slowness, b.sources)]
     return b, seeds
 

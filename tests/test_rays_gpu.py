@@ -47,17 +47,17 @@ def compare_rows(gpu, nnz, nodes, lens, tg):
     return worst_len
 
 
-def config0_tables():
-    p = syn.config0()
+def single_source_61_tables():
+    p = syn.single_source_61()
     og = O.Grid.of(p.grid)
     si, st = point_source(p.grid, p.slowness[0], *p.stations[0])
     t, ok, _ = O.relax(og, p.slowness[0], si, st)
     return p, O.to_table(t)
 
 
-def test_trace_rows_config0_vs_oracle(solver):
-    """Config 0: 25 surface receivers traced back to the source at (30, 30, 10) km."""
-    p, tb = config0_tables()
+def test_trace_rows_single_source_61_vs_oracle(solver):
+    """61×61×31 at 1 km: 25 surface receivers traced back to the source at (30, 30, 10) km."""
+    p, tb = single_source_61_tables()
     step = p.step_km
     gpu = trace_rows(solver, p.grid, tb[None, :], p.stations, p.inv, np.zeros(25, np.int32), p.events, step)
     nnz, nodes, lens, tg = O.ray_rows_many(O.Grid.of(p.grid), tb[None, :], np.zeros(25, np.int32),
@@ -69,7 +69,7 @@ def test_trace_rows_config0_vs_oracle(solver):
 def test_trace_rows_edge_cases(solver):
     """Events outside the grid (clamped), at the station, on the surface and at the bottom, and an
     event in an unreached region (dropped)."""
-    p, tb = config0_tables()
+    p, tb = single_source_61_tables()
     g = p.grid
     st = p.stations[0]
     ev = np.array([
@@ -93,9 +93,9 @@ def test_trace_rows_edge_cases(solver):
     compare_rows(gpu, nnz, nodes, lens, tg)
 
 
-def test_trace_rows_config1_sample_vs_oracle(solver):
-    """Config 1: 600 P and S rays (a seeded sample of the 7,500) on oracle tables."""
-    p = syn.config1()
+def test_trace_rows_inversion_step_121_sample_vs_oracle(solver):
+    """121×121×61 at 0.5 km: 600 P and S rays (a seeded sample of the 7,500) on oracle tables."""
+    p = syn.inversion_step_121()
     og = O.Grid.of(p.grid)
     st_ids = [0, 4, 11]
     tabs, tstations = [], []
@@ -115,9 +115,9 @@ def test_trace_rows_config1_sample_vs_oracle(solver):
     assert gpu.nnz == int(nnz[nnz >= 0].sum())
 
 
-def test_forward_step_config0_f64(solver):
+def test_forward_step_single_source_61_f64(solver):
     """RayKernels.Compute on the device (tables + rays) against the oracle pipeline, FP64."""
-    p, tb = config0_tables()
+    p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
     gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64)
     nnz, nodes, lens, tg = O.ray_rows_many(O.Grid.of(p.grid), tb[None, :], np.zeros(25, np.int32),
@@ -129,7 +129,7 @@ def test_forward_step_config0_f64(solver):
 
 def test_forward_step_f32_close(solver):
     """The FP32 forward step: rows close to the FP64 oracle's (tables differ by the FP32 error)."""
-    p, tb = config0_tables()
+    p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
     gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=32)
     nnz, nodes, lens, tg = O.ray_rows_many(O.Grid.of(p.grid), tb[None, :], np.zeros(25, np.int32),
@@ -143,7 +143,7 @@ def test_forward_step_f32_close(solver):
 
 def test_row_time_consistency(solver):
     """Σ length·slowness of each row is close to TCalc (the reference's 'rays' validation, <5 %)."""
-    p, tb = config0_tables()
+    p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
     gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64)
     s_inv = p.slowness[0].reshape(p.grid.shape)[::2, ::2, ::2].reshape(-1)  # inversion nodes are every other

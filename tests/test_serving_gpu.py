@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def models():
-    return syn.config3_models()
+    return syn.serving_models()
 
 
 def submit_spec(server, ids, models, r, tables=True):
@@ -34,7 +34,7 @@ def rows_equal(a, b):
 
 
 def test_solo_equals_mix_equals_one_shot(models, solver):
-    stream = syn.config3_stream(models, rate=200, duration=0.25, seed=4)
+    stream = syn.serving_stream(models, rate=200, duration=0.25, seed=4)
     kinds = {r.kind for r in stream}
     assert {"eikonal+rays", "resolution"} <= kinds
     with Server(tile=2, budget_bytes=16e9, rounds_per_epoch=1) as server:
@@ -72,7 +72,7 @@ def test_solo_equals_mix_equals_one_shot(models, solver):
 
 def test_admission_keeps_within_budget(models, solver):
     m = models["checker81"]
-    stream = [r for r in syn.config3_stream(models, rate=200, duration=1.0, seed=4) if r.kind == "resolution"][:4]
+    stream = [r for r in syn.serving_stream(models, rate=200, duration=1.0, seed=4) if r.kind == "resolution"][:4]
     # Room for a little more than one resolution batch at a time: 25 fields of 81×81×41 hold 3.57 MB
     # each (8×8×4 tiles, FP64 field, due masks and its float32 table).
     budget = 1.3 * 25 * 3.57e6
@@ -105,7 +105,7 @@ def test_request_beyond_budget_is_refused(models):
 def test_flow_scheduler_time_budgeted_epochs(models, solver):
     """Flow scheduler with epochs that end on time (fields pausing at a round end after 5 ms): every
     request still gets the one-shot engine's bits."""
-    stream = syn.config3_stream(models, rate=200, duration=0.1, seed=4)
+    stream = syn.serving_stream(models, rate=200, duration=0.1, seed=4)
     with Server(tile=4, budget_bytes=16e9, rounds_per_epoch=8, scheduler=1, epoch_ms=5.0) as server:
         ids = {name: server.model_put(m.grid, m.slowness) for name, m in models.items()}
         rid = [submit_spec(server, ids, models, r) for r in stream]

@@ -45,8 +45,8 @@ def test_struct_layouts_match_the_header(tmp_path):
 
 
 def test_serving_load_mix_and_rate():
-    models = syn.config3_models()
-    stream = syn.config3_stream(models, rate=200, duration=60, seed=4)
+    models = syn.serving_models()
+    stream = syn.serving_stream(models, rate=200, duration=60, seed=4)
     n = len(stream)
     assert abs(n - 12000) < 4 * np.sqrt(12000)
     kinds = np.array([r.kind for r in stream])
@@ -61,7 +61,7 @@ def test_serving_load_mix_and_rate():
     eik = [r for r in stream if r.kind == "eikonal+rays"]
     assert all(20 <= len(r.events) <= 150 and r.model == "forward121" for r in eik)
     # Deterministic from the stream seed.
-    again = syn.config3_stream(models, rate=200, duration=60, seed=4)
+    again = syn.serving_stream(models, rate=200, duration=60, seed=4)
     assert np.allclose([r.t for r in again[:50]], t[:50])
     assert models["forward121"].grid.shape == (61, 121, 121)
     assert models["reloc161"].grid.count == 161 * 161 * 81

@@ -46,7 +46,7 @@ def regular_solve(solver, grid, slowness, seeds):
 
 def test_no_alloc_matches_regular_entry_point_twice(solver):
     """Two calls in a row on different inputs, each equal to ts_eik_solve's field."""
-    p = syn.config0()
+    p = syn.single_source_61()
     a_seeds = point_source(p.grid, p.slowness[0], *p.stations[0])
     a, ra = no_alloc_solve(p.grid, p.slowness[0], a_seeds)
     assert np.array_equal(a, regular_solve(solver, p.grid, p.slowness[0], a_seeds))

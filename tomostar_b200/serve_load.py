@@ -19,8 +19,8 @@ from .serving import Server
 def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 2, rounds_per_epoch: int = 1,
         budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 0,
         epoch_ms: float = 0.0) -> dict:
-    models = syn.config3_models()
-    stream = syn.config3_stream(models, rate=rate, duration=seconds, seed=seed)
+    models = syn.serving_models()
+    stream = syn.serving_stream(models, rate=rate, duration=seconds, seed=seed)
     # Seeds of every field on the host before the clock starts (PointSource, ts_point_source).
     prepared = []
     for r in stream:

@@ -81,7 +81,7 @@ def vp_linear(grid: GridDef, v0: float = 5.0, grad: float = 0.03) -> np.ndarray:
     return np.broadcast_to((v0 + grad * dep)[:, None, None], grid.shape).reshape(-1).copy()
 
 
-def config0() -> Problem:
+def single_source_61() -> Problem:
     """61×61×31 at 1 km; Vp = (5 + 0.03 z)·(1 ± 5 % checkerboard of 10 km); source (30, 30, 10) km;
     25 receivers uniformly at random on the surface (seed 0). FP64, compared with the CPU solver."""
     h = 1.0
@@ -93,12 +93,12 @@ def config0() -> Problem:
     rlon, rlat = km_to_geo(g, xy[:, 0], xy[:, 1], h)
     events = np.stack([rlon, rlat, np.zeros(25)], axis=1)
     arrivals = np.stack([np.arange(25), np.zeros(25, int), np.zeros(25, int)], axis=1).astype(np.int32)
-    return Problem("config0", g, g.coarsened(2), (1 / vp)[None, :], np.array([[slon, slat, 10.0]]), events,
+    return Problem("single_source_61", g, g.coarsened(2), (1 / vp)[None, :], np.array([[slon, slat, 10.0]]), events,
                    arrivals, h)
 
 
-def config1() -> Problem:
-    """121×121×61 at 0.5 km; Vp as config 0; Vp/Vs = 1.73·(1 ± 3 % checkerboard of 10 km); 25 surface
+def inversion_step_121() -> Problem:
+    """121×121×61 at 0.5 km; Vp as the 61×61×31 model; Vp/Vs = 1.73·(1 ± 3 % checkerboard of 10 km); 25 surface
     stations (seed 1), 150 events in the box at 2–20 km depth (seed 2); P and S: 50 fields, 7,500 rays."""
     h = 0.5
     g = regular_grid(121, 121, 61, h)
@@ -115,7 +115,7 @@ def config1() -> Problem:
     events = np.stack([elon, elat, exyz[:, 2]], axis=1)
     ev, st, ph = np.meshgrid(np.arange(150), np.arange(25), np.arange(2), indexing="ij")
     arrivals = np.stack([ev.ravel(), st.ravel(), ph.ravel()], axis=1).astype(np.int32)
-    return Problem("config1", g, g.coarsened(2), np.stack([1 / vp, 1 / vs]), stations, events, arrivals, h)
+    return Problem("inversion_step_121", g, g.coarsened(2), np.stack([1 / vp, 1 / vs]), stations, events, arrivals, h)
 
 
 def selftest_case():
@@ -150,7 +150,7 @@ def ellipsoid_bodies(grid: GridDef, h_km: float, rng, n: int = 3, amplitude: flo
     return out.reshape(-1)
 
 
-def config4(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000, seed: int = 5) -> Problem:
+def regional_401(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000, seed: int = 5) -> Problem:
     """401×401×121 at 0.25 km (19.46 M nodes): Vp = 5 + 0.04 z km/s plus three ellipsoidal ±8 % bodies,
     Vs = Vp / 1.73; 400 surface stations and 5,000 events (2–25 km deep) → 800 P and S fields;
     1.5 M (event, station, phase) arrivals drawn uniformly without replacement. One generator,
@@ -175,7 +175,7 @@ def config4(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000
     slow = np.empty((2, g.count))
     np.divide(1.0, vp, out=slow[0])
     np.divide(1.0, vs, out=slow[1])
-    return Problem("config4", g, g.coarsened(2), slow, stations, events, arrivals, h)
+    return Problem("regional_401", g, g.coarsened(2), slow, stations, events, arrivals, h)
 
 
 @dataclass
@@ -198,7 +198,7 @@ def smooth3(a: np.ndarray) -> np.ndarray:
     return a
 
 
-def config2(n_sources: int = 200, seed: int = 3, variable_share: float = 0.5,
+def uneven_grids(n_sources: int = 200, seed: int = 3, variable_share: float = 0.5,
             dims_scale: float = 1.0) -> GridBatch:
     """200 sources, each on its own grid: nx, ny uniform in 48–192, nz in 32–96, spacing h uniform in
     0.25–1 km. Half the grids (a coin per grid) have depth levels whose spacing grows geometrically
@@ -233,7 +233,7 @@ def config2(n_sources: int = 200, seed: int = 3, variable_share: float = 0.5,
         slow.append((1.0 / vp).reshape(-1))
         src.append((lon, lat, fz * g.max_depth_km))
         hs.append(h)
-    return GridBatch("config2", grids, slow, np.asarray(src), np.asarray(hs))
+    return GridBatch("uneven_grids", grids, slow, np.asarray(src), np.asarray(hs))
 
 
 @dataclass
@@ -291,12 +291,12 @@ def spikes(grid: GridDef, h_km: float, cell_km: float, amplitude_percent: float,
     return out.reshape(-1)
 
 
-def config3_models() -> dict:
+def serving_models() -> dict:
     """Resident models of the serving load: the 121×121×61 forward model of the inversion step
-    (config 1, P and S); two 81×81×41 resolution-test models at 1 km (Vp(z) times a ±5 %
+    (the 121×121×61 inversion-step model, P and S); two 81×81×41 resolution-test models at 1 km (Vp(z) times a ±5 %
     checkerboard and ±5 % spikes of 8 km cells); a 161×161×81 relocation model at 0.5 km (Vp(z),
     Vs = Vp/1.73)."""
-    p1 = config1()
+    p1 = inversion_step_121()
     models = {"forward121": ServeModel("forward121", p1.grid, p1.slowness, 0.5)}
     g81 = regular_grid(81, 81, 41, 1.0)
     v81 = vp_linear(g81)
@@ -309,7 +309,7 @@ def config3_models() -> dict:
     return models
 
 
-def config3_stream(models: dict, rate: float = 200.0, duration: float = 60.0, seed: int = 4) -> list:
+def serving_stream(models: dict, rate: float = 200.0, duration: float = 60.0, seed: int = 4) -> list:
     """The serving load: Poisson arrivals at `rate` per second for `duration` seconds, mixed 60 %
     single-station eikonal-plus-rays requests on forward121 (P or S, 20–150 rays from events at
     2–20 km), 25 % resolution-test batches of 25 fields on checker81 or spike81 (no rays), 15 %
