@@ -268,6 +268,26 @@ int ts_forward(ts_ctx* ctx, const ts_grid* fwd, const double* slowness, int32_t 
                int32_t n_arrivals, const int32_t* arr_event, const int32_t* arr_station, const int32_t* arr_phase,
                int32_t precision, double step_km, ts_rows** out, ts_eik_stats* stats);
 
+/* ---- LSQR on the device (Numerics/Lsqr.cs:33-152, LsqrOpenCl.cs) ----
+ * Damped LSQR, min ‖A x − b‖² + damp² ‖x‖², with the reference's stopping rules (atol, btol,
+ * conlim, iteration budget). stop: 0 empty system, 1 zero right-hand side, 2 Aᵀb = 0, 3 iteration
+ * budget, 4 btol, 5 atol, 6 conlim, 7–9 machine precision (residual, normal equations, condition),
+ * 10 bidiagonalisation terminated. The solve repeats to the bit on a given device and agrees with
+ * the sequential host solver to rounding. */
+typedef struct ts_lsqr_info {
+    int32_t iterations, stop;
+    double bnorm, rnorm, acond;   /* ‖b‖, ‖r‖ of the damped system, condition estimate */
+    double device_ms;             /* the iteration loop */
+} ts_lsqr_info;
+/* A as host CSR (row_ptr[m+1], col, val), b[m] on the host; x_out[n]. */
+int ts_lsqr_solve(ts_ctx* ctx, int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                  const double* b, double damp, int32_t max_iterations, double atol, double btol, double conlim,
+                  double* x_out, ts_lsqr_info* info);
+/* A = the rows of a ray result (ts_forward / ts_rays_trace) as they lie on the device, n columns
+ * (the inversion grid's nodes); rows the reference drops are empty and their b entries should be 0. */
+int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, double damp, int32_t max_iterations,
+                       double atol, double btol, double conlim, double* x_out, ts_lsqr_info* info);
+
 /* Sizes of a result: rows (= rays or arrivals) and total non-zeros. */
 int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz);
 /* Copies a result to the host: row_ptr[n_rows+1], col[nnz] (int32 node), len[nnz] (float32 km),

@@ -956,3 +956,136 @@ int32_t or_relax_wake(const or_grid_def* d, const double* slowness, int32_t n_se
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// ---- LSQR (Numerics/Lsqr.cs:33-152): damped LSQR of Paige & Saunders on a CSR matrix --------------
+// Sequential sums throughout; the transpose product is built the reference's way (CsrMatrix.Transpose,
+// SparseMatrix.cs:79-96: a stable counting sort by column, rows ascending within a column).
+// Stop codes: 0 empty system, 1 zero right-hand side, 2 Aᵀb = 0, 3 iteration budget, 4 btol,
+// 5 atol, 6 conlim, 7 residual at machine precision, 8 normal equations at machine precision,
+// 9 condition number at machine precision, 10 bidiagonalisation terminated.
+// info[4]: iterations, ‖b‖, ‖r‖, condition estimate.
+
+static double lsqr_dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0;
+    for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+    return s;
+}
+
+// SimdVector.Norm (Numerics/SimdVector.cs:33-45): scaled when the entries are extreme.
+static double lsqr_norm(const std::vector<double>& a) {
+    double mx = 0;
+    for (double x : a) mx = std::max(mx, std::fabs(x));
+    if (mx == 0 || !std::isfinite(mx)) return mx;
+    if (mx > 1e150 || mx < 1e-150) {
+        double s = 0, inv = 1.0 / mx;
+        for (double x : a) { double y = x * inv; s += y * y; }
+        return mx * std::sqrt(s);
+    }
+    return std::sqrt(lsqr_dot(a, a));
+}
+
+static void csr_mul(int32_t rows, const int32_t* rs, const int32_t* ci, const double* va, const std::vector<double>& x,
+                    std::vector<double>& y) {
+    for (int32_t i = 0; i < rows; i++) {
+        double s = 0;
+        for (int32_t k = rs[i]; k < rs[i + 1]; k++) s += va[k] * x[ci[k]];
+        y[i] = s;
+    }
+}
+
+int32_t or_lsqr(int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                double damp, int32_t max_iterations, double atol, double btol, double conlim, double* x_out,
+                double* info) {
+    std::vector<double> x(n, 0.0);
+    auto done = [&](int code, int it, double bn, double rn, double ac) {
+        for (int32_t j = 0; j < n; j++) x_out[j] = x[j];
+        info[0] = it; info[1] = bn; info[2] = rn; info[3] = ac;
+        return code;
+    };
+    if (m == 0 || n == 0) return done(0, 0, 0, 0, 0);
+    // Transpose (CsrMatrix.Transpose).
+    const int64_t nnz = row_ptr[m];
+    std::vector<int32_t> trs(n + 1, 0), tci(nnz);
+    std::vector<double> tva(nnz);
+    for (int64_t k = 0; k < nnz; k++) trs[col[k] + 1]++;
+    for (int32_t c = 0; c < n; c++) trs[c + 1] += trs[c];
+    std::vector<int32_t> next(trs.begin(), trs.end() - 1);
+    for (int32_t i = 0; i < m; i++)
+        for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; k++) {
+            int32_t p = next[col[k]]++;
+            tci[p] = i;
+            tva[p] = val[k];
+        }
+    std::vector<double> u(b, b + m), v(n), w(n), tm(m), tn(n);
+    double beta = lsqr_norm(u);
+    if (beta == 0) return done(1, 0, 0, 0, 0);
+    const double bnorm = beta;
+    for (auto& e : u) e *= 1.0 / beta;
+    csr_mul(n, trs.data(), tci.data(), tva.data(), u, v);
+    double alpha = lsqr_norm(v);
+    if (alpha == 0) return done(2, 0, bnorm, bnorm, 0);
+    for (auto& e : v) e *= 1.0 / alpha;
+    w = v;
+    double rhobar = alpha, phibar = beta;
+    double ddnorm = 0, xxnorm = 0, z = 0, cs2 = -1, sn2 = 0, anorm2 = 0, damped2 = 0, rnorm = beta, acond = 0;
+    const double ctol = conlim > 0 ? 1.0 / conlim : 0.0;
+    int stop = 3, it = 0;
+    for (int k = 0; k < max_iterations; k++) {
+        it = k + 1;
+        csr_mul(m, row_ptr, col, val, v, tm);
+        for (int32_t i = 0; i < m; i++) u[i] = tm[i] - alpha * u[i];
+        beta = lsqr_norm(u);
+        if (beta > 0) {
+            for (auto& e : u) e *= 1.0 / beta;
+            anorm2 += alpha * alpha + beta * beta + damp * damp;
+            csr_mul(n, trs.data(), tci.data(), tva.data(), u, tn);
+            for (int32_t j = 0; j < n; j++) v[j] = tn[j] - beta * v[j];
+            alpha = lsqr_norm(v);
+            if (alpha > 0) for (auto& e : v) e *= 1.0 / alpha;
+        }
+        double rhobar1 = std::sqrt(rhobar * rhobar + damp * damp);
+        double cs1 = rhobar / rhobar1, sn1 = damp / rhobar1;
+        double psi = sn1 * phibar;
+        phibar = cs1 * phibar;
+        double rho = std::sqrt(rhobar1 * rhobar1 + beta * beta);
+        double cs = rhobar1 / rho, sn = beta / rho;
+        double theta = sn * alpha;
+        rhobar = -cs * alpha;
+        double phi = cs * phibar;
+        phibar = sn * phibar;
+        double tau = sn * phi;
+        ddnorm += lsqr_dot(w, w) / (rho * rho);
+        double t1c = phi / rho, t2c = -theta / rho;
+        for (int32_t j = 0; j < n; j++) x[j] += t1c * w[j];
+        for (int32_t j = 0; j < n; j++) w[j] = v[j] + t2c * w[j];
+        double delta = sn2 * rho, gambar = -cs2 * rho, rhs = phi - delta * z;
+        double gamma = std::sqrt(gambar * gambar + theta * theta);
+        cs2 = gambar / gamma;
+        sn2 = theta / gamma;
+        z = rhs / gamma;
+        xxnorm += z * z;
+        damped2 += psi * psi;
+        double anorm = std::sqrt(anorm2);
+        acond = anorm * std::sqrt(ddnorm);
+        double arnorm = alpha * std::fabs(tau);
+        rnorm = std::sqrt(phibar * phibar + damped2);
+        double xnorm = std::sqrt(xxnorm);
+        double test1 = rnorm / bnorm;
+        double test2 = arnorm / std::max(1e-300, anorm * rnorm);
+        double test3 = 1.0 / std::max(1e-300, acond);
+        double t1 = test1 / (1 + anorm * xnorm / bnorm);
+        double rtol = btol + atol * anorm * xnorm / bnorm;
+        if (test1 <= rtol) { stop = 4; break; }
+        if (test2 <= atol) { stop = 5; break; }
+        if (ctol > 0 && test3 <= ctol) { stop = 6; break; }
+        if (1 + t1 <= 1) { stop = 7; break; }
+        if (1 + test2 <= 1) { stop = 8; break; }
+        if (1 + test3 <= 1) { stop = 9; break; }
+        if (beta == 0 || alpha == 0) { stop = 10; break; }
+    }
+    return done(stop, it, bnorm, rnorm, acond);
+}
+
+}  // extern "C"

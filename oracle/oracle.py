@@ -70,6 +70,7 @@ def lib():
             "or_ray_row": (i32, [g, fp, d, d, d, g, d, d, d, d, ip, fp, i32, dp]),
             "or_ray_rows_many": (None, [g, fp, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32]),
             "or_relax_wake": (i32, [g, dp, i32, ip, dp, d, d, i32, dp, ip, P(C.c_int64)]),
+            "or_lsqr": (i32, [i32, i32, ip, ip, dp, dp, d, i32, d, d, d, dp, dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -312,3 +313,23 @@ def ray_rows_many(fwd: Grid, tables, tab_of, stations, inv: Grid, events, step_k
                            _p(ev, C.c_double), nr, step_km, cap_per_row, _p(nnz, C.c_int32), _p(nodes, C.c_int32),
                            _p(lens, C.c_float), _p(tg, C.c_double), threads or os.cpu_count())
     return nnz, nodes.reshape(nr, cap_per_row), lens.reshape(nr, cap_per_row), tg
+
+
+LSQR_STOPS = ["empty system", "zero right-hand side", "A^T b = 0", "iteration budget exhausted",
+              "residual reduced to tolerance (btol)", "normal equations satisfied (atol)",
+              "condition-number limit reached (conlim)", "residual at machine precision",
+              "normal equations at machine precision", "condition number at machine precision",
+              "bidiagonalisation terminated"]
+
+
+def lsqr(m, n, row_ptr, col, val, b, damp=0.0, max_iterations=500, atol=1e-8, btol=1e-8, conlim=1e8):
+    """Lsqr.Solve (Numerics/Lsqr.cs:33-152) on a CSR matrix; returns (x, stop code, info dict)."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col, np.int32)
+    va = np.ascontiguousarray(val, np.float64)
+    bb = np.ascontiguousarray(b, np.float64)
+    x = np.empty(n)
+    info = np.empty(4)
+    code = lib().or_lsqr(m, n, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(va, C.c_double), _p(bb, C.c_double), damp,
+                         max_iterations, atol, btol, conlim, _p(x, C.c_double), _p(info, C.c_double))
+    return x, int(code), {"iterations": int(info[0]), "bnorm": info[1], "rnorm": info[2], "acond": info[3]}

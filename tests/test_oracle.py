@@ -186,3 +186,29 @@ def test_relax_wake_causal_rule_bound():
         assert ok and ok2 and np.array_equal(fin, np.isfinite(a))
         assert np.max(np.abs(a[fin] - b[fin]) / np.maximum(b[fin], 1e-9)) < 1e-10
         assert ev < ev_ref
+
+
+def test_lsqr_oracle_pinned_to_scipy():
+    """The LSQR restatement (Lsqr.cs) follows the SOL kernel SciPy's lsqr implements: the same first
+    iterates to rounding, the same stopping rule and solution at convergence, and the damped normal
+    equations' solution."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+
+    rng = np.random.default_rng(3)
+    A = sp.random(300, 120, density=0.05, random_state=4, format="csr")
+    b = rng.standard_normal(300)
+    for damp in (0.0, 0.3):
+        x5, code5, _ = O.lsqr(300, 120, A.indptr, A.indices, A.data, b, damp=damp, max_iterations=5, atol=0, btol=0,
+                              conlim=0)
+        r5 = sla.lsqr(A, b, damp=damp, atol=0, btol=0, conlim=0, iter_lim=5)
+        assert code5 == 3 and np.max(np.abs(x5 - r5[0])) <= 1e-12 * np.max(np.abs(r5[0]))
+        x, code, info = O.lsqr(300, 120, A.indptr, A.indices, A.data, b, damp=damp)
+        r = sla.lsqr(A, b, damp=damp, atol=1e-8, btol=1e-8, conlim=1e8, iter_lim=500)
+        assert code == 5 and r[1] == 2  # normal equations satisfied (atol) in both
+        assert np.max(np.abs(x - r[0])) <= 1e-6 * np.max(np.abs(r[0]))
+        xs = np.linalg.solve((A.T @ A).toarray() + damp ** 2 * np.eye(120), A.T @ b)
+        assert np.max(np.abs(x - xs)) <= 1e-6 * np.max(np.abs(xs))
+    # Degenerate systems end as the reference says.
+    _, code, _ = O.lsqr(300, 120, A.indptr, A.indices, A.data, np.zeros(300))
+    assert O.LSQR_STOPS[code] == "zero right-hand side"

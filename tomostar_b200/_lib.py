@@ -88,8 +88,17 @@ class ServeStats(C.Structure):
     ]
 
 
+class LsqrInfo(C.Structure):
+    """ts_lsqr_info."""
+
+    _fields_ = [("iterations", C.c_int32), ("stop", C.c_int32), ("bnorm", C.c_double), ("rnorm", C.c_double),
+                ("acond", C.c_double), ("device_ms", C.c_double)]
+
+
 _gp = _P(GridStruct)
 SIGNATURES = {
+    "ts_lsqr_solve": (C.c_int, [_vp, _i32, _i32, _ip, _ip, _dp, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
+    "ts_lsqr_solve_rows": (C.c_int, [_vp, _vp, _i32, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
     "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
     "ts_serve_destroy": (None, [_vp]),
     "ts_serve_set_epoch_ms": (C.c_int, [_vp, _d]),

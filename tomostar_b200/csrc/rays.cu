@@ -566,6 +566,14 @@ int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begi
 
 void free_rows(ts_rows* rows) { delete rows; }
 
+void rows_view(const ts_rows* rows, int* n_rows, int64_t* nnz, const int** row_ptr, const int** col, const float** len) {
+    *n_rows = rows->n_rows;
+    *nnz = rows->nnz;
+    *row_ptr = rows->row_ptr;
+    *col = rows->col;
+    *len = rows->len;
+}
+
 }  // namespace rays
 }  // namespace ts
 

@@ -29,6 +29,8 @@ int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const std::vector<const 
 // own (stream-ordered copies on the context's stream).
 int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begin, std::vector<ts_rows*>& parts);
 void free_rows(ts_rows* rows);
+// The device arrays of a result (row_ptr[n_rows + 1], col[nnz], len[nnz]).
+void rows_view(const ts_rows* rows, int* n_rows, int64_t* nnz, const int** row_ptr, const int** col, const float** len);
 
 }  // namespace rays
 }  // namespace ts
