@@ -75,8 +75,14 @@ def test_lsqr_on_device_resident_rays(solver):
     assert rc == 0, solver.last_error
     n = p.inv.count
     b = np.random.default_rng(9).standard_normal(len(ar)) * 0.05
+    with pytest.raises(L.TsError):  # columns beyond n are refused, not written
+        lsqr.solve_rows(solver, h, 10, b)
     d = lsqr.solve_rows(solver, h, n, b, damp=0.1)
     rows = _fetch(h)  # copies the rows to the host and frees them
+    # The transpose built on the device equals the host's (the reference's order): the same system
+    # given as host CSR runs the same device arithmetic, so the solutions agree to the bit.
+    h_res = lsqr.solve(solver, rows.row_ptr, rows.col, rows.len.astype(np.float64), n, b, damp=0.1)
+    assert np.array_equal(h_res.solution, d.solution) and h_res.iterations == d.iterations
     o, code, info = O.lsqr(len(ar), n, rows.row_ptr, rows.col, rows.len.astype(np.float64), b, damp=0.1)
     assert d.stop == code
     assert np.max(np.abs(d.solution - o)) <= 1e-8 * np.max(np.abs(o))

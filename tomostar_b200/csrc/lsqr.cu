@@ -9,8 +9,8 @@
 // Partial sums are reduced in a fixed order, so a solve repeats to the bit on a given device; it
 // agrees with the sequential host solver to rounding (the sums are ordered differently).
 //
-// The transpose is the reference's (CsrMatrix.Transpose, SparseMatrix.cs:79-96): a stable counting
-// sort by column on the host, rows ascending within each column.
+// The transpose is the reference's (CsrMatrix.Transpose, SparseMatrix.cs:79-96): rows ascending within
+// each column; built on the host for a host matrix and on the device for device-resident rows.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -102,6 +102,51 @@ __global__ void gather_values(int64_t nnz, const int* __restrict__ perm, const f
 __global__ void widen(int64_t nnz, const float* __restrict__ len, double* __restrict__ out) {
     for (int64_t p = blockIdx.x * int64_t(kThreads) + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * kThreads)
         out[p] = double(len[p]);
+}
+
+// ---- the transpose on the device, in the reference's order -------------------------------------
+// Counts per column, column pointers (a host scan of the counts), an unordered scatter, then each
+// column's entries put in ascending row order by their rank among the column's rows (rows are
+// distinct within a column), so the result equals CsrMatrix.Transpose entry for entry.
+
+// Entries whose column is not below `cols` are not counted (the host then refuses the matrix).
+__global__ void count_columns(int rows, int cols, const int* __restrict__ rs, const int* __restrict__ ci,
+                              int* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * kThreads + threadIdx.x) >> 5; i < rows; i += (gridDim.x * kThreads) >> 5)
+        for (int k = rs[i] + lane; k < rs[i + 1]; k += 32) {
+            const int c = ci[k];
+            if (unsigned(c) < unsigned(cols)) atomicAdd(&cnt[c], 1);
+        }
+}
+
+__global__ void scatter_columns(int rows, int cols, const int* __restrict__ rs, const int* __restrict__ ci,
+                                const int* __restrict__ cptr, int* __restrict__ cursor, int* __restrict__ trow,
+                                int* __restrict__ tsrc) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * kThreads + threadIdx.x) >> 5; i < rows; i += (gridDim.x * kThreads) >> 5)
+        for (int k = rs[i] + lane; k < rs[i + 1]; k += 32) {
+            const int c = ci[k];
+            if (unsigned(c) >= unsigned(cols)) continue;
+            const int p = cptr[c] + atomicAdd(&cursor[c], 1);
+            trow[p] = i;
+            tsrc[p] = k;
+        }
+}
+
+// One block per column: entry e goes to cptr[c] + (number of the column's rows smaller than its row).
+__global__ void order_columns(int cols, const int* __restrict__ cptr, const int* __restrict__ trow,
+                              const int* __restrict__ tsrc, int* __restrict__ tci, int* __restrict__ perm) {
+    for (int c = blockIdx.x; c < cols; c += gridDim.x) {
+        const int b = cptr[c], e = cptr[c + 1];
+        for (int q = b + threadIdx.x; q < e; q += kThreads) {
+            const int r = trow[q];
+            int rank = 0;
+            for (int t = b; t < e; t++) rank += trow[t] < r;
+            tci[b + rank] = r;
+            perm[b + rank] = tsrc[q];
+        }
+    }
 }
 
 // CsrMatrix.Transpose: column pointers, row of each transposed entry and the entry it came from.
@@ -318,28 +363,39 @@ int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, d
     ts::rays::rows_view(rows, &m, &nnz, &rs, &ci, &len);
     if (n <= 0 || m == 0 || !b || !x_out) return ctx->fail(TS_E_ARG, "empty system or null array");
     cudaStream_t s = ctx->stream;
-    // The transpose's structure on the host (the reference's order); its values gathered on the device.
-    std::vector<int> hrs(static_cast<size_t>(m) + 1), hci(static_cast<size_t>(nnz));
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(hrs.data(), rs, sizeof(int) * (m + 1), cudaMemcpyDeviceToHost, s));
-    if (nnz) TS_CUDA_TRY(ctx, cudaMemcpyAsync(hci.data(), ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
-    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-    for (int64_t k = 0; k < nnz; k++)
-        if (uint32_t(hci[k]) >= uint32_t(n)) return ctx->fail(TS_E_ARG, "column index beyond n");
-    std::vector<int> trs, tci, perm;
-    transpose_host(m, n, hrs.data(), hci.data(), trs, tci, perm);
+    // The transpose built on the device in the reference's order; its values gathered there too.
     TS_BUF(ctx, d_va, double, "lsqr.va", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_trs, int, "lsqr.trs", n + 1);
     TS_BUF(ctx, d_tci, int, "lsqr.tci", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_tva, double, "lsqr.tva", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_perm, int, "lsqr.perm", std::max<int64_t>(1, nnz));
+    TS_BUF(ctx, d_trow, int, "lsqr.trow", std::max<int64_t>(1, nnz));
+    TS_BUF(ctx, d_tsrc, int, "lsqr.tsrc", std::max<int64_t>(1, nnz));
+    TS_BUF(ctx, d_cnt, int, "lsqr.cnt", n);
+    TS_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(int) * n, s));
+    count_columns<<<kBlocks * 8, kThreads, 0, s>>>(m, n, rs, ci, d_cnt);
+    TS_CUDA_TRY(ctx, cudaGetLastError());
+    std::vector<int> trs(static_cast<size_t>(n) + 1, 0);
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(trs.data() + 1, d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    int64_t total = 0;
+    for (int c = 0; c < n; c++) {
+        total += trs[c + 1];
+        trs[c + 1] = int(total);
+    }
+    if (total != nnz) return ctx->fail(TS_E_ARG, "column index beyond n");
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_trs, trs.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_tci, tci.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
-    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
+    TS_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(int) * n, s));
+    scatter_columns<<<kBlocks * 8, kThreads, 0, s>>>(m, n, rs, ci, d_trs, d_cnt, d_trow, d_tsrc);
+    order_columns<<<std::min(n, 262140), kThreads, 0, s>>>(n, d_trs, d_trow, d_tsrc, d_tci, d_perm);
     widen<<<kBlocks * 4, kThreads, 0, s>>>(nnz, len, d_va);
     gather_values<<<kBlocks * 4, kThreads, 0, s>>>(nnz, d_perm, len, d_tva);
     TS_CUDA_TRY(ctx, cudaGetLastError());
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     ctx->release("lsqr.perm");
+    ctx->release("lsqr.trow");
+    ctx->release("lsqr.tsrc");
+    ctx->release("lsqr.cnt");
     System A{m, n, nnz, rs, ci, d_trs, d_tci, d_va, d_tva};
     return run(ctx, A, b, damp, max_iterations, atol, btol, conlim, x_out, info);
 }
