@@ -287,6 +287,19 @@ int ts_lsqr_solve(ts_ctx* ctx, int32_t m, int32_t n, const int32_t* row_ptr, con
  * (the inversion grid's nodes); rows the reference drops are empty and their b entries should be 0. */
 int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, double damp, int32_t max_iterations,
                        double atol, double btol, double conlim, double* x_out, ts_lsqr_info* info);
+/* The rows' transpose is built on the device in CsrMatrix.Transpose's order (SparseMatrix.cs:79-96);
+ * a column index not below n is refused with TS_E_ARG. */
+
+/* Lsqr.Solve's onIteration (Lsqr.cs:43,140; LsqrOpenCl.TrySolve's, LsqrOpenCl.cs:250-256): fn is called
+ * on the calling thread after every iteration with the iteration number (from 1) and ‖r‖ of the damped
+ * system. NULL removes it. */
+typedef void (*ts_lsqr_iteration_fn)(int32_t iteration, double rnorm, void* user);
+int ts_lsqr_set_callback(ts_ctx* ctx, ts_lsqr_iteration_fn fn, void* user);
+/* LsqrOpenCl.SelfTest (LsqrOpenCl.cs:541-557): a random 3000 x 1200 damped system with 12 non-zeros per
+ * row solved on the device and by the sequential host solver (damp 0.05, 300 iterations, atol = btol =
+ * 1e-12, conlim 1e10); *rel_err = max |dx| / max |x_host|. TS_OK when <= 1e-8 (SelfTestTolerance, :33),
+ * otherwise TS_E_SELFTEST. */
+int ts_lsqr_selftest(ts_ctx* ctx, double* rel_err, char* msg, int32_t cap);
 
 /* Sizes of a result: rows (= rays or arrivals) and total non-zeros. */
 int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz);

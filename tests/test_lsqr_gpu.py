@@ -44,6 +44,30 @@ def test_lsqr_matches_oracle(solver, damp):
     assert np.array_equal(again.solution, d.solution) and again.iterations == d.iterations
 
 
+def test_lsqr_self_test_gate(solver):
+    """LsqrOpenCl.SelfTest's gate: the device and the sequential host solver on a random damped
+    3000 x 1200 system, 12 non-zeros per row, agree within SelfTestTolerance = 1e-8."""
+    rel, message = lsqr.self_test(solver)
+    assert rel <= lsqr.SELF_TEST_TOLERANCE, message
+    assert "iterations" in message
+
+
+def test_lsqr_on_iteration(solver):
+    """onIteration (Lsqr.cs:140): one call per iteration, numbered from 1, with the ‖r‖ the result
+    reports last; LSQR's ‖r‖ never increases. Removed after the call."""
+    A, b = system()
+    seen = []
+    r = lsqr.solve(solver, A.indptr, A.indices, A.data, A.shape[1], b, damp=0.1,
+                   on_iteration=lambda it, rn: seen.append((it, rn)))
+    assert [it for it, _ in seen] == list(range(1, r.iterations + 1))
+    assert seen[-1][1] == r.residual_norm
+    rn = np.array([v for _, v in seen])
+    assert np.all(np.diff(rn) <= 1e-12 * rn[0])
+    calls = len(seen)
+    lsqr.solve(solver, A.indptr, A.indices, A.data, A.shape[1], b, damp=0.1)
+    assert len(seen) == calls
+
+
 def test_lsqr_degenerate_systems(solver):
     A, b = system()
     m, n = A.shape

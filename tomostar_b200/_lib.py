@@ -99,6 +99,8 @@ _gp = _P(GridStruct)
 SIGNATURES = {
     "ts_lsqr_solve": (C.c_int, [_vp, _i32, _i32, _ip, _ip, _dp, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
     "ts_lsqr_solve_rows": (C.c_int, [_vp, _vp, _i32, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
+    "ts_lsqr_set_callback": (C.c_int, [_vp, C.c_void_p, _vp]),
+    "ts_lsqr_selftest": (C.c_int, [_vp, _dp, C.c_char_p, _i32]),
     "ts_serve_create": (C.c_int, [_i32, _i32, _i32, _i32, _i32, _d, _i32, _P(_vp)]),
     "ts_serve_destroy": (None, [_vp]),
     "ts_serve_set_epoch_ms": (C.c_int, [_vp, _d]),

@@ -239,5 +239,10 @@ inline int point_source(const Grid& g, const double* slowness, double lon, doubl
 std::vector<double> relax_for_selftest(const Grid& g, const double* slowness, const std::vector<int32_t>& seed_idx,
                                        const std::vector<double>& seed_t);
 
+// The LSQR self-test gate's host solver: Lsqr.Solve (Numerics/Lsqr.cs:33-152), sequential sums.
+// Returns the iteration count and writes x[n].
+int lsqr_for_selftest(int m, int n, const int32_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                      double damp, int max_it, double atol, double btol, double conlim, double* x);
+
 }  // namespace host
 }  // namespace ts

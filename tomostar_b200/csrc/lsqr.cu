@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "host_geo.h"
 #include "rays.h"
 
 namespace ts {
@@ -289,6 +290,7 @@ static int run(ts_ctx* ctx, const System& A, const double* b, double damp, int m
         const double arnorm = alpha * std::fabs(tau);
         rnorm = std::sqrt(phibar * phibar + damped2);
         const double xnorm = std::sqrt(xxnorm);
+        if (ctx->lsqr_on_iteration) ctx->lsqr_on_iteration(iterations, rnorm, ctx->lsqr_user);
         const double test1 = rnorm / bnorm;
         const double test2 = arnorm / std::max(1e-300, anorm * rnorm);
         const double test3 = 1.0 / std::max(1e-300, acond);
@@ -398,6 +400,76 @@ int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, d
     ctx->release("lsqr.cnt");
     System A{m, n, nnz, rs, ci, d_trs, d_tci, d_va, d_tva};
     return run(ctx, A, b, damp, max_iterations, atol, btol, conlim, x_out, info);
+}
+
+int ts_lsqr_set_callback(ts_ctx* ctx, ts_lsqr_iteration_fn fn, void* user) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    ctx->lsqr_on_iteration = fn;
+    ctx->lsqr_user = user;
+    return TS_OK;
+}
+
+int ts_lsqr_selftest(ts_ctx* ctx, double* rel_err, char* msg, int32_t cap) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    // A random sparse damped system with a few non-zeros per row, as a ray matrix has
+    // (LsqrOpenCl.TestSystem(3000, 1200, 12, 17), LsqrOpenCl.cs:559-573): distinct ascending columns,
+    // values in [0.1, 1.1), right-hand side in [-0.5, 0.5). Its own generator (splitmix64).
+    const int m = 3000, n = 1200, per_row = 12;
+    uint64_t state = 17;
+    auto next = [&]() {
+        uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    auto uniform = [&]() { return double(next() >> 11) * (1.0 / 9007199254740992.0); };
+    std::vector<int32_t> rp(m + 1, 0), ci;
+    std::vector<double> va, b(m);
+    for (int i = 0; i < m; i++) {
+        std::vector<int32_t> c;
+        while (int(c.size()) < per_row) {
+            int32_t q = int32_t(next() % uint64_t(n));
+            if (std::find(c.begin(), c.end(), q) == c.end()) c.push_back(q);
+        }
+        std::sort(c.begin(), c.end());
+        for (int32_t q : c) {
+            ci.push_back(q);
+            va.push_back(uniform() + 0.1);
+        }
+        b[i] = uniform() - 0.5;
+        rp[i + 1] = int32_t(ci.size());
+    }
+    // LsqrOpenCl.SelfTest (:541-557): damp 0.05, 300 iterations, atol = btol = 1e-12, conlim 1e10.
+    std::vector<double> host(n), dev(n);
+    const int host_it = ts::host::lsqr_for_selftest(m, n, rp.data(), ci.data(), va.data(), b.data(), 0.05, 300, 1e-12,
+                                                    1e-12, 1e10, host.data());
+    auto fn = ctx->lsqr_on_iteration;
+    ctx->lsqr_on_iteration = nullptr;  // the gate reports no iterations
+    ts_lsqr_info info{};
+    const int rc = ts_lsqr_solve(ctx, m, n, rp.data(), ci.data(), va.data(), b.data(), 0.05, 300, 1e-12, 1e-12, 1e10,
+                                 dev.data(), &info);
+    ctx->lsqr_on_iteration = fn;
+    char text[256];
+    double rel = INFINITY;
+    if (rc) {
+        std::snprintf(text, sizeof text, "%s", ctx->err.c_str());
+    } else {
+        double worst = 0, scale = 0;
+        for (int q = 0; q < n; q++) {
+            worst = std::max(worst, std::fabs(dev[q] - host[q]));
+            scale = std::max(scale, std::fabs(host[q]));
+        }
+        rel = worst / std::max(1e-300, scale);
+        std::snprintf(text, sizeof text, "max |dx| %.2E of max |x| after %d iterations (host %d)", rel,
+                      info.iterations, host_it);
+    }
+    if (rel_err) *rel_err = rel;
+    if (msg && cap > 0) std::snprintf(msg, size_t(cap), "%s", text);
+    if (rc) return rc;
+    // LsqrOpenCl.SelfTestTolerance (:33).
+    return rel <= 1e-8 ? TS_OK : ctx->fail(TS_E_SELFTEST, text);
 }
 
 }  // extern "C"

@@ -1,8 +1,11 @@
-// The self-test gate's host solver (EikonalOpenCl.SelfTest compares the device with
-// SphericalEikonal.Relax on the host, Forward/EikonalOpenCl.cs:346-374). Used by ts_cuda_selftest
-// only; no solve ever returns its result. Compiled with -ffp-contract=off.
+// The self-test gates' host solvers (EikonalOpenCl.SelfTest compares the device with
+// SphericalEikonal.Relax on the host, Forward/EikonalOpenCl.cs:346-374; LsqrOpenCl.SelfTest with
+// Lsqr.Solve, Numerics/LsqrOpenCl.cs:541-557). Used by ts_cuda_selftest and ts_lsqr_selftest only;
+// no solve ever returns their results. Compiled with -ffp-contract=off.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <vector>
 
 #include "host_geo.h"
 
@@ -102,6 +105,89 @@ std::vector<double> relax_for_selftest(const Grid& g, const double* slow, const 
             if (!changed) break;
         }
     return a;
+}
+
+// Lsqr.Solve (Numerics/Lsqr.cs:33-152), sequential, for LsqrOpenCl.SelfTest's host side
+// (Numerics/LsqrOpenCl.cs:541-557). Returns the iteration count; x has n entries.
+int lsqr_for_selftest(int m, int n, const int32_t* rp, const int32_t* ci, const double* va, const double* b,
+                      double damp, int max_it, double atol, double btol, double conlim, double* x) {
+    const size_t nn = static_cast<size_t>(n);
+    std::vector<double> u(b, b + m), v(nn, 0.0), w(nn, 0.0), tn(nn, 0.0);
+    std::fill(x, x + n, 0.0);
+    auto norm = [](const std::vector<double>& a) {
+        double s = 0;
+        for (double e : a) s += e * e;
+        return std::sqrt(s);
+    };
+    auto scale = [](std::vector<double>& a, double f) {
+        for (double& e : a) e *= f;
+    };
+    auto atx = [&](const std::vector<double>& in, std::vector<double>& out) {  // out = Aᵀ in
+        std::fill(out.begin(), out.end(), 0.0);
+        for (int i = 0; i < m; i++)
+            for (int e = rp[i]; e < rp[i + 1]; e++) out[ci[e]] += va[e] * in[i];
+    };
+    double beta = norm(u);
+    if (beta == 0) return 0;
+    const double bnorm = beta;
+    scale(u, 1.0 / beta);
+    atx(u, v);
+    double alpha = norm(v);
+    if (alpha == 0) return 0;
+    scale(v, 1.0 / alpha);
+    w = v;
+    double rhobar = alpha, phibar = beta, ddnorm = 0, xxnorm = 0, z = 0, cs2 = -1, sn2 = 0, anorm2 = 0, damped2 = 0;
+    const double ctol = conlim > 0 ? 1.0 / conlim : 0.0;
+    int it = 0;
+    while (it < max_it) {
+        it++;
+        for (int i = 0; i < m; i++) {
+            double acc = 0;
+            for (int e = rp[i]; e < rp[i + 1]; e++) acc += va[e] * v[ci[e]];
+            u[i] = acc - alpha * u[i];
+        }
+        beta = norm(u);
+        if (beta > 0) {
+            scale(u, 1.0 / beta);
+            anorm2 += alpha * alpha + beta * beta + damp * damp;
+            atx(u, tn);
+            for (int q = 0; q < n; q++) v[q] = tn[q] - beta * v[q];
+            alpha = norm(v);
+            if (alpha > 0) scale(v, 1.0 / alpha);
+        }
+        const double rhobar1 = std::sqrt(rhobar * rhobar + damp * damp);
+        const double cs1 = rhobar / rhobar1, sn1 = damp / rhobar1, psi = sn1 * phibar;
+        phibar = cs1 * phibar;
+        const double rho = std::sqrt(rhobar1 * rhobar1 + beta * beta);
+        const double cs = rhobar1 / rho, sn = beta / rho, theta = sn * alpha;
+        rhobar = -cs * alpha;
+        const double phi = cs * phibar;
+        phibar = sn * phibar;
+        const double tau = sn * phi;
+        double ww = 0;
+        for (double e : w) ww += e * e;
+        ddnorm += ww / (rho * rho);
+        for (int q = 0; q < n; q++) {
+            x[q] += phi / rho * w[q];
+            w[q] = v[q] - theta / rho * w[q];
+        }
+        const double delta = sn2 * rho, gambar = -cs2 * rho, rhs = phi - delta * z;
+        const double gamma = std::sqrt(gambar * gambar + theta * theta);
+        cs2 = gambar / gamma;
+        sn2 = theta / gamma;
+        z = rhs / gamma;
+        xxnorm += z * z;
+        damped2 += psi * psi;
+        const double anorm = std::sqrt(anorm2), acond = anorm * std::sqrt(ddnorm), arnorm = alpha * std::fabs(tau);
+        const double rnorm = std::sqrt(phibar * phibar + damped2), xnorm = std::sqrt(xxnorm);
+        const double test1 = rnorm / bnorm, test2 = arnorm / std::max(1e-300, anorm * rnorm);
+        const double test3 = 1.0 / std::max(1e-300, acond), t1 = test1 / (1 + anorm * xnorm / bnorm);
+        const double rtol = btol + atol * anorm * xnorm / bnorm;
+        if (test1 <= rtol || test2 <= atol || (ctol > 0 && test3 <= ctol) || 1 + t1 <= 1 || 1 + test2 <= 1 ||
+            1 + test3 <= 1 || beta == 0 || alpha == 0)
+            break;
+    }
+    return it;
 }
 
 }  // namespace host
