@@ -301,6 +301,60 @@ int ts_lsqr_set_callback(ts_ctx* ctx, ts_lsqr_iteration_fn fn, void* user);
  * otherwise TS_E_SELFTEST. */
 int ts_lsqr_selftest(ts_ctx* ctx, double* rel_err, char* msg, int32_t cap);
 
+/* ---- Travel-time tables kept on the device (TravelTimeTableSet, Forward/TravelTimeTable.cs:247-412) ----
+ * n_tables float32 fields on one uniform grid, node-major per table as a .qttb file holds them. */
+typedef struct ts_tables ts_tables;
+/* TravelTimeTableSet.Build (:264-308): table t is the field of the source sources[3t..3t+2] (lon, lat,
+ * depth km; seeds by PointSource, :373) for the slowness of phase source_phase[t] (slowness holds
+ * n_phases fields on grid), solved by the engine (bitwise the reference's sweeping) and rounded to
+ * float32 (TravelTimeTable.Write, :73). */
+int ts_tables_build(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int32_t n_phases, int32_t n_tables,
+                    const double* sources, const int32_t* source_phase, int32_t precision, ts_tables** out,
+                    ts_eik_stats* stats);
+/* Tables from the host (e.g. .qttb files read by TravelTimeTable.Open, :99-111). */
+int ts_tables_upload(ts_ctx* ctx, const ts_grid* grid, int32_t n_tables, const float* tables, ts_tables** out);
+int ts_tables_info(ts_tables* tables, int32_t* n_tables, int64_t* nodes_per_table);
+/* Tables first .. first+count-1 to the host (count * nodes floats). */
+int ts_tables_copy(ts_tables* tables, int32_t first, int32_t count, float* out);
+void ts_tables_free(ts_tables* tables);
+
+/* ---- Event location on resident tables (Location/EventLocator.cs:59-342, Relocation.cs:48-97) ---- */
+typedef struct ts_locator_settings {   /* LocatorSettings (EventLocator.cs:10-36); defaults in brackets */
+    int32_t global_search;             /* [1] whole grid on a stride lattice first; 0: within 6 nodes of the start */
+    int32_t coarse_candidates;         /* [8000] */
+    int32_t max_geiger_iterations;     /* [20] */
+    int32_t min_phases;                /* [4] */
+    double damping;                    /* [0.01] Levenberg-Marquardt damping relative to the diagonal */
+    double outlier_mads;               /* [4] */
+    double outlier_floor;              /* [0.5] s */
+    int32_t fix_depth;                 /* [0] */
+    int32_t reserved;
+} ts_locator_settings;
+typedef struct ts_location {           /* LocationResult + Hypocentre (EventLocator.cs:38, Model/Catalogue.cs:92-114) */
+    double t0;                         /* origin time, s after the event's reference time */
+    double lon, lat, depth_km;
+    double rms;                        /* s */
+    double err_h_km, err_minor_km, err_azimuth_deg, err_depth_km, err_time_s;  /* NaN: singular covariance */
+    double gap_deg;                    /* azimuthal gap of the stations in use */
+    int32_t used, rejected, iterations;
+    int32_t status;                    /* 0 ok; 1 fewer than min_phases observations; 2 local search box outside the grid */
+} ts_location;
+typedef struct ts_locate_stats {
+    double device_ms;                  /* the whole call on the device */
+    int64_t candidates;                /* grid-search nodes evaluated */
+    int32_t rounds, reserved;          /* location rounds run (outlier rejection relocates) */
+} ts_locate_stats;
+/* EventLocator.Locate for n_events events. Event e's observations are obs_offsets[e] ..
+ * obs_offsets[e+1]-1 (at most 1024): obs_table (its station's table for its phase), obs_seconds (the
+ * pick time in s after the event's reference time), obs_weight, obs_correction (the station
+ * correction). start: lon, lat, depth per event (the catalogue location). table_station: lon, lat of
+ * each table's station (the gap). residual_out[q]: every pick's residual at the solution (rejected
+ * picks included; NaN for an event not located). Not located (status != 0): the start is returned. */
+int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settings* settings, int32_t n_events,
+              const double* start, const int32_t* obs_offsets, const int32_t* obs_table, const double* obs_seconds,
+              const double* obs_weight, const double* obs_correction, const double* table_station, ts_location* out,
+              double* residual_out, ts_locate_stats* stats);
+
 /* Sizes of a result: rows (= rays or arrivals) and total non-zeros. */
 int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz);
 /* Copies a result to the host: row_ptr[n_rows+1], col[nnz] (int32 node), len[nnz] (float32 km),

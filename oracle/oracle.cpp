@@ -1089,3 +1089,411 @@ int32_t or_lsqr(int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col
 }
 
 }  // extern "C"
+
+// ---- Event location (Location/EventLocator.cs:59-342, Relocation.Absolute's per-event loop,
+// Location/Relocation.cs:48-97) -----------------------------------------------------------------
+// Settings and result follow LocatorSettings (EventLocator.cs:10-36) and LocationResult + Hypocentre
+// (EventLocator.cs:38, Model/Catalogue.cs:92-114). An event's observations are its usable picks with
+// a table (EventLocator.cs:64-73): the table, the pick time in s after the event's reference time,
+// the weight and the station correction. t0 is the origin time in s after the reference time.
+
+namespace {
+
+struct LocSettings {
+    int32_t global_search, coarse_candidates, max_geiger_iterations, min_phases;
+    double damping, outlier_mads, outlier_floor;
+    int32_t fix_depth, reserved;
+};
+
+struct LocResult {
+    double t0, lon, lat, depth_km, rms, err_h_km, err_minor_km, err_azimuth_deg, err_depth_km, err_time_s, gap_deg;
+    int32_t used, rejected, iterations, status;
+};
+
+struct LocObs {
+    const float* table;
+    double obs, weight, corr, st_lon, st_lat;
+};
+
+// Math.Max / Math.Min / Math.Clamp of .NET: NaN propagates, +0 preferred over -0 by Max.
+inline double net_max(double a, double b) {
+    if (std::isnan(a) || std::isnan(b)) return std::nan("");
+    if (a == b) return std::signbit(a) ? b : a;
+    return a > b ? a : b;
+}
+inline double net_clamp(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// DateTime.AddSeconds then (OriginTime - reference).TotalSeconds: t0 truncated to 100 ns ticks
+// (integral and fractional parts converted separately), then ticks / 1e7.
+inline double tick_seconds(double t0) {
+    double ip = std::trunc(t0);
+    double fp = t0 - ip;
+    int64_t ticks = int64_t(ip) * 10000000LL + int64_t(fp * 10000000.0);
+    return double(ticks) / 10000000.0;
+}
+
+// EventLocator.WeightedMedian (EventLocator.cs:297-309): NaN dropped, stable sort by value, the first
+// value whose running weight reaches half the total.
+double weighted_median(const std::vector<double>& v, const std::vector<double>& w) {
+    std::vector<std::pair<double, double>> p;
+    for (size_t i = 0; i < v.size(); i++)
+        if (!std::isnan(v[i])) p.push_back({v[i], w[i]});
+    std::stable_sort(p.begin(), p.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    if (p.empty()) return 0;
+    double sum = 0;
+    for (auto& e : p) sum += e.second;
+    double half = sum / 2, acc = 0;
+    for (auto& e : p) {
+        acc += e.second;
+        if (acc >= half) return e.first;
+    }
+    return p.back().first;
+}
+
+// EventLocator.Median (EventLocator.cs:311-317).
+double plain_median(const std::vector<double>& v) {
+    std::vector<double> s;
+    for (double x : v)
+        if (!std::isnan(x)) s.push_back(x);
+    if (s.empty()) return 0;
+    std::stable_sort(s.begin(), s.end(), [](double a, double b) { return a < b; });
+    size_t n = s.size();
+    return n % 2 == 1 ? s[n / 2] : 0.5 * (s[n / 2 - 1] + s[n / 2]);
+}
+
+// EventLocator.Gap (EventLocator.cs:320-327).
+double azimuth_gap(std::vector<double> az) {
+    std::vector<double> a;
+    for (double x : az)
+        if (std::find(a.begin(), a.end(), x) == a.end()) a.push_back(x);
+    std::sort(a.begin(), a.end());
+    if (a.size() < 2) return 360;
+    double gap = 360 - a.back() + a[0];
+    for (size_t i = 1; i < a.size(); i++) gap = std::max(gap, a[i] - a[i - 1]);
+    return gap;
+}
+
+// GeoMath.Azimuth (Geo/GeoMath.cs:98-107).
+double azimuth_deg(double lon1, double lat1, double lon2, double lat2) {
+    double p1 = lat1 * kDeg2Rad, p2 = lat2 * kDeg2Rad, dl = (lon2 - lon1) * kDeg2Rad;
+    double y = std::sin(dl) * std::cos(p2);
+    double x = std::cos(p1) * std::sin(p2) - std::sin(p1) * std::cos(p2) * std::cos(dl);
+    double az = std::atan2(y, x) * kRad2Deg;
+    return std::fmod(az + 360, 360);
+}
+
+// GeoMath.NormalizeLon and GeoMath.Destination (Geo/GeoMath.cs:123-138).
+double normalize_lon(double lon) {
+    lon = std::fmod(lon + 180, 360);
+    if (lon < 0) lon += 360;
+    return lon - 180;
+}
+void destination(double lon, double lat, double az_deg, double dist_km, double& lon2, double& lat2) {
+    double d = dist_km / kEarthRadiusKm;
+    double p1 = lat * kDeg2Rad, l1 = lon * kDeg2Rad, az = az_deg * kDeg2Rad;
+    double p2 = std::asin(std::sin(p1) * std::cos(d) + std::cos(p1) * std::sin(d) * std::cos(az));
+    double l2 = l1 + std::atan2(std::sin(az) * std::sin(d) * std::cos(p1), std::cos(d) - std::sin(p1) * std::sin(p2));
+    lon2 = normalize_lon(l2 * kRad2Deg);
+    lat2 = p2 * kRad2Deg;
+}
+
+// EventLocator.Solve (EventLocator.cs:259-282): Gauss-Jordan with partial pivoting; false for null.
+bool solve_small(const double a[4][4], const double* b, int n, double* x) {
+    double m[4][5];
+    for (int i = 0; i < n; i++) {
+        for (int j = 0; j < n; j++) m[i][j] = a[i][j];
+        m[i][n] = b[i];
+    }
+    for (int c = 0; c < n; c++) {
+        int p = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::fabs(m[r][c]) > std::fabs(m[p][c])) p = r;
+        if (std::fabs(m[p][c]) < 1e-30) return false;
+        if (p != c)
+            for (int j = 0; j <= n; j++) std::swap(m[c][j], m[p][j]);
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            double f = m[r][c] / m[c][c];
+            for (int j = c; j <= n; j++) m[r][j] -= f * m[c][j];
+        }
+    }
+    for (int i = 0; i < n; i++) x[i] = m[i][n] / m[i][i];
+    return true;
+}
+
+}  // namespace
+
+namespace {
+
+struct Locator {
+    const Grid& g;
+    const LocSettings& s;
+
+    // GridSearch's Misfit (EventLocator.cs:111-124): weighted median origin time, weighted L1 misfit.
+    double node_misfit(const std::vector<LocObs>& obs, int idx, double& t0) const {
+        std::vector<double> r(obs.size()), w(obs.size());
+        for (size_t q = 0; q < obs.size(); q++) {
+            float t = obs[q].table[idx];
+            r[q] = std::isfinite(t) ? obs[q].obs - double(t) - obs[q].corr : std::nan("");
+            w[q] = obs[q].weight;
+        }
+        t0 = weighted_median(r, w);
+        double m = 0;
+        for (size_t q = 0; q < obs.size(); q++) m += std::isnan(r[q]) ? 10 * w[q] : w[q] * std::fabs(r[q] - t0);
+        return m;
+    }
+
+    // Search (EventLocator.cs:143-163).
+    int search(const std::vector<LocObs>& obs, double start_dep, double start_lon, double start_lat, int i0, int i1,
+               int j0, int j1, int k0, int k1, int stride) const {
+        i0 = std::max(0, i0); j0 = std::max(0, j0); k0 = std::max(0, k0);
+        i1 = std::min(g.nx - 1, i1); j1 = std::min(g.ny - 1, j1); k1 = std::min(g.nz - 1, k1);
+        int best = -1;
+        double best_m = kInf;
+        if (s.fix_depth) {
+            double fx, fy, fz;
+            g.fractional(start_lon, start_lat, start_dep, fx, fy, fz);
+            k0 = k1 = std::clamp(int(std::nearbyint(fz)), 0, g.nz - 1);
+        }
+        // A box wholly outside the grid (a local search from a start far outside it): the reference
+        // would read past its table and Relocation.Absolute reports the exception; here -1.
+        if (i0 > i1 || j0 > j1 || k0 > k1) return -1;
+        for (int kk = k0; kk <= k1; kk += stride)
+            for (int jj = j0; jj <= j1; jj += stride)
+                for (int ii = i0; ii <= i1; ii += stride) {
+                    int idx = g.index(ii, jj, kk);
+                    double t0;
+                    double m = node_misfit(obs, idx, t0);
+                    if (m < best_m) { best_m = m; best = idx; }
+                }
+        return best < 0 ? g.index(i0, j0, k0) : best;
+    }
+
+    // GridSearch (EventLocator.cs:107-141).
+    bool grid_search(const std::vector<LocObs>& obs, double slon, double slat, double sdep, double& lon, double& lat,
+                     double& dep, double& t0) const {
+        int best;
+        if (s.global_search) {
+            int stride = std::max(1, int(std::ceil(std::cbrt(double(g.count()) / s.coarse_candidates))));
+            best = search(obs, sdep, slon, slat, 0, g.nx - 1, 0, g.ny - 1, 0, g.nz - 1, stride);
+            int bk = best / (g.nx * g.ny), bj = (best / g.nx) % g.ny, bi = best % g.nx;
+            best = search(obs, sdep, slon, slat, bi - 2 * stride, bi + 2 * stride, bj - 2 * stride, bj + 2 * stride,
+                          bk - 2 * stride, bk + 2 * stride, 1);
+        } else {
+            double fx, fy, fz;
+            g.fractional(slon, slat, sdep, fx, fy, fz);
+            int ci = int(std::nearbyint(fx)), cj = int(std::nearbyint(fy)), ck = int(std::nearbyint(fz));
+            best = search(obs, sdep, slon, slat, ci - 6, ci + 6, cj - 6, cj + 6, ck - 6, ck + 6, 1);
+            if (best < 0) return false;
+        }
+        int k = best / (g.nx * g.ny), j = (best / g.nx) % g.ny, i = best % g.nx;
+        node_misfit(obs, best, t0);
+        lon = g.lon[i];
+        lat = g.lat[j];
+        dep = s.fix_depth ? sdep : g.dep[k];
+        return true;
+    }
+
+    // Geiger's Misfit (EventLocator.cs:173-198).
+    double geiger_misfit(const std::vector<LocObs>& obs, int npar, double x, double y, double z, double t, bool normal,
+                         double ata[4][4], double* atb) const {
+        if (normal) {
+            std::memset(ata, 0, sizeof(double) * 16);
+            std::memset(atb, 0, sizeof(double) * 4);
+        }
+        double sum = 0;
+        int rows = 0;
+        for (const LocObs& o : obs) {
+            Table tb{g, o.table, 0, 0, 0};
+            double tt = tb.time(x, y, z);
+            if (!std::isfinite(tt)) continue;
+            double res = o.obs - t - tt - o.corr;
+            double w = o.weight * o.weight;
+            sum += w * res * res;
+            rows++;
+            if (!normal) continue;
+            double ge, gn, gz;
+            tb.gradient(x, y, z, ge, gn, gz);
+            double row[4] = {1, ge, gn, gz};
+            for (int a = 0; a < npar; a++) {
+                atb[a] += w * row[a] * res;
+                for (int b = 0; b < npar; b++) ata[a][b] += w * row[a] * row[b];
+            }
+        }
+        return rows >= npar ? sum : kInf;
+    }
+
+    // Geiger (EventLocator.cs:166-256).
+    int geiger(const std::vector<LocObs>& obs, double& lon, double& lat, double& dep, double& t0, LocResult& out) const {
+        const int npar = s.fix_depth ? 3 : 4;
+        double ata[4][4], atb[4];
+        double lambda = net_max(1e-6, s.damping);
+        double chi2 = geiger_misfit(obs, npar, lon, lat, dep, t0, true, ata, atb);
+        int it = 0;
+        for (; it < s.max_geiger_iterations && std::isfinite(chi2); it++) {
+            bool accepted = false, have_step = false;
+            double step[4] = {0, 0, 0, 0};
+            while (lambda < 1e8) {
+                double lhs[4][4];
+                std::memcpy(lhs, ata, sizeof lhs);
+                for (int a = 0; a < npar; a++) lhs[a][a] *= 1 + lambda;
+                have_step = solve_small(lhs, atb, npar, step);
+                if (!have_step) break;
+                double nlon, nlat;
+                destination(lon, lat, std::atan2(step[1], step[2]) * kRad2Deg,
+                            std::sqrt(step[1] * step[1] + step[2] * step[2]), nlon, nlat);
+                double tlon = net_clamp(unwrap_lon(nlon, g.centre_lon), g.lon[0], g.lon[g.nx - 1]);
+                double tlat = net_clamp(nlat, g.lat[0], g.lat[g.ny - 1]);
+                double tdep = s.fix_depth ? dep : net_clamp(dep + step[3], g.dep[0], g.dep[g.nz - 1]);
+                double tt0 = t0 + step[0];
+                double trial = geiger_misfit(obs, npar, tlon, tlat, tdep, tt0, false, ata, atb);
+                if (trial <= chi2) {
+                    lon = tlon; lat = tlat; dep = tdep; t0 = tt0;
+                    chi2 = geiger_misfit(obs, npar, lon, lat, dep, t0, true, ata, atb);
+                    lambda = net_max(1e-6, lambda / 10);
+                    accepted = true;
+                    break;
+                }
+                lambda *= 10;
+            }
+            if (!accepted || !have_step) break;
+            double moved = std::sqrt(step[1] * step[1] + step[2] * step[2] + (npar > 3 ? step[3] * step[3] : 0));
+            if (moved < 0.005 && std::fabs(step[0]) < 0.001) { it++; break; }
+        }
+        geiger_misfit(obs, npar, lon, lat, dep, t0, true, ata, atb);
+        double ss = 0;
+        for (const LocObs& o : obs) {
+            Table tb{g, o.table, 0, 0, 0};
+            double r = o.obs - t0 - tb.time(lon, lat, dep) - o.corr;
+            ss += r * r;
+        }
+        out.t0 = t0; out.lon = lon; out.lat = lat; out.depth_km = dep;
+        out.rms = std::sqrt(ss / double(obs.size()));
+        out.err_h_km = out.err_minor_km = out.err_azimuth_deg = out.err_depth_km = out.err_time_s = std::nan("");
+        // Invert (EventLocator.cs:284-295): column by column.
+        double cov[4][4];
+        bool ok = true;
+        for (int c = 0; c < npar && ok; c++) {
+            double e[4] = {0, 0, 0, 0}, col[4];
+            e[c] = 1;
+            ok = solve_small(ata, e, npar, col);
+            for (int r = 0; ok && r < npar; r++) cov[r][c] = col[r];
+        }
+        if (ok) {
+            double dof = std::max(1, int(obs.size()) - npar);
+            double scale = net_max(1, chi2 / dof);
+            double cee = cov[1][1] * scale, cnn = cov[2][2] * scale, cen = cov[1][2] * scale;
+            double tr = 0.5 * (cee + cnn);
+            double det = cee * cnn - cen * cen;
+            double root = std::sqrt(net_max(0, tr * tr - det));
+            out.err_h_km = std::sqrt(net_max(0, tr + root));
+            out.err_minor_km = std::sqrt(net_max(0, tr - root));
+            double theta = 0.5 * std::atan2(2 * cen, cee - cnn) * kRad2Deg;
+            out.err_azimuth_deg = std::fmod(std::fmod(90 - theta, 180) + 180, 180);
+            out.err_depth_km = npar > 3 ? std::sqrt(net_max(0, cov[3][3] * scale)) : 0;
+            out.err_time_s = std::sqrt(net_max(0, cov[0][0] * scale));
+        }
+        return it;
+    }
+
+    // Locate (EventLocator.cs:59-104). residual[q] for every observation (NaN when not located).
+    LocResult locate(const std::vector<LocObs>& all, double slon, double slat, double sdep, double* residual) const {
+        LocResult out{};
+        out.t0 = 0; out.lon = slon; out.lat = slat; out.depth_km = sdep;
+        out.rms = out.err_h_km = out.err_minor_km = out.err_azimuth_deg = out.err_depth_km = out.err_time_s =
+            out.gap_deg = std::nan("");
+        for (size_t q = 0; q < all.size(); q++) residual[q] = std::nan("");
+        if (int(all.size()) < s.min_phases) {
+            out.used = int(all.size());
+            out.status = 1;
+            return out;
+        }
+        std::vector<LocObs> used = all;
+        int rejected = 0, iterations = 0;
+        LocResult best{};
+        for (int round = 0; round < 3; round++) {
+            double lon, lat, dep, t0;
+            if (!grid_search(used, slon, slat, sdep, lon, lat, dep, t0)) {
+                out.status = 2;  // Relocation.Absolute's exception result: start kept, nothing used
+                return out;
+            }
+            iterations = geiger(used, lon, lat, dep, t0, best);
+            const double tq = tick_seconds(best.t0);
+            std::vector<double> res(used.size());
+            for (size_t q = 0; q < used.size(); q++) {
+                Table tb{g, used[q].table, 0, 0, 0};
+                res[q] = used[q].obs - tq - tb.time(best.lon, best.lat, best.depth_km) - used[q].corr;
+            }
+            double med = plain_median(res);
+            std::vector<double> dev(res.size());
+            for (size_t q = 0; q < res.size(); q++) dev[q] = std::fabs(res[q] - med);
+            double mad = 1.4826 * plain_median(dev);
+            double limit = net_max(s.outlier_floor, s.outlier_mads * mad);
+            std::vector<LocObs> keep;
+            for (size_t q = 0; q < used.size(); q++)
+                if (std::fabs(res[q] - med) <= limit) keep.push_back(used[q]);
+            if (keep.size() == used.size() || int(keep.size()) < s.min_phases) break;
+            rejected += int(used.size() - keep.size());
+            used = keep;
+        }
+        const double tq = tick_seconds(best.t0);
+        for (size_t q = 0; q < all.size(); q++) {
+            Table tb{g, all[q].table, 0, 0, 0};
+            residual[q] = all[q].obs - tq - tb.time(best.lon, best.lat, best.depth_km) - all[q].corr;
+        }
+        std::vector<double> az;
+        for (const LocObs& o : used) az.push_back(azimuth_deg(best.lon, best.lat, o.st_lon, o.st_lat));
+        best.gap_deg = azimuth_gap(az);
+        best.used = int(used.size());
+        best.rejected = rejected;
+        best.iterations = iterations;
+        best.status = 0;
+        return best;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Relocation.Absolute's loop (Location/Relocation.cs:76-91): every event located on its own,
+// events spread over n_threads host threads. tables: n_tables float32 fields on g; table_station:
+// lon, lat of each table's station; start: lon, lat, depth per event; out: 16 x 8 bytes per event
+// (LocResult); residual: one per observation.
+void or_locate_many(const or_grid_def* d, const float* tables, int32_t n_tables, const double* table_station,
+                    const void* settings, int32_t n_events, const double* start, const int32_t* obs_offsets,
+                    const int32_t* obs_table, const double* obs_seconds, const double* obs_weight,
+                    const double* obs_corr, int32_t n_threads, void* out, double* residual) {
+    Grid g(*d);
+    const LocSettings& s = *static_cast<const LocSettings*>(settings);
+    LocResult* res = static_cast<LocResult*>(out);
+    const int64_t n = g.count();
+    Locator loc{g, s};
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int e = next++; e < n_events; e = next++) {
+            std::vector<LocObs> obs;
+            for (int q = obs_offsets[e]; q < obs_offsets[e + 1]; q++) {
+                int t = obs_table[q];
+                obs.push_back({tables + int64_t(t) * n, obs_seconds[q], obs_weight[q], obs_corr[q],
+                               table_station[2 * t], table_station[2 * t + 1]});
+            }
+            res[e] = loc.locate(obs, start[3 * e], start[3 * e + 1], start[3 * e + 2], residual + obs_offsets[e]);
+        }
+    };
+    (void)n_tables;
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, n_threads); t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+}
+
+// WeightedMedian, Median and Gap on their own (known-answer tests).
+double or_weighted_median(int32_t n, const double* v, const double* w) {
+    return weighted_median(std::vector<double>(v, v + n), std::vector<double>(w, w + n));
+}
+double or_median(int32_t n, const double* v) { return plain_median(std::vector<double>(v, v + n)); }
+double or_gap(int32_t n, const double* az) { return azimuth_gap(std::vector<double>(az, az + n)); }
+double or_tick_seconds(double t0) { return tick_seconds(t0); }
+
+}  // extern "C"

@@ -71,6 +71,12 @@ def lib():
             "or_ray_rows_many": (None, [g, fp, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32]),
             "or_relax_wake": (i32, [g, dp, i32, ip, dp, d, d, i32, dp, ip, P(C.c_int64)]),
             "or_lsqr": (i32, [i32, i32, ip, ip, dp, dp, d, i32, d, d, d, dp, dp]),
+            "or_locate_many": (None, [g, fp, i32, dp, C.c_void_p, i32, dp, ip, ip, dp, dp, dp, i32, C.c_void_p,
+                                      dp]),
+            "or_weighted_median": (d, [i32, dp, dp]),
+            "or_median": (d, [i32, dp]),
+            "or_gap": (d, [i32, dp]),
+            "or_tick_seconds": (d, [d]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -333,3 +339,69 @@ def lsqr(m, n, row_ptr, col, val, b, damp=0.0, max_iterations=500, atol=1e-8, bt
     code = lib().or_lsqr(m, n, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(va, C.c_double), _p(bb, C.c_double), damp,
                          max_iterations, atol, btol, conlim, _p(x, C.c_double), _p(info, C.c_double))
     return x, int(code), {"iterations": int(info[0]), "bnorm": info[1], "rnorm": info[2], "acond": info[3]}
+
+
+class LocatorSettings(C.Structure):
+    """LocatorSettings (Location/EventLocator.cs:10-36) with the reference's defaults."""
+
+    _fields_ = [("global_search", C.c_int32), ("coarse_candidates", C.c_int32),
+                ("max_geiger_iterations", C.c_int32), ("min_phases", C.c_int32), ("damping", C.c_double),
+                ("outlier_mads", C.c_double), ("outlier_floor", C.c_double), ("fix_depth", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def __init__(self, **kw):
+        base = dict(global_search=1, coarse_candidates=8000, max_geiger_iterations=20, min_phases=4, damping=0.01,
+                    outlier_mads=4.0, outlier_floor=0.5, fix_depth=0)
+        base.update(kw)
+        super().__init__(**base)
+
+
+LOCATION_FIELDS = ["t0", "lon", "lat", "depth_km", "rms", "err_h_km", "err_minor_km", "err_azimuth_deg",
+                   "err_depth_km", "err_time_s", "gap_deg"]
+LOCATION_DTYPE = np.dtype([(f, np.float64) for f in LOCATION_FIELDS] +
+                          [(f, np.int32) for f in ("used", "rejected", "iterations", "status")])
+
+
+def locate_many(g: Grid, tables, table_station, settings: LocatorSettings, start, obs_offsets, obs_table, obs_seconds,
+                obs_weight, obs_corr, threads=None):
+    """EventLocator.Locate for every event (Relocation.Absolute's loop, Location/Relocation.cs:76-91).
+
+    tables: (n_tables, nodes) float32; table_station: (n_tables, 2) lon, lat; start: (n_events, 3)
+    lon, lat, depth. Returns (a LOCATION_DTYPE record per event, the residual of every observation).
+    """
+    tb = np.ascontiguousarray(tables, np.float32)
+    ts_ = np.ascontiguousarray(table_station, np.float64)
+    st = np.ascontiguousarray(start, np.float64)
+    off = np.ascontiguousarray(obs_offsets, np.int32)
+    ot = np.ascontiguousarray(obs_table, np.int32)
+    osec = np.ascontiguousarray(obs_seconds, np.float64)
+    ow = np.ascontiguousarray(obs_weight, np.float64)
+    oc = np.ascontiguousarray(obs_corr, np.float64)
+    ne = len(off) - 1
+    out = np.zeros(ne, LOCATION_DTYPE)
+    res = np.empty(max(1, len(ot)))
+    lib().or_locate_many(g.ref, _p(tb, C.c_float), len(tb), _p(ts_, C.c_double), C.byref(settings), ne,
+                         _p(st, C.c_double), _p(off, C.c_int32), _p(ot, C.c_int32), _p(osec, C.c_double),
+                         _p(ow, C.c_double), _p(oc, C.c_double), threads or os.cpu_count(),
+                         out.ctypes.data_as(C.c_void_p), _p(res, C.c_double))
+    return out, res[: len(ot)]
+
+
+def weighted_median(v, w):
+    v = np.ascontiguousarray(v, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    return lib().or_weighted_median(len(v), _p(v, C.c_double), _p(w, C.c_double))
+
+
+def median(v):
+    v = np.ascontiguousarray(v, np.float64)
+    return lib().or_median(len(v), _p(v, C.c_double))
+
+
+def gap(az):
+    a = np.ascontiguousarray(az, np.float64)
+    return lib().or_gap(len(a), _p(a, C.c_double))
+
+
+def tick_seconds(t0):
+    return lib().or_tick_seconds(t0)

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from tomostar_b200 import synthetic as syn
 
 KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kat.json")))
 
@@ -212,3 +213,54 @@ def test_lsqr_oracle_pinned_to_scipy():
     # Degenerate systems end as the reference says.
     _, code, _ = O.lsqr(300, 120, A.indptr, A.indices, A.data, np.zeros(300))
     assert O.LSQR_STOPS[code] == "zero right-hand side"
+
+
+def _oracle_tables(job):
+    """The job's P and S tables from the oracle's sweeping (SphericalEikonal.Relax), rounded to float32."""
+    g = O.Grid.of(job.grid)
+    tabs = []
+    for phase, src in zip(job.table_phase, job.table_source):
+        idx, t = O.point_source(g, job.slowness[phase], *src)
+        f, ok, _ = O.relax(g, job.slowness[phase], idx, t)
+        assert ok
+        tabs.append(O.to_table(f))
+    return g, np.stack(tabs)
+
+
+def test_location_helpers_known_answers():
+    """WeightedMedian, Median and Gap (Location/EventLocator.cs:297-327) on hand-worked cases, and the
+    origin time as a DateTime holds it (100 ns ticks, truncated)."""
+    # Sorted (value, weight): (1, 1) (2, 1) (3, 1); NaN dropped; half of 3 is 1.5 -> 2.
+    assert O.weighted_median([3, 1, 2, np.nan], [1, 1, 1, 5]) == 2.0
+    # A heavy value takes the median: (1, 0.5) (5, 3) (9, 0.5) -> half 2, reached at 5.
+    assert O.weighted_median([9, 1, 5], [0.5, 0.5, 3]) == 5.0
+    # Ties keep their input order (stable): the first 2 reaches half.
+    assert O.weighted_median([2, 2, 7], [1, 1, 1]) == 2.0
+    assert O.weighted_median([np.nan], [1]) == 0.0
+    assert O.median([4, 1, 3, 2]) == 2.5 and O.median([5, 1, 3]) == 3.0 and O.median([]) == 0.0
+    assert O.median([np.nan, 2.0]) == 2.0
+    assert O.gap([10, 100, 100, 300]) == 200.0 and O.gap([45]) == 360.0
+    assert O.gap([0, 90, 180, 270]) == 90.0
+    assert O.tick_seconds(1.23456789012) == 1.2345678
+    assert O.tick_seconds(-2.00000019) == -2.0000001
+    assert O.tick_seconds(3.0) == 3.0
+
+
+def test_location_oracle_moves_events_towards_the_truth():
+    """PipelineTests.RelocationMovesEventsTowardsTheTruth (tests/TomoStar.Tests/PipelineTests.cs:95-107):
+    12 stations, 30 events, picks with 30 ms noise; every event located, the median horizontal error
+    at least halved. Also: gross errors rejected, and the residuals of the kept picks near the noise."""
+    job = syn.relocation_small()
+    g, tabs = _oracle_tables(job)
+    picks = syn.relocation_picks(job, tabs)
+    ts_ = np.ascontiguousarray(job.table_source[:, :2])
+    out, res = O.locate_many(g, tabs, ts_, O.LocatorSettings(), job.start, picks.offsets, picks.table,
+                             picks.seconds, picks.weight, picks.correction)
+    assert (out["status"] == 0).all()
+    before = syn.surface_distance_km(job.start[:, 0], job.start[:, 1], job.truth[:, 0], job.truth[:, 1])
+    after = syn.surface_distance_km(out["lon"], out["lat"], job.truth[:, 0], job.truth[:, 1])
+    assert np.median(after) < 0.5 * np.median(before), (np.median(before), np.median(after))
+    assert np.median(np.abs(out["t0"] - job.truth[:, 3])) < 0.1
+    assert out["rejected"].sum() > 0 and np.median(out["rms"]) < 0.05
+    assert (out["used"] + out["rejected"] == np.diff(picks.offsets)).all()
+    assert np.isfinite(res).all() and (out["gap_deg"] > 0).all() and (out["gap_deg"] <= 360).all()

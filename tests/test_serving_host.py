@@ -18,6 +18,10 @@ STRUCTS = {
     "ts_serve_request": (L.ServeRequest, ["n_rays", "seed_offsets", "inv", "step_km", "tables_out"]),
     "ts_serve_result": (L.ServeResult, ["queue_ms", "rows", "error"]),
     "ts_serve_stats_t": (L.ServeStats, ["device_ms", "complete_ms", "queued", "in_flight"]),
+    "ts_lsqr_info": (L.LsqrInfo, [f for f, _ in L.LsqrInfo._fields_]),
+    "ts_locator_settings": (L.LocatorSettings, [f for f, _ in L.LocatorSettings._fields_]),
+    "ts_location": (L.Location, [f for f, _ in L.Location._fields_]),
+    "ts_locate_stats": (L.LocateStats, [f for f, _ in L.LocateStats._fields_]),
 }
 
 

@@ -95,8 +95,45 @@ class LsqrInfo(C.Structure):
                 ("acond", C.c_double), ("device_ms", C.c_double)]
 
 
+class LocatorSettings(C.Structure):
+    """ts_locator_settings = LocatorSettings (Location/EventLocator.cs:10-36), the reference's defaults."""
+
+    _fields_ = [("global_search", C.c_int32), ("coarse_candidates", C.c_int32),
+                ("max_geiger_iterations", C.c_int32), ("min_phases", C.c_int32), ("damping", C.c_double),
+                ("outlier_mads", C.c_double), ("outlier_floor", C.c_double), ("fix_depth", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def __init__(self, **kw):
+        base = dict(global_search=1, coarse_candidates=8000, max_geiger_iterations=20, min_phases=4, damping=0.01,
+                    outlier_mads=4.0, outlier_floor=0.5, fix_depth=0)
+        base.update(kw)
+        super().__init__(**base)
+
+
+class Location(C.Structure):
+    """ts_location = LocationResult + Hypocentre."""
+
+    _fields_ = [(f, C.c_double) for f in ("t0", "lon", "lat", "depth_km", "rms", "err_h_km", "err_minor_km",
+                                          "err_azimuth_deg", "err_depth_km", "err_time_s", "gap_deg")] + \
+               [(f, C.c_int32) for f in ("used", "rejected", "iterations", "status")]
+
+
+class LocateStats(C.Structure):
+    """ts_locate_stats."""
+
+    _fields_ = [("device_ms", C.c_double), ("candidates", C.c_int64), ("rounds", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 _gp = _P(GridStruct)
 SIGNATURES = {
+    "ts_tables_build": (C.c_int, [_vp, _gp, _dp, _i32, _i32, _dp, _ip, _i32, _P(_vp), _P(EikStats)]),
+    "ts_tables_upload": (C.c_int, [_vp, _gp, _i32, _fp, _P(_vp)]),
+    "ts_tables_info": (C.c_int, [_vp, _P(_i32), _P(_i64)]),
+    "ts_tables_copy": (C.c_int, [_vp, _i32, _i32, _fp]),
+    "ts_tables_free": (None, [_vp]),
+    "ts_locate": (C.c_int, [_vp, _vp, _P(LocatorSettings), _i32, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _P(Location),
+                            _dp, _P(LocateStats)]),
     "ts_lsqr_solve": (C.c_int, [_vp, _i32, _i32, _ip, _ip, _dp, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
     "ts_lsqr_solve_rows": (C.c_int, [_vp, _vp, _i32, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
     "ts_lsqr_set_callback": (C.c_int, [_vp, C.c_void_p, _vp]),

@@ -24,39 +24,27 @@ static int upload_slowness(ts_ctx* ctx, const double* src, size_t count, Real* d
     return TS_OK;
 }
 
+// The float32 tables of `tables` ((phase, source) pairs; sources hold lon, lat, depth) on g, solved
+// by the engine in batches that fit the device next to the tables, each rounded to float32 into its
+// slot of `tab` (n_nodes floats per table): TravelTimeTableSet.Build (Forward/TravelTimeTable.cs:264-308)
+// with the seeds of PointSource at the source (:373).
 template <typename Real>
-static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slowness, int n_phases,
-                        const ts_grid* inv_def, int n_stations, const double* stations, int n_events,
-                        const double* events, int n_arr, const int32_t* arr_event, const int32_t* arr_station,
-                        const int32_t* arr_phase, double step_km, ts_rows** out, ts_eik_stats* stats) {
-    host::Grid g(*fwd_def), gi(*inv_def);
+int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n_phases,
+                 const std::vector<std::pair<int, int>>& tables, const double* sources, float* tab,
+                 ts_eik_stats* stats) {
     host::Metric m(g);
     const int64_t n = g.count();
-    // Tables of the (station, phase) pairs in use, ordered by phase then station (TravelTimeTable.cs:319).
-    std::map<std::pair<int, int>, int> table_id;
-    for (int a = 0; a < n_arr; a++) {
-        if (arr_event[a] < 0 || arr_event[a] >= n_events || arr_station[a] < 0 || arr_station[a] >= n_stations ||
-            arr_phase[a] < 0 || arr_phase[a] >= n_phases)
-            return ctx->fail(TS_E_ARG, "arrival " + std::to_string(a) + " refers outside the inputs");
-        table_id[{arr_phase[a], arr_station[a]}] = 0;
-    }
-    std::vector<std::pair<int, int>> tables;
-    for (auto& kv : table_id) {
-        kv.second = int(tables.size());
-        tables.push_back(kv.first);
-    }
     const int nt = int(tables.size());
-    // Slowness per phase and the fields, on the device.
+    // Slowness per phase on the device.
     Real* slow_d = static_cast<Real*>(ctx->buf("fwd.slowness", sizeof(Real) * size_t(n) * n_phases));
     if (!slow_d) return TS_E_NOMEM;
     int rc = upload_slowness<Real>(ctx, slowness, size_t(n) * n_phases, slow_d);
     if (rc) return rc;
-    // Seeds: PointSource at each station (TravelTimeTable.cs:373).
+    // Seeds: PointSource at each source (TravelTimeTable.cs:373).
     std::vector<std::vector<int32_t>> sidx(nt);
     std::vector<std::vector<double>> st(nt);
-    std::vector<double> table_station(3 * std::max(1, nt));
     for (int t = 0; t < nt; t++) {
-        const double* sp = stations + 3 * tables[t].second;
+        const double* sp = sources + 3 * tables[t].second;
         const double* sl = slowness + size_t(n) * tables[t].first;
         std::vector<int32_t> idx(8192);
         std::vector<double> tv(8192);
@@ -69,17 +57,7 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
         // TrySolve's merge (EikonalOpenCl.cs:150-163): PointSource gives distinct nodes in order.
         sidx[t].assign(idx.begin(), idx.begin() + c);
         st[t].assign(tv.begin(), tv.begin() + c);
-        if (c == 0) return ctx->fail(TS_E_NOSEEDS, "no seed nodes for station " + std::to_string(tables[t].second));
-        table_station[3 * t] = sp[0];
-        table_station[3 * t + 1] = sp[1];
-        table_station[3 * t + 2] = sp[2];
-    }
-    // Tables in batches that fit next to the tables themselves: each batch solved by the engine and
-    // rounded to float32 into its slots (TravelTimeTable.Write's rounding).
-    float* tab = nullptr;
-    if (nt > 0) {
-        tab = static_cast<float*>(ctx->buf("fwd.tables", sizeof(float) * size_t(n) * nt));
-        if (!tab) return TS_E_NOMEM;
+        if (c == 0) return ctx->fail(TS_E_NOSEEDS, "no seed nodes for source " + std::to_string(tables[t].second));
     }
     const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
     const int tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
@@ -144,10 +122,48 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
         stats->device_ms = field_ms;
     }
     ctx->stats = std::to_string(r0) + "+" + std::to_string(r1) + " rounds of 8 sweeps";
-    // The engine's field buffers are not needed by the rays: give their memory to the rows.
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->release("eng.fields");
-    // Arrivals → rays.
+    return TS_OK;
+}
+
+template int solve_tables<double>(ts_ctx*, const host::Grid&, const double*, int, const std::vector<std::pair<int, int>>&,
+                                  const double*, float*, ts_eik_stats*);
+template int solve_tables<float>(ts_ctx*, const host::Grid&, const double*, int, const std::vector<std::pair<int, int>>&,
+                                 const double*, float*, ts_eik_stats*);
+
+template <typename Real>
+static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slowness, int n_phases,
+                        const ts_grid* inv_def, int n_stations, const double* stations, int n_events,
+                        const double* events, int n_arr, const int32_t* arr_event, const int32_t* arr_station,
+                        const int32_t* arr_phase, double step_km, ts_rows** out, ts_eik_stats* stats) {
+    host::Grid g(*fwd_def), gi(*inv_def);
+    const int64_t n = g.count();
+    // Tables of the (station, phase) pairs in use, ordered by phase then station (TravelTimeTable.cs:319).
+    std::map<std::pair<int, int>, int> table_id;
+    for (int a = 0; a < n_arr; a++) {
+        if (arr_event[a] < 0 || arr_event[a] >= n_events || arr_station[a] < 0 || arr_station[a] >= n_stations ||
+            arr_phase[a] < 0 || arr_phase[a] >= n_phases)
+            return ctx->fail(TS_E_ARG, "arrival " + std::to_string(a) + " refers outside the inputs");
+        table_id[{arr_phase[a], arr_station[a]}] = 0;
+    }
+    std::vector<std::pair<int, int>> tables;
+    for (auto& kv : table_id) {
+        kv.second = int(tables.size());
+        tables.push_back(kv.first);
+    }
+    const int nt = int(tables.size());
+    std::vector<double> table_station(3 * std::max(1, nt));
+    for (int t = 0; t < nt; t++)
+        for (int c = 0; c < 3; c++) table_station[3 * t + c] = stations[3 * tables[t].second + c];
+    float* tab = nullptr;
+    if (nt > 0) {
+        tab = static_cast<float*>(ctx->buf("fwd.tables", sizeof(float) * size_t(n) * nt));
+        if (!tab) return TS_E_NOMEM;
+    }
+    int rc = solve_tables<Real>(ctx, g, slowness, n_phases, tables, stations, tab, stats);
+    if (rc) return rc;
+    // Arrivals → rays (the engine's field buffers were released for the rows).
     std::vector<int32_t> table_of(std::max(1, n_arr));
     std::vector<double> ev(3 * std::max(1, n_arr));
     for (int a = 0; a < n_arr; a++) {

@@ -339,3 +339,126 @@ def serving_stream(models: dict, rate: float = 200.0, duration: float = 60.0, se
                                         _surface_points(m.grid, m.h_km, 1, rng),
                                         _volume_points(m.grid, m.h_km, nr, 2, 25, rng), np.zeros(nr, np.int32)))
     return out
+
+
+@dataclass
+class RelocationJob:
+    """Events to locate on the tables of their stations (Relocation.Absolute, Location/Relocation.cs:48-97).
+
+    Table t is station t % n_stations for phase t // n_stations (0 P, 1 S). truth holds each event's
+    lon, lat, depth and origin time in s after its catalogue origin time; start is the catalogue
+    location the search starts from."""
+
+    name: str
+    grid: GridDef
+    slowness: np.ndarray       # (2, n) s/km, P then S
+    stations: np.ndarray       # (n_stations, 3) lon, lat, depth
+    truth: np.ndarray          # (n_events, 4)
+    start: np.ndarray          # (n_events, 3)
+    h_km: float
+
+    @property
+    def table_source(self) -> np.ndarray:
+        return np.concatenate([self.stations, self.stations])
+
+    @property
+    def table_phase(self) -> np.ndarray:
+        return np.repeat(np.arange(2, dtype=np.int32), len(self.stations))
+
+
+def _relocation_job(name: str, g: GridDef, h: float, n_stations: int, n_events: int, rng) -> RelocationJob:
+    vp = vp_linear(g, 5.0, 0.04) * (1 + ellipsoid_bodies(g, h, rng, n=2, amplitude=0.05))
+    slow = np.empty((2, g.count))
+    np.divide(1.0, vp, out=slow[0])
+    np.divide(1.73, vp, out=slow[1])
+    span_x, span_y = (g.nx - 1) * h, (g.ny - 1) * h
+    sx, sy = rng.uniform(0.05 * span_x, 0.95 * span_x, n_stations), rng.uniform(0.05 * span_y, 0.95 * span_y, n_stations)
+    slon, slat = km_to_geo(g, sx, sy, h)
+    stations = np.stack([slon, slat, np.zeros(n_stations)], axis=1)
+    bottom = g.max_depth_km
+    ex = rng.uniform(0.15 * span_x, 0.85 * span_x, n_events)
+    ey = rng.uniform(0.15 * span_y, 0.85 * span_y, n_events)
+    ez = rng.uniform(0.15 * bottom, 0.75 * bottom, n_events)
+    elon, elat = km_to_geo(g, ex, ey, h)
+    truth = np.stack([elon, elat, ez, rng.uniform(-1.0, 1.0, n_events)], axis=1)
+    # The catalogue locations: a few km off horizontally, off in depth, inside the grid.
+    qx = np.clip(ex + rng.normal(0, 3.0, n_events), 0, span_x)
+    qy = np.clip(ey + rng.normal(0, 3.0, n_events), 0, span_y)
+    qz = np.clip(ez + rng.normal(0, 2.0, n_events), 0, bottom)
+    qlon, qlat = km_to_geo(g, qx, qy, h)
+    start = np.stack([qlon, qlat, qz], axis=1)
+    return RelocationJob(name, g, slow, stations, truth, start, h)
+
+
+def relocation_small(seed: int = 99) -> RelocationJob:
+    """The reference's pipeline test set-up (tests/TomoStar.Tests/PipelineTests.cs:23-30, 95-107): 12
+    stations, 30 events, a 5 km inversion grid down to 20 km refined twice for the tables: 21×21×17
+    nodes at 2.5 km horizontally and 1.25 km vertically."""
+    g0 = regular_grid(21, 21, 17, 2.5)
+    g = GridDef(g0.min_lon, g0.max_lon, g0.min_lat, g0.max_lat, 0.0, 20.0, 21, 21, 17)
+    return _relocation_job("relocation_small", g, 2.5, 12, 30, np.random.default_rng(seed))
+
+
+def relocation_regional(n_stations: int = 60, n_events: int = 4000, seed: int = 8) -> RelocationJob:
+    """A regional relocation: the 161×161×81 model at 0.5 km (2.1 M nodes), 60 surface stations (120 P
+    and S tables, 1.0 GB of float32), 4,000 events 6–30 km deep."""
+    g = regular_grid(161, 161, 81, 0.5)
+    return _relocation_job("relocation_regional", g, 0.5, n_stations, n_events, np.random.default_rng(seed))
+
+
+def table_time(g: GridDef, table: np.ndarray, lon, lat, dep) -> np.ndarray:
+    """TravelTimeTable.Time (Forward/TravelTimeTable.cs:116-136) on a uniform grid for arrays of points:
+    trilinear on the float32 nodes, +inf when a weighted corner is not finite."""
+    lon, lat, dep = (np.atleast_1d(np.asarray(a, np.float64)) for a in (lon, lat, dep))
+    fx = np.clip((lon - g.min_lon) / g.dlon, 0, g.nx - 1)
+    fy = np.clip((lat - g.min_lat) / g.dlat, 0, g.ny - 1)
+    fz = np.clip((dep - g.min_depth_km) / g.ddepth, 0, g.nz - 1)
+    i0 = np.minimum(fx.astype(np.int64), g.nx - 2)
+    j0 = np.minimum(fy.astype(np.int64), g.ny - 2)
+    k0 = np.minimum(fz.astype(np.int64), g.nz - 2)
+    tx, ty, tz = fx - i0, fy - j0, fz - k0
+    t = np.zeros(len(lon))
+    bad = np.zeros(len(lon), bool)
+    for dk in (0, 1):
+        for dj in (0, 1):
+            for di in (0, 1):
+                w = (tx if di else 1 - tx) * (ty if dj else 1 - ty) * (tz if dk else 1 - tz)
+                v = table[((k0 + dk) * g.ny + j0 + dj) * g.nx + i0 + di].astype(np.float64)
+                use = w != 0
+                bad |= use & ~np.isfinite(v)
+                t += np.where(use & np.isfinite(v), v * w, 0.0)
+    return np.where(bad, np.inf, t)
+
+
+@dataclass
+class Picks:
+    """The observations of every event, event after event (obs_offsets[e] .. obs_offsets[e+1])."""
+
+    offsets: np.ndarray      # (n_events + 1,) int32
+    table: np.ndarray        # int32
+    seconds: np.ndarray      # pick time, s after the catalogue origin time
+    weight: np.ndarray
+    correction: np.ndarray   # station correction, s
+
+
+def relocation_picks(job: RelocationJob, tables: np.ndarray, pick_share: float = 0.8, noise_s: float = 0.03,
+                     outlier_share: float = 0.03, seed: int = 12) -> Picks:
+    """Picks of P and S at a share of the stations: the travel time at the true hypocentre from the
+    tables, the station correction, 30 ms of noise, a few gross errors of 1–3 s, and the weights of
+    four quality classes (1, 0.75, 0.5, 0.25)."""
+    rng = np.random.default_rng(seed)
+    n_ev, n_st = len(job.truth), len(job.stations)
+    nt = 2 * n_st
+    corr = rng.normal(0, 0.05, nt)
+    tt = np.stack([table_time(job.grid, tables[t], job.truth[:, 0], job.truth[:, 1], job.truth[:, 2])
+                   for t in range(nt)], axis=1)                    # (n_events, n_tables)
+    take = (rng.random((n_ev, nt)) < pick_share) & np.isfinite(tt)
+    noise = rng.normal(0, noise_s, (n_ev, nt))
+    gross = np.where(rng.random((n_ev, nt)) < outlier_share, rng.uniform(1.0, 3.0, (n_ev, nt)), 0.0)
+    quality = rng.choice(np.array([1.0, 0.75, 0.5, 0.25]), size=(n_ev, nt), p=[0.5, 0.25, 0.15, 0.1])
+    obs = job.truth[:, 3:4] + tt + corr[None, :] + noise + gross
+    counts = take.sum(axis=1)
+    offsets = np.zeros(n_ev + 1, np.int32)
+    offsets[1:] = np.cumsum(counts)
+    ev, tb = np.nonzero(take)
+    return Picks(offsets, tb.astype(np.int32), obs[ev, tb], quality[ev, tb], corr[tb])
