@@ -160,6 +160,67 @@ def cpu_fmm_sample(problem, n_fields: int, threads: int):
     return n_fields / dt, dt
 
 
+def location_job(device: int, n_events: int, cpu_events: int, threads: int) -> dict:
+    """Relocation of a regional catalogue on resident tables (Relocation.Absolute): the 120 P and S
+    tables of 60 stations on the 161x161x81 model built by the engine and kept on the device, then
+    EventLocator.Locate for every event in one call; the oracle locates a bounded sample of the same
+    events on the host cores (the CPU baseline), whose results are compared with the device's."""
+    from oracle import oracle as O
+    from tomostar_b200 import location as loc
+    from tomostar_b200 import synthetic as syn
+    from tomostar_b200.eikonal import EikonalCuda
+
+    job = syn.relocation_regional(n_events=n_events)
+    with EikonalCuda.create(device, 64) as s:
+        t0 = time.perf_counter()
+        tables = loc.Tables.build(s, job.grid, job.slowness, job.table_source, job.table_phase)
+        build_s = time.perf_counter() - t0
+        tabs = tables.copy()
+        picks = syn.relocation_picks(job, tabs)
+        tsta = job.table_source[:, :2]
+
+        def sub(k):
+            o = picks.offsets[: k + 1]
+            e = o[-1]
+            return (job.start[:k], o, picks.table[:e], picks.seconds[:e], picks.weight[:e], picks.correction[:e])
+
+        loc.locate(s, tables, *sub(min(64, n_events)), tsta)  # warm-up
+        t1 = time.perf_counter()
+        r = loc.locate(s, tables, job.start, picks.offsets, picks.table, picks.seconds, picks.weight,
+                       picks.correction, tsta)
+        wall = time.perf_counter() - t1
+        tables.close()
+    k = min(cpu_events, n_events)
+    st, o, tb, sec, w, corr = sub(k)
+    t2 = time.perf_counter()
+    ora, _ = O.locate_many(O.Grid.of(job.grid), tabs, tsta, O.LocatorSettings(), st, o, tb, sec, w, corr,
+                           threads=threads)
+    cpu_s = time.perf_counter() - t2
+    d = r.locations[:k]
+    ok = r.locations["status"] == 0
+    err = syn.surface_distance_km(r.locations["lon"], r.locations["lat"], job.truth[:, 0], job.truth[:, 1])
+    err0 = syn.surface_distance_km(job.start[:, 0], job.start[:, 1], job.truth[:, 0], job.truth[:, 1])
+    picks_per_event = float(np.mean(np.diff(picks.offsets)))
+    return {
+        "workload": "relocation_regional: 161x161x81 at 0.5 km, 60 stations x P,S = 120 float32 tables "
+                    f"(1.0 GB) resident, {n_events} events, {picks_per_event:.1f} picks per event (seed 8)",
+        "events": n_events, "located": int(ok.sum()), "wall_s": wall, "events_per_s": n_events / wall,
+        "device_ms": r.device_ms, "rounds": r.rounds, "candidates": r.candidates,
+        "candidates_per_s": r.candidates / (r.device_ms / 1e3),
+        "node_misfits_picks_per_s": r.candidates * picks_per_event / (r.device_ms / 1e3),
+        "tables_build_s": build_s,
+        "median_error_km": {"start": float(np.median(err0)), "located": float(np.median(err[ok]))},
+        "cpu_baseline": {"events_per_s": k / cpu_s, "cores": threads, "kind": "port",
+                         "sample": f"the first {k} events, oracle EventLocator restated in C++, one event per thread"},
+        "speedup_vs_cpu": (n_events / wall) / (k / cpu_s),
+        "parity_sample": {"events": k, "status_equal": bool(np.array_equal(d["status"], ora["status"])),
+                          "used_equal": bool(np.array_equal(d["used"], ora["used"])),
+                          "max_dlon_deg": float(np.max(np.abs(d["lon"] - ora["lon"]))),
+                          "max_ddepth_km": float(np.max(np.abs(d["depth_km"] - ora["depth_km"]))),
+                          "max_dt0_s": float(np.max(np.abs(d["t0"] - ora["t0"])))},
+    }
+
+
 def run_reference(args, problem_fn):
     # The CPU arm needs no process group: rank 0 alone runs it and prints the line.
     if int(os.environ.get("RANK", "0")) != 0:
@@ -373,6 +434,9 @@ def run_ours(args, problem_fn):
                             "note": "setup = transpose built on the device from the resident rows, column order as the host transpose"}}
         del rows
         fsolver.close()
+    location = None
+    if world == 1 and not args.no_location:
+        location = location_job(local, args.location_events, args.location_cpu_events, os.cpu_count() or 1)
     # The serving load (Poisson stream of mixed requests) on one GPU, after the batch job's buffers
     # are released; at N = 1 only (the scaling runs measure the batch job).
     serving = None
@@ -407,6 +471,7 @@ def run_ours(args, problem_fn):
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "forward_step": forward,
+            "location": location,
             "serving": serving,
             "node_updates_per_step": updates // args.steps,
             "wall_s_timed": t_wall,
@@ -433,6 +498,9 @@ def main():
     ap.add_argument("--scheduler", type=int, default=0, help="0 lockstep diagonals, 1 flow (per field)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-load measurement")
     ap.add_argument("--no-forward", action="store_true", help="skip the forward step (tables + rays)")
+    ap.add_argument("--no-location", action="store_true", help="skip the relocation measurement")
+    ap.add_argument("--location-events", type=int, default=4000)
+    ap.add_argument("--location-cpu-events", type=int, default=256, help="events the CPU baseline locates")
     ap.add_argument("--serve-scheduler", type=int, default=1)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-tile", type=int, default=2)

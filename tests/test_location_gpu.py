@@ -50,10 +50,13 @@ def test_tables_equal_the_oracle_sweeping(small):
 
 def test_grid_search_and_outlier_rule_bitwise(solver, small):
     """Geiger off: the search's node and weighted-median origin time, the outlier rounds, residuals,
-    counts and gap equal the oracle's exactly."""
+    counts and gap equal the oracle's exactly; with the quality-class weights (the warp search) and
+    with weights whose sums round (0.3 times them: the thread search)."""
     job, tables, tabs, picks = small
-    for kw in ({}, {"fix_depth": 1}, {"global_search": 0}, {"coarse_candidates": 300}):
-        dev, ora, res = _both(solver, job, tables, tabs, picks, max_geiger_iterations=0, **kw)
+    odd = syn.Picks(picks.offsets, picks.table, picks.seconds, picks.weight * 0.3, picks.correction)
+    for pk, kw in ((picks, {}), (picks, {"fix_depth": 1}), (picks, {"global_search": 0}),
+                   (picks, {"coarse_candidates": 300}), (odd, {}), (odd, {"fix_depth": 1})):
+        dev, ora, res = _both(solver, job, tables, tabs, pk, max_geiger_iterations=0, **kw)
         d = dev.locations
         for f in ("t0", "lon", "lat", "depth_km", "rms", "gap_deg", "used", "rejected", "iterations", "status"):
             assert np.array_equal(d[f], ora[f]), (kw, f)

@@ -112,39 +112,28 @@ __device__ __forceinline__ bool better(double m1, int c1, double m2, int c2) {
     return m1 < m2 || (m1 == m2 && c1 < c2);
 }
 
-// Candidates of all tasks, one thread each; per block the smallest misfit (first in scan order).
-template <int NMAX>
-__global__ void __launch_bounds__(kSearchThreads) search_kernel(const SearchTask* __restrict__ tasks, int n_tasks,
-                                                                const int* __restrict__ off,
-                                                                const EvState* __restrict__ st,
-                                                                const ObsD* __restrict__ olist, int nx, int ny,
-                                                                Partial* __restrict__ partial) {
-    __shared__ ObsD so[NMAX];
-    __shared__ double wm[kSearchThreads / 32];
-    __shared__ int wc[kSearchThreads / 32];
-    // The task of this block: the last one whose first block is not after it.
+// The task of a block: the last one whose first block is not after it.
+__device__ __forceinline__ int task_of_block(const SearchTask* tasks, int n_tasks) {
     int lo = 0, hi = n_tasks - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (tasks[mid].block0 <= int(blockIdx.x)) lo = mid;
         else hi = mid - 1;
     }
-    const SearchTask t = tasks[lo];
-    const int n = st[t.event].nused;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) so[q] = olist[off[t.event] + q];
-    __syncthreads();
-    const int c = (int(blockIdx.x) - t.block0) * kSearchThreads + threadIdx.x;
-    double m = dinf();
-    int cc = 0x7fffffff;
-    if (c < t.count) {
-        const int ii = t.i0 + (c % t.ci) * t.stride;
-        const int jj = t.j0 + ((c / t.ci) % t.cj) * t.stride;
-        const int kk = t.k0 + (c / (t.ci * t.cj)) * t.stride;
-        const int64_t idx = (int64_t(kk) * ny + jj) * nx + ii;
-        double t0;
-        m = node_misfit<NMAX>(so, n, idx, t0);
-        cc = c;
-    }
+    return lo;
+}
+
+__device__ __forceinline__ int64_t candidate_node(const SearchTask& t, int c, int nx, int ny) {
+    const int ii = t.i0 + (c % t.ci) * t.stride;
+    const int jj = t.j0 + ((c / t.ci) % t.cj) * t.stride;
+    const int kk = t.k0 + (c / (t.ci * t.cj)) * t.stride;
+    return (int64_t(kk) * ny + jj) * nx + ii;
+}
+
+// Block-wide first minimum of (m, c) over 256 threads; thread 0 writes the block's partial.
+__device__ __forceinline__ void block_best(double m, int cc, Partial* partial) {
+    __shared__ double wm[kSearchThreads / 32];
+    __shared__ int wc[kSearchThreads / 32];
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         const double m2 = __shfl_down_sync(kFull, m, d);
@@ -172,17 +161,225 @@ __global__ void __launch_bounds__(kSearchThreads) search_kernel(const SearchTask
     }
 }
 
+// Exact path, any weights and up to 1024 picks: one thread per candidate, the residuals ordered by a
+// stable insertion sort and every sum taken in the reference's order.
+template <int NMAX>
+__global__ void __launch_bounds__(kSearchThreads) search_kernel(const SearchTask* __restrict__ tasks, int n_tasks,
+                                                                const int* __restrict__ off,
+                                                                const EvState* __restrict__ st,
+                                                                const ObsD* __restrict__ olist, int nx, int ny,
+                                                                Partial* __restrict__ partial) {
+    __shared__ ObsD so[NMAX];
+    const SearchTask t = tasks[task_of_block(tasks, n_tasks)];
+    const int n = st[t.event].nused;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) so[q] = olist[off[t.event] + q];
+    __syncthreads();
+    const int c = (int(blockIdx.x) - t.block0) * kSearchThreads + threadIdx.x;
+    double m = dinf();
+    int cc = 0x7fffffff;
+    if (c < t.count) {
+        double t0;
+        m = node_misfit<NMAX>(so, n, candidate_node(t, c, nx, ny), t0);
+        cc = c;
+    }
+    block_best(m, cc, partial);
+}
+
+// Bitonic sort of 32*E (key, pick) pairs held E per lane (element j*32 + lane in slot j), ascending by
+// key then pick: a total order, so the result is the stable sort by key.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(double (&key)[E], int (&q)[E], int lane) {
+    constexpr int N = 32 * E;
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+        for (int d = k >> 1; d > 0; d >>= 1) {
+            if (d >= 32) {
+#pragma unroll
+                for (int j = 0; j < E; j++) {
+                    const int jp = j ^ (d >> 5);
+                    if (jp > j) {
+                        const bool up = (((j * 32 + lane) & k) == 0);
+                        const bool gt = key[j] > key[jp] || (key[j] == key[jp] && q[j] > q[jp]);
+                        if (gt == up) {
+                            const double tk = key[j];
+                            key[j] = key[jp];
+                            key[jp] = tk;
+                            const int tq = q[j];
+                            q[j] = q[jp];
+                            q[jp] = tq;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < E; j++) {
+                    const double ok = __shfl_xor_sync(kFull, key[j], d);
+                    const int oq = __shfl_xor_sync(kFull, q[j], d);
+                    const bool up = (((j * 32 + lane) & k) == 0);
+                    const bool lower = (lane & d) == 0;
+                    const bool gt = key[j] > ok || (key[j] == ok && q[j] > oq);
+                    if (lower ? (gt == up) : (gt != up)) {
+                        key[j] = ok;
+                        q[j] = oq;
+                    }
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFull, v, d);
+    return v;
+}
+
+// GridSearch's Misfit at one node by one warp, for dyadic non-negative weights (sums of at most 128
+// of them are exact in any order): the weighted-median origin time exactly as the reference's, and
+// the misfit either as a tree sum (fast) or in pick order (exact, the reference's rounding).
+template <int E>
+__device__ double warp_node_misfit(const ObsD* so, int n, int64_t idx, int lane, bool exact) {
+    double key[E], r0[E], w0[E];
+    int q[E];
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+        const int qq = j * 32 + lane;
+        r0[j] = dnan();
+        w0[j] = 0;
+        key[j] = dinf();
+        q[j] = 1024 + qq;  // padding sorts after every pick
+        if (qq < n) {
+            const float t = __ldg(so[qq].tb + idx);
+            w0[j] = so[qq].w;
+            q[j] = qq;
+            if (isfinite(t)) {
+                r0[j] = so[qq].sec - double(t) - so[qq].corr;
+                key[j] = r0[j];
+            }
+        }
+    }
+    warp_bitonic<E>(key, q, lane);
+    // Weights in sorted order (finite residuals only), their total and inclusive prefix sums.
+    double ws[E];
+    double total = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+        ws[j] = (key[j] < dinf()) ? so[q[j]].w : 0.0;
+        total += ws[j];
+    }
+    total = warp_sum(total);
+    const double half = total / 2;
+    const unsigned finite0 = __ballot_sync(kFull, key[0] < dinf());
+    double t0 = 0;
+    if (finite0 != 0) {
+        double carry = 0;
+        bool found = false;
+        double last = 0;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            double x = ws[j];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const double y = __shfl_up_sync(kFull, x, d);
+                if (lane >= d) x += y;
+            }
+            const double acc = carry + x;
+            carry += __shfl_sync(kFull, x, 31);
+            const unsigned fin = __ballot_sync(kFull, key[j] < dinf());
+            if (fin) last = __shfl_sync(kFull, key[j], 31 - __clz(fin));
+            const unsigned hit = __ballot_sync(kFull, key[j] < dinf() && acc >= half);
+            if (!found && hit) {
+                t0 = __shfl_sync(kFull, key[j], __ffs(hit) - 1);
+                found = true;
+            }
+        }
+        if (!found) t0 = last;
+    }
+    double term[E];
+    double m = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+        term[j] = (j * 32 + lane < n) ? (isnan(r0[j]) ? 10 * w0[j] : w0[j] * fabs(r0[j] - t0)) : 0.0;
+        m += term[j];
+    }
+    if (!exact) return warp_sum(m);
+    m = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++)
+        for (int l = 0; l < 32 && j * 32 + l < n; l++) m += __shfl_sync(kFull, term[j], l);
+    return m;
+}
+
+// Fast path: one warp per candidate, kWarpCands consecutive candidates per warp. Each block then
+// re-sums in pick order the candidates whose tree-summed misfit lies within 1e-12 (relative) of the
+// block's smallest, which holds every candidate that can be the block's exact first minimum (two
+// summation orders of n non-negative terms differ by at most 2(n-1)u of the sum), and reports the
+// exact first minimum among them.
+constexpr int kWarpCands = 8;
+constexpr int kBlockCands = kWarpCands * (kSearchThreads / 32);
+
+template <int E>
+__global__ void __launch_bounds__(kSearchThreads) search_warp_kernel(const SearchTask* __restrict__ tasks,
+                                                                     int n_tasks, const int* __restrict__ off,
+                                                                     const EvState* __restrict__ st,
+                                                                     const ObsD* __restrict__ olist, int nx, int ny,
+                                                                     Partial* __restrict__ partial) {
+    __shared__ ObsD so[32 * E];
+    __shared__ double fm[kBlockCands];
+    __shared__ double fmin_s;
+    const SearchTask t = tasks[task_of_block(tasks, n_tasks)];
+    const int n = st[t.event].nused;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) so[q] = olist[off[t.event] + q];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cb = (int(blockIdx.x) - t.block0) * kBlockCands;
+    for (int k = 0; k < kWarpCands; k++) {
+        const int slot = warp * kWarpCands + k;
+        const int c = cb + slot;
+        double m = dinf();
+        if (c < t.count) m = warp_node_misfit<E>(so, n, candidate_node(t, c, nx, ny), lane, false);
+        if (lane == 0) fm[slot] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = fm[0];
+        for (int i = 1; i < kBlockCands; i++) b = fmin(b, fm[i]);
+        fmin_s = b;
+    }
+    __syncthreads();
+    const double band = fmin_s + fmin_s * 1e-12;
+    double best = dinf();
+    int bc = 0x7fffffff;
+    for (int k = 0; k < kWarpCands; k++) {
+        const int slot = warp * kWarpCands + k;
+        const int c = cb + slot;
+        if (c >= t.count || !(fm[slot] <= band)) continue;
+        const double m = warp_node_misfit<E>(so, n, candidate_node(t, c, nx, ny), lane, true);
+        if (m < best || bc == 0x7fffffff) {
+            best = m;
+            bc = c;
+        }
+    }
+    if (fmin_s == dinf()) {  // every misfit +inf: the first candidate stands for the block
+        best = dinf();
+        bc = cb;
+    }
+    // Warp 0's lane 0 of each warp holds that warp's exact best; reduce over warps.
+    block_best(lane == 0 ? best : dinf(), lane == 0 ? bc : 0x7fffffff, partial);
+}
+
 // The best candidate of each task over its blocks (first minimum in scan order; every misfit +inf
 // gives the first candidate, as Search returns Index(i0, j0, k0)), its node, origin time and place.
 template <int NMAX>
 __global__ void pick_best(const RGrid g, const SearchTask* __restrict__ tasks, int n_tasks,
                           const Partial* __restrict__ partial, const int* __restrict__ off,
-                          const ObsD* __restrict__ olist, EvState* __restrict__ st, int fix_depth,
+                          const ObsD* __restrict__ olist, EvState* __restrict__ st, int fix_depth, int per_block,
                           int* __restrict__ best_out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n_tasks) return;
     const SearchTask t = tasks[k];
-    const int nb = (t.count + kSearchThreads - 1) / kSearchThreads;
+    const int nb = (t.count + per_block - 1) / per_block;
     double bm = partial[t.block0].m;
     int bc = partial[t.block0].c;
     for (int b = 1; b < nb; b++)
@@ -584,14 +781,16 @@ bool make_task(const host::Grid& g, int e, int i0, int i1, int j0, int j1, int k
     return true;
 }
 
-template <int NMAX>
+// E > 0: the warp kernel with E picks per lane; E == 0: the thread kernel.
+template <int NMAX, int E>
 int run_search(ts_ctx* ctx, const RGrid& rg, std::vector<SearchTask>& tasks, const int* off_d, EvState* st_d,
                const ObsD* olist_d, int fix_depth, std::vector<int>& best, int64_t& candidates) {
     cudaStream_t s = ctx->stream;
+    const int per_block = E > 0 ? kBlockCands : kSearchThreads;
     int blocks = 0;
     for (auto& t : tasks) {
         t.block0 = blocks;
-        blocks += (t.count + kSearchThreads - 1) / kSearchThreads;
+        blocks += (t.count + per_block - 1) / per_block;
         candidates += t.count;
     }
     const int nt = int(tasks.size());
@@ -599,8 +798,14 @@ int run_search(ts_ctx* ctx, const RGrid& rg, std::vector<SearchTask>& tasks, con
     TS_BUF(ctx, part_d, Partial, "loc.partial", std::max(1, blocks));
     TS_BUF(ctx, best_d, int, "loc.best", std::max(1, nt));
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(tasks_d, tasks.data(), sizeof(SearchTask) * nt, cudaMemcpyHostToDevice, s));
-    search_kernel<NMAX><<<blocks, kSearchThreads, 0, s>>>(tasks_d, nt, off_d, st_d, olist_d, rg.nx, rg.ny, part_d);
-    pick_best<NMAX><<<(nt + 127) / 128, 128, 0, s>>>(rg, tasks_d, nt, part_d, off_d, olist_d, st_d, fix_depth, best_d);
+    if constexpr (E > 0)
+        search_warp_kernel<E><<<blocks, kSearchThreads, 0, s>>>(tasks_d, nt, off_d, st_d, olist_d, rg.nx, rg.ny,
+                                                                part_d);
+    else
+        search_kernel<NMAX><<<blocks, kSearchThreads, 0, s>>>(tasks_d, nt, off_d, st_d, olist_d, rg.nx, rg.ny,
+                                                              part_d);
+    pick_best<NMAX><<<(nt + 127) / 128, 128, 0, s>>>(rg, tasks_d, nt, part_d, off_d, olist_d, st_d, fix_depth,
+                                                     per_block, best_d);
     TS_CUDA_TRY(ctx, cudaGetLastError());
     best.resize(nt);
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(best.data(), best_d, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
@@ -609,17 +814,25 @@ int run_search(ts_ctx* ctx, const RGrid& rg, std::vector<SearchTask>& tasks, con
 }
 
 int search_classes(ts_ctx* ctx, const RGrid& rg, const std::vector<SearchTask>& tasks, const std::vector<int>& cls,
-                   const int* off_d, EvState* st_d, const ObsD* olist_d, int fix_depth, std::vector<int>& best_of_event,
-                   int64_t& candidates) {
+                   const int* off_d, EvState* st_d, const ObsD* olist_d, int fix_depth, bool dyadic,
+                   std::vector<int>& best_of_event, int64_t& candidates) {
     for (int c = 0; c < 3; c++) {
         std::vector<SearchTask> part;
         for (const auto& t : tasks)
             if (cls[t.event] == c) part.push_back(t);
         if (part.empty()) continue;
         std::vector<int> best;
-        int rc = c == 0   ? run_search<32>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates)
-                 : c == 1 ? run_search<128>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates)
-                          : run_search<kMaxObs>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates);
+        // Dyadic non-negative weights: one warp per candidate (registers only); otherwise, and above
+        // 128 picks, one thread per candidate.
+        int rc;
+        if (c == 0)
+            rc = dyadic ? run_search<32, 1>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates)
+                        : run_search<32, 0>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates);
+        else if (c == 1)
+            rc = dyadic ? run_search<128, 4>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates)
+                        : run_search<128, 0>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates);
+        else
+            rc = run_search<kMaxObs, 0>(ctx, rg, part, off_d, st_d, olist_d, fix_depth, best, candidates);
         if (rc) return rc;
         for (size_t k = 0; k < part.size(); k++) best_of_event[part[k].event] = best[k];
     }
@@ -808,6 +1021,14 @@ extern "C" int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settin
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(st_d, st.data(), sizeof(EvState) * n_events, cudaMemcpyHostToDevice, s));
     Params prm{set->max_geiger_iterations, set->min_phases, fix, 0, set->damping, set->outlier_mads,
                set->outlier_floor};
+    // Weights that are non-negative multiples of 2^-24 below 2^18: any sum of at most 128 of them is
+    // exact, whatever the order (the warp search relies on it; otherwise the thread search runs).
+    bool dyadic = true;
+    for (int q = 0; q < n_obs && dyadic; q++) {
+        const double w = obs_weight[q];
+        const double sc = std::ldexp(w, 24);
+        dyadic = std::isfinite(w) && w >= 0 && w < 262144.0 && sc == std::floor(sc);
+    }
     const int stride =
         std::max(1, int(std::ceil(std::cbrt(double(g.count()) / set->coarse_candidates))));  // EventLocator.cs:128
     int64_t candidates = 0;
@@ -839,7 +1060,7 @@ extern "C" int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settin
             if (ok) tasks.push_back(t);
             else outside[e] = 1;
         }
-        int rc = search_classes(ctx, rg, tasks, cls, off_d, st_d, olist_d, fix, best, candidates);
+        int rc = search_classes(ctx, rg, tasks, cls, off_d, st_d, olist_d, fix, dyadic, best, candidates);
         if (rc) return rc;
         if (set->global_search) {
             std::vector<SearchTask> fine;
@@ -851,7 +1072,7 @@ extern "C" int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settin
                               bk - 2 * stride, bk + 2 * stride, 1, kfix[t0.event], t))
                     fine.push_back(t);
             }
-            rc = search_classes(ctx, rg, fine, cls, off_d, st_d, olist_d, fix, best, candidates);
+            rc = search_classes(ctx, rg, fine, cls, off_d, st_d, olist_d, fix, dyadic, best, candidates);
             if (rc) return rc;
         }
         // Geiger and the outlier rule for the events whose search ran.
