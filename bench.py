@@ -189,6 +189,33 @@ def location_job(device: int, n_events: int, cpu_events: int, threads: int) -> d
         r = loc.locate(s, tables, job.start, picks.offsets, picks.table, picks.seconds, picks.weight,
                        picks.correction, tsta)
         wall = time.perf_counter() - t1
+        # The tables as .qttb files (TravelTimeTable.Write) and back (TravelTimeTable.Open).
+        from oracle import qttb as OQ
+        from tomostar_b200 import qttb
+
+        with tempfile.TemporaryDirectory() as tmp:
+            heads = [qttb.header_json(f"S{t % 60:02d}", "PS"[job.table_phase[t]], *job.table_source[t], job.grid)
+                     for t in range(len(tabs))]
+            paths = [os.path.join(tmp, f"S{t % 60:02d}.{'PS'[job.table_phase[t]]}.qttb") for t in range(len(tabs))]
+            t3 = time.perf_counter()
+            qttb.write(tables, paths, heads)
+            write_s = time.perf_counter() - t3
+            t4 = time.perf_counter()
+            back = qttb.load(s, job.grid, paths)
+            load_s = time.perf_counter() - t4
+            same = bool(np.array_equal(back.copy(0, 3), tabs[:3]))
+            back.close()
+            same_bytes = open(paths[0], "rb").read() == OQ.write_bytes(heads[0], tabs[0].astype(np.float64))
+            t5 = time.perf_counter()
+            for t in range(8):
+                with open(os.path.join(tmp, "cpu.qttb"), "wb") as f:
+                    f.write(OQ.write_bytes(heads[t], tabs[t].astype(np.float64)))
+            cpu_write_s = (time.perf_counter() - t5) / 8 * len(tabs)
+        gb = tabs.nbytes / 1e9
+        qttb_line = {"tables": len(tabs), "gb": gb, "write_s": write_s, "write_gbs": gb / write_s, "load_s": load_s,
+                     "load_gbs": gb / load_s, "round_trip_equal": same, "bytes_equal_restatement": same_bytes,
+                     "cpu_baseline": {"write_gbs": gb / cpu_write_s, "kind": "port", "cores": 1,
+                                      "sample": "8 tables written by the byte restatement (numpy), scaled to 120"}}
         tables.close()
     k = min(cpu_events, n_events)
     st, o, tb, sec, w, corr = sub(k)
@@ -209,6 +236,7 @@ def location_job(device: int, n_events: int, cpu_events: int, threads: int) -> d
         "candidates_per_s": r.candidates / (r.device_ms / 1e3),
         "node_misfits_picks_per_s": r.candidates * picks_per_event / (r.device_ms / 1e3),
         "tables_build_s": build_s,
+        "qttb": qttb_line,
         "median_error_km": {"start": float(np.median(err0)), "located": float(np.median(err[ok]))},
         "cpu_baseline": {"events_per_s": k / cpu_s, "cores": threads, "kind": "port",
                          "sample": f"the first {k} events, oracle EventLocator restated in C++, one event per thread"},

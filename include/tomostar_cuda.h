@@ -317,6 +317,16 @@ int ts_tables_info(ts_tables* tables, int32_t* n_tables, int64_t* nodes_per_tabl
 /* Tables first .. first+count-1 to the host (count * nodes floats). */
 int ts_tables_copy(ts_tables* tables, int32_t first, int32_t count, float* out);
 void ts_tables_free(ts_tables* tables);
+/* TravelTimeTable.Write (Forward/TravelTimeTable.cs:57-80) for tables first .. first+count-1: file k
+ * at paths[k] holds the magic "QTTB" 01 00 00 00, header_len[k] as a little-endian int32, the
+ * header bytes headers[k] (the caller's TravelTimeTableHeader serialised with TomoJson.Options,
+ * Model/Basics.cs:60-75), zero bytes up to a multiple of 64, then the table as little-endian float32
+ * with every non-finite value written as +inf; written to path + ".tmp" and renamed over path. */
+int ts_tables_write_qttb(ts_tables* tables, int32_t first, int32_t count, const char* const* paths,
+                         const char* const* headers, const int32_t* header_len);
+/* TravelTimeTable.Open (:99-111) of count files into a resident table set on `grid` (the grid their
+ * headers name): the magic is checked and each file must hold the grid's nodes after its header. */
+int ts_tables_load_qttb(ts_ctx* ctx, const ts_grid* grid, int32_t count, const char* const* paths, ts_tables** out);
 
 /* ---- Event location on resident tables (Location/EventLocator.cs:59-342, Relocation.cs:48-97) ---- */
 typedef struct ts_locator_settings {   /* LocatorSettings (EventLocator.cs:10-36); defaults in brackets */

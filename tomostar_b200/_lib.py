@@ -132,6 +132,8 @@ SIGNATURES = {
     "ts_tables_info": (C.c_int, [_vp, _P(_i32), _P(_i64)]),
     "ts_tables_copy": (C.c_int, [_vp, _i32, _i32, _fp]),
     "ts_tables_free": (None, [_vp]),
+    "ts_tables_write_qttb": (C.c_int, [_vp, _i32, _i32, _P(C.c_char_p), _P(C.c_char_p), _P(_i32)]),
+    "ts_tables_load_qttb": (C.c_int, [_vp, _gp, _i32, _P(C.c_char_p), _P(_vp)]),
     "ts_locate": (C.c_int, [_vp, _vp, _P(LocatorSettings), _i32, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _P(Location),
                             _dp, _P(LocateStats)]),
     "ts_lsqr_solve": (C.c_int, [_vp, _i32, _i32, _ip, _ip, _dp, _dp, _d, _i32, _d, _d, _d, _dp, _P(LsqrInfo)]),
