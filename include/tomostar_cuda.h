@@ -301,6 +301,32 @@ int ts_lsqr_set_callback(ts_ctx* ctx, ts_lsqr_iteration_fn fn, void* user);
  * otherwise TS_E_SELFTEST. */
 int ts_lsqr_selftest(ts_ctx* ctx, double* rel_err, char* msg, int32_t cap);
 
+/* ---- Forward domain and model (Forward/ForwardDomain.cs:24-137, Forward/TravelTimeTable.cs:213-241) ---- */
+/* VelocityModel1D's nodes (Model/VelocityModel1D.cs:8-45): n depths (non-decreasing; a repeated depth is
+ * a discontinuity) with Vp and Vs, km/s; piecewise linear, the first node's value above it. */
+typedef struct ts_background {
+    int32_t n, reserved;
+    const double* depth_km;
+    const double* vp;
+    const double* vs;
+} ts_background;
+/* ForwardDomain.Covering (:51-107) on the host: the inversion grid refined `refinement` times, or,
+ * when some of the points (lon, lat, depth per point) lie outside the inversion grid, the grid that
+ * holds them with a margin of two cells, coarsened by 1.25 steps until it has at most max_nodes
+ * nodes (<= 0: 12,000,000). *extended: 1 when it reaches beyond the inversion grid; *coarsening: the
+ * spacing factor applied. Errors as text in ts_last_error(NULL). */
+int ts_domain_covering(const ts_grid* inversion, int32_t refinement, int32_t n_points, const double* points,
+                       int64_t max_nodes, ts_grid* out, int32_t* extended, double* coarsening);
+/* ForwardModel.FromInversionGrid (TravelTimeTable.cs:217-241) on the device, into a resident model on
+ * `forward` (as ts_model_put makes): per phase (1: P, 2: P and S) the inversion grid's velocity
+ * 1/inv_slowness interpolated at every forward node (SphericalGrid.ResampleFrom, :241-252), the
+ * background's Vp or Vs where a node lies outside the inversion grid (bg non-NULL: the extended
+ * domain), then slowness = 1/v. Bitwise the reference's arithmetic. */
+int ts_model_put_resampled(ts_ctx* ctx, const ts_grid* forward, const ts_grid* inversion, const double* inv_slowness,
+                           int32_t n_phases, const ts_background* bg, int32_t precision, int32_t* model_id);
+/* A resident model's slowness of one phase to the host (grid-count doubles). */
+int ts_model_copy_slowness(ts_ctx* ctx, int32_t model_id, int32_t phase, double* out);
+
 /* ---- Travel-time tables kept on the device (TravelTimeTableSet, Forward/TravelTimeTable.cs:247-412) ----
  * n_tables float32 fields on one uniform grid, node-major per table as a .qttb file holds them. */
 typedef struct ts_tables ts_tables;

@@ -1497,3 +1497,124 @@ double or_gap(int32_t n, const double* az) { return azimuth_gap(std::vector<doub
 double or_tick_seconds(double t0) { return tick_seconds(t0); }
 
 }  // extern "C"
+
+// ---- Forward domain and model (Forward/ForwardDomain.cs:51-107, Forward/TravelTimeTable.cs:217-241,
+// Model/VelocityModel1D.cs:31-45) ----------------------------------------------------------------
+
+namespace {
+
+// VelocityModel1D.Evaluate.
+double evaluate_1d(const double* depth, const double* v, int n, double d) {
+    if (d <= depth[0]) return v[0];
+    for (int i = 1; i < n; i++) {
+        double a = depth[i - 1], b = depth[i];
+        if (d > b) continue;
+        if (b - a <= 1e-12) continue;
+        double t = (d - a) / (b - a);
+        return v[i - 1] + t * (v[i] - v[i - 1]);
+    }
+    return v[n - 1];
+}
+
+// SphericalGrid.Contains (Geo/SphericalGrid.cs:186-192).
+bool grid_contains(const Grid& g, double lon, double lat, double dep, double tol) {
+    double fx, fy, fz;
+    g.fractional(lon, lat, dep, fx, fy, fz);
+    return fx >= -tol && fx <= g.nx - 1 + tol && fy >= -tol && fy <= g.ny - 1 + tol && fz >= -tol && fz <= g.nz - 1 + tol;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ForwardModel.FromInversionGrid: velocities 1/inv_slowness resampled to the forward nodes
+// (ResampleFrom = Interpolate at LonDeg[i], LatDeg[j], DepthKm[k]); with a background (nbg > 0),
+// nodes outside the inversion grid (tolerance 1e-6) take its Vp (phase 0) or Vs (phase 1); then 1/v.
+void or_resample(const or_grid_def* fwd, const or_grid_def* inv, const double* inv_slowness, int32_t n_phases,
+                 int32_t nbg, const double* bg_depth, const double* bg_vp, const double* bg_vs, double* out) {
+    Grid f(*fwd), g(*inv);
+    const int64_t fn = f.count(), in = g.count();
+    for (int p = 0; p < n_phases; p++) {
+        std::vector<double> v(in);
+        for (int64_t q = 0; q < in; q++) v[q] = 1 / inv_slowness[p * in + q];
+        for (int k = 0; k < f.nz; k++)
+            for (int j = 0; j < f.ny; j++)
+                for (int i = 0; i < f.nx; i++) {
+                    double x = g.interpolate(v.data(), f.lon[i], f.lat[j], f.dep[k]);
+                    if (nbg > 0 && !grid_contains(g, f.lon[i], f.lat[j], f.dep[k], 1e-6))
+                        x = evaluate_1d(bg_depth, p == 0 ? bg_vp : bg_vs, nbg, f.dep[k]);
+                    out[p * fn + f.index(i, j, k)] = 1 / x;
+                }
+    }
+}
+
+// ForwardDomain.Covering; returns 0, or 1 when the points span the globe. Refined is
+// GridDefinition.Refined (Geo/SphericalGrid.cs:51-56).
+int32_t or_covering(const or_grid_def* inv, int32_t refinement, int32_t n_points, const double* points,
+                    int64_t max_nodes, or_grid_def* out, int32_t* extended, double* coarsening) {
+    const int fct = std::max(1, refinement);
+    or_grid_def fine = *inv;
+    if (fct > 1) {
+        fine.nx = (inv->nx - 1) * fct + 1;
+        fine.ny = (inv->ny - 1) * fct + 1;
+        fine.nz = (inv->nz - 1) * fct + 1;
+    }
+    const double fdlon = (fine.max_lon - fine.min_lon) / std::max(1, fine.nx - 1);
+    const double fdlat = (fine.max_lat - fine.min_lat) / std::max(1, fine.ny - 1);
+    const double fddep = (fine.max_depth_km - fine.min_depth_km) / std::max(1, fine.nz - 1);
+    const double centre = 0.5 * (inv->min_lon + inv->max_lon);
+    double min_lon = inv->min_lon, max_lon = inv->max_lon, min_lat = inv->min_lat, max_lat = inv->max_lat;
+    double top = inv->min_depth_km, bottom = inv->max_depth_km;
+    int outside = 0;
+    for (int q = 0; q < n_points; q++) {
+        double lon = unwrap_lon(points[3 * q], centre), lat = points[3 * q + 1], dep = points[3 * q + 2];
+        bool inside = lon >= inv->min_lon && lon <= inv->max_lon && lat >= inv->min_lat && lat <= inv->max_lat &&
+                      dep >= inv->min_depth_km && dep <= inv->max_depth_km;
+        if (inside) continue;
+        outside++;
+        min_lon = std::min(min_lon, lon); max_lon = std::max(max_lon, lon);
+        min_lat = std::min(min_lat, lat); max_lat = std::max(max_lat, lat);
+        bottom = std::max(bottom, dep);
+    }
+    *extended = outside > 0;
+    *coarsening = 1.0;
+    if (outside == 0) {
+        *out = fine;
+        out->depth_km = nullptr;
+        return 0;
+    }
+    min_lon -= 2 * fdlon; max_lon += 2 * fdlon;
+    min_lat = std::max(-89.0, min_lat - 2 * fdlat); max_lat = std::min(89.0, max_lat + 2 * fdlat);
+    if (bottom > inv->max_depth_km) bottom += 2 * fddep;
+    if (max_lon - min_lon >= 359) return 1;
+    double dlon = fdlon, dlat = fdlat, ddep = fddep;
+    auto count = [&](double f) {
+        return int64_t(std::ceil((max_lon - min_lon) / (dlon * f)) + 1) * int64_t(std::ceil((max_lat - min_lat) / (dlat * f)) + 1) *
+               int64_t(std::ceil((bottom - top) / (ddep * f)) + 1);
+    };
+    double factor = 1.0;
+    while (count(factor) > max_nodes) factor *= 1.25;
+    dlon *= factor; dlat *= factor; ddep *= factor;
+    int west = int(std::ceil((inv->min_lon - min_lon) / dlon)), east = int(std::ceil((max_lon - inv->max_lon) / dlon));
+    int south = int(std::ceil((inv->min_lat - min_lat) / dlat)), north = int(std::ceil((max_lat - inv->max_lat) / dlat));
+    int down = int(std::ceil((bottom - inv->max_depth_km) / ddep));
+    int nx = int(std::nearbyint((inv->max_lon - inv->min_lon) / dlon));
+    int ny = int(std::nearbyint((inv->max_lat - inv->min_lat) / dlat));
+    int nz = int(std::nearbyint((inv->max_depth_km - inv->min_depth_km) / ddep));
+    or_grid_def d{};
+    d.min_lon = inv->min_lon - west * dlon;
+    d.max_lon = inv->min_lon - west * dlon + (west + nx + east) * dlon;
+    d.min_lat = inv->min_lat - south * dlat;
+    d.max_lat = inv->min_lat - south * dlat + (south + ny + north) * dlat;
+    d.min_depth_km = inv->min_depth_km;
+    d.max_depth_km = inv->min_depth_km + (nz + down) * ddep;
+    d.nx = west + nx + east + 1; d.ny = south + ny + north + 1; d.nz = nz + down + 1;
+    d.depth_km = nullptr;
+    *out = d;
+    *coarsening = factor;
+    return 0;
+}
+
+double or_background(const double* depth, const double* v, int32_t n, double d) { return evaluate_1d(depth, v, n, d); }
+
+}  // extern "C"

@@ -77,6 +77,9 @@ def lib():
             "or_median": (d, [i32, dp]),
             "or_gap": (d, [i32, dp]),
             "or_tick_seconds": (d, [d]),
+            "or_resample": (None, [g, g, dp, i32, i32, dp, dp, dp, dp]),
+            "or_covering": (i32, [g, i32, i32, dp, i64, g, ip, dp]),
+            "or_background": (d, [dp, dp, i32, d]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -405,3 +408,41 @@ def gap(az):
 
 def tick_seconds(t0):
     return lib().or_tick_seconds(t0)
+
+
+def resample(fwd: Grid, inv: Grid, inv_slowness, background=None):
+    """ForwardModel.FromInversionGrid (Forward/TravelTimeTable.cs:217-241): (n_phases, fwd nodes) slowness.
+    background: (depth, vp, vs) arrays of a VelocityModel1D, or None for the plain refined domain."""
+    s = np.ascontiguousarray(inv_slowness, np.float64).reshape(-1, inv.count)
+    npz = len(s)
+    if background is None:
+        bd = bp = bs = np.zeros(1)
+        nbg = 0
+    else:
+        bd, bp, bs = (np.ascontiguousarray(a, np.float64) for a in background)
+        nbg = len(bd)
+    out = np.empty((npz, fwd.count))
+    lib().or_resample(fwd.ref, inv.ref, _p(s, C.c_double), npz, nbg, _p(bd, C.c_double), _p(bp, C.c_double),
+                      _p(bs, C.c_double), _p(out, C.c_double))
+    return out
+
+
+def covering(inv: Grid, refinement: int, points, max_nodes: int = 12_000_000):
+    """ForwardDomain.Covering (Forward/ForwardDomain.cs:51-107): (GridDef fields, extended, coarsening)."""
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    out = GridDef()
+    ext = C.c_int32()
+    fac = C.c_double()
+    rc = lib().or_covering(inv.ref, refinement, len(pts), _p(pts, C.c_double), max_nodes, C.byref(out), C.byref(ext),
+                           C.byref(fac))
+    if rc:
+        raise ValueError("Stations and events outside the area span the whole globe")
+    fields = (out.min_lon, out.max_lon, out.min_lat, out.max_lat, out.min_depth_km, out.max_depth_km, out.nx, out.ny,
+              out.nz)
+    return fields, bool(ext.value), fac.value
+
+
+def background(depth, v, d):
+    dd = np.ascontiguousarray(depth, np.float64)
+    vv = np.ascontiguousarray(v, np.float64)
+    return lib().or_background(_p(dd, C.c_double), _p(vv, C.c_double), len(dd), d)

@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtomostar_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NO_FMA = {"rays.cu", "locate.cu"}
+NO_FMA = {"rays.cu", "locate.cu", "domain.cu"}
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
           "-I", os.path.join(HERE, "..", "include")]
 
