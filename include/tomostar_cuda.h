@@ -324,6 +324,12 @@ int ts_domain_covering(const ts_grid* inversion, int32_t refinement, int32_t n_p
  * domain), then slowness = 1/v. Bitwise the reference's arithmetic. */
 int ts_model_put_resampled(ts_ctx* ctx, const ts_grid* forward, const ts_grid* inversion, const double* inv_slowness,
                            int32_t n_phases, const ts_background* bg, int32_t precision, int32_t* model_id);
+/* The extended domain's background for the rays (RayKernels.Compute with domain.Extended,
+ * RayKernels.cs:63-65): from this call on, ts_forward and the other ray calls integrate only the
+ * pieces inside the inversion grid (tolerance 1e-6) and sum the others' length times 1/Vp or 1/Vs of
+ * the background (the arrival's phase; ts_rays_trace: Vp) into the row's outside time
+ * (RayTracing.Kernel, RayTracing.cs:126-159). NULL or n = 0 restores the plain domain. */
+int ts_set_background(ts_ctx* ctx, const ts_background* bg);
 /* A resident model's slowness of one phase to the host (grid-count doubles). */
 int ts_model_copy_slowness(ts_ctx* ctx, int32_t model_id, int32_t phase, double* out);
 
@@ -396,6 +402,9 @@ int ts_rows_info(ts_rows* rows, int32_t* n_rows, int64_t* nnz);
 /* Copies a result to the host: row_ptr[n_rows+1], col[nnz] (int32 node), len[nnz] (float32 km),
  * tcalc_grad[4*n_rows] (TCalc s, Ge, Gn, Gz s/km), ok[n_rows]. Any pointer may be NULL. */
 int ts_rows_copy(ts_rows* rows, int32_t* row_ptr, int32_t* col, float* len, double* tcalc_grad, uint8_t* ok);
+/* RayRow.OutsideTime (Tomography/RayKernels.cs:15-19, 95) of every row: the time spent outside the
+ * inversion grid in the background set by ts_set_background (0 without one); n_rows doubles. */
+int ts_rows_outside(ts_rows* rows, double* outside);
 void ts_rows_free(ts_rows* rows);
 
 #ifdef __cplusplus

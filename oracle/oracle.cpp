@@ -453,9 +453,16 @@ bool backtrack(const Table& tb, double lon, double lat, double dep, double step_
     return true;
 }
 
-// RayTracing.Kernel without an outside domain (RayTracing.cs:126-159): (node, length) in first-visit
-// order, each length summed in visit order like the reference's dictionary.
-void ray_kernel(const Grid& inv, const std::vector<Geo>& ray, std::vector<int>& keys, std::vector<double>& vals) {
+double evaluate_1d(const double* depth, const double* v, int n, double d);
+bool grid_contains(const Grid& g, double lon, double lat, double dep, double tol);
+
+// RayTracing.Kernel (RayTracing.cs:126-159): (node, length) in first-visit order, each length summed
+// in visit order like the reference's dictionary. With a background (nbg > 0), pieces outside the
+// inversion grid (tolerance 1e-6) are not attributed: their length times the background's slowness
+// 1/v(depth) is summed into *outside instead.
+void ray_kernel(const Grid& inv, const std::vector<Geo>& ray, std::vector<int>& keys, std::vector<double>& vals,
+                int nbg = 0, const double* bgd = nullptr, const double* bgv = nullptr, double* outside = nullptr) {
+    if (outside) *outside = 0;
     keys.clear();
     vals.clear();
     // node -> slot of keys/vals: open addressing with linear probing, kept under half full
@@ -495,6 +502,10 @@ void ray_kernel(const Grid& inv, const std::vector<Geo>& ray, std::vector<int>& 
         double dl = len / pieces;
         for (int q = 0; q < pieces; q++) {
             Geo mid = from_cartesian(add(a, scale(sub(b, a), (q + 0.5) / pieces)));
+            if (nbg > 0 && !grid_contains(inv, mid.lon, mid.lat, mid.depth, 1e-6)) {
+                *outside += dl * (1 / evaluate_1d(bgd, bgv, nbg, mid.depth));
+                continue;
+            }
             inv.weights(mid.lon, mid.lat, mid.depth, nodes, w);
             for (int n = 0; n < 8; n++) {
                 if (w[n] == 0) continue;
@@ -810,9 +821,25 @@ int32_t or_kernel(const or_grid_def* inv, const double* pts, int32_t n_pts, int3
 // table, TCalc and the source gradient, the kernel on the inversion grid, nodes ascending, lengths
 // cast to float32. Returns nnz (>= 0, an empty row is kept), -1 for an arrival the reference drops,
 // or -2 - needed when cap is too small.
+int32_t or_ray_row_bg(const or_grid_def* fwd, const float* table, double st_lon, double st_lat, double st_dep,
+                      const or_grid_def* inv, double ev_lon, double ev_lat, double ev_dep, double step_km,
+                      int32_t* nodes, float* lens, int32_t cap, double* tcalc_grad4, int32_t nbg, const double* bgd,
+                      const double* bgv, double* outside);
+
 int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, double st_lat, double st_dep,
                    const or_grid_def* inv, double ev_lon, double ev_lat, double ev_dep, double step_km,
                    int32_t* nodes, float* lens, int32_t cap, double* tcalc_grad4) {
+    double outside = 0;
+    return or_ray_row_bg(fwd, table, st_lon, st_lat, st_dep, inv, ev_lon, ev_lat, ev_dep, step_km, nodes, lens, cap,
+                         tcalc_grad4, 0, nullptr, nullptr, &outside);
+}
+
+// RayKernels.Compute's row with the extended domain's background (RayKernels.cs:63-65, 95): bgv is
+// the background's Vp or Vs (the arrival's phase); *outside is RayRow.OutsideTime.
+int32_t or_ray_row_bg(const or_grid_def* fwd, const float* table, double st_lon, double st_lat, double st_dep,
+                      const or_grid_def* inv, double ev_lon, double ev_lat, double ev_dep, double step_km,
+                      int32_t* nodes, float* lens, int32_t cap, double* tcalc_grad4, int32_t nbg, const double* bgd,
+                      const double* bgv, double* outside) {
     Grid g(*fwd);
     Grid ig(*inv);
     Table tb{g, table, st_lon, st_lat, st_dep};
@@ -824,7 +851,7 @@ int32_t or_ray_row(const or_grid_def* fwd, const float* table, double st_lon, do
     if (!std::isfinite(tcalc)) return -1;
     std::vector<int> keys;
     std::vector<double> vals;
-    ray_kernel(ig, path, keys, vals);
+    ray_kernel(ig, path, keys, vals, nbg, bgd, bgv, outside);
     if (int(keys.size()) > cap) return -2 - int(keys.size());
     std::vector<int> order(keys.size());
     for (size_t q = 0; q < order.size(); q++) order[q] = int(q);
@@ -852,6 +879,31 @@ void or_ray_rows_many(const or_grid_def* fwd, const float* tables, const int32_t
             nnz[a] = or_ray_row(fwd, tables + size_t(tab_of[a]) * n, st[3 * a], st[3 * a + 1], st[3 * a + 2], inv,
                                 ev[3 * a], ev[3 * a + 1], ev[3 * a + 2], step_km, nodes + size_t(a) * cap_per_row,
                                 lens + size_t(a) * cap_per_row, cap_per_row, tcalc_grad4 + 4 * size_t(a));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); t++) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+}
+
+// or_ray_rows_many with the background of the extended domain: tab_phase[t] picks Vp (0) or Vs (1);
+// outside[a] is row a's time outside the inversion grid.
+void or_ray_rows_many_bg(const or_grid_def* fwd, const float* tables, const int32_t* tab_of, const int32_t* tab_phase,
+                         const double* st, const or_grid_def* inv, const double* ev, int32_t n_rays, double step_km,
+                         int32_t cap_per_row, int32_t* nnz, int32_t* nodes, float* lens, double* tcalc_grad4,
+                         int32_t nbg, const double* bgd, const double* bgvp, const double* bgvs, double* outside,
+                         int32_t threads) {
+    int64_t n = int64_t(fwd->nx) * fwd->ny * fwd->nz;
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (;;) {
+            int a = next.fetch_add(1);
+            if (a >= n_rays) return;
+            const double* bgv = tab_phase[tab_of[a]] == 0 ? bgvp : bgvs;
+            nnz[a] = or_ray_row_bg(fwd, tables + size_t(tab_of[a]) * n, st[3 * a], st[3 * a + 1], st[3 * a + 2], inv,
+                                   ev[3 * a], ev[3 * a + 1], ev[3 * a + 2], step_km, nodes + size_t(a) * cap_per_row,
+                                   lens + size_t(a) * cap_per_row, cap_per_row, tcalc_grad4 + 4 * size_t(a), nbg, bgd,
+                                   bgv, outside + a);
         }
     };
     std::vector<std::thread> pool;

@@ -80,6 +80,8 @@ def lib():
             "or_resample": (None, [g, g, dp, i32, i32, dp, dp, dp, dp]),
             "or_covering": (i32, [g, i32, i32, dp, i64, g, ip, dp]),
             "or_background": (d, [dp, dp, i32, d]),
+            "or_ray_rows_many_bg": (None, [g, fp, ip, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32, dp, dp, dp, dp,
+                                           i32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -446,3 +448,26 @@ def background(depth, v, d):
     dd = np.ascontiguousarray(depth, np.float64)
     vv = np.ascontiguousarray(v, np.float64)
     return lib().or_background(_p(dd, C.c_double), _p(vv, C.c_double), len(dd), d)
+
+
+def ray_rows_many_bg(fwd: Grid, tables, tab_of, tab_phase, stations, inv: Grid, events, step_km, background,
+                     cap_per_row=4096, threads=None):
+    """ray_rows_many with the extended domain's background (depth, vp, vs): also each row's outside time."""
+    tb = np.ascontiguousarray(tables, np.float32)
+    to = np.ascontiguousarray(tab_of, np.int32)
+    tp = np.ascontiguousarray(tab_phase, np.int32)
+    st = np.ascontiguousarray(stations, np.float64)
+    ev = np.ascontiguousarray(events, np.float64)
+    bd, bp, bs = (np.ascontiguousarray(a, np.float64) for a in background)
+    nr = len(to)
+    nnz = np.zeros(nr, np.int32)
+    nodes = np.empty(nr * cap_per_row, np.int32)
+    lens = np.empty(nr * cap_per_row, np.float32)
+    tg = np.empty((nr, 4))
+    out = np.zeros(nr)
+    lib().or_ray_rows_many_bg(fwd.ref, _p(tb, C.c_float), _p(to, C.c_int32), _p(tp, C.c_int32), _p(st, C.c_double),
+                              inv.ref, _p(ev, C.c_double), nr, step_km, cap_per_row, _p(nnz, C.c_int32),
+                              _p(nodes, C.c_int32), _p(lens, C.c_float), _p(tg, C.c_double), len(bd),
+                              _p(bd, C.c_double), _p(bp, C.c_double), _p(bs, C.c_double), _p(out, C.c_double),
+                              threads or os.cpu_count())
+    return nnz, nodes.reshape(nr, cap_per_row), lens.reshape(nr, cap_per_row), tg, out

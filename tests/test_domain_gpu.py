@@ -66,3 +66,54 @@ def test_resample_refusals(solver):
         domain.put_resampled(solver, g, inv, s)
     with pytest.raises(L.TsError):
         domain.put_resampled(solver, inv.refined(2), inv, np.concatenate([s, s]))  # three or four phases
+
+
+def test_forward_step_extended_domain_outside_time(solver):
+    """RayKernels.Compute on a covering domain (RayKernels.cs:63-95): stations and events outside the
+    inversion grid, the forward model resampled with a 1-D background outside it, rays whose pieces
+    outside the inversion grid give time outside (RayRow.OutsideTime) instead of row entries; against
+    the oracle's pipeline on the same tables."""
+    from test_rays_gpu import compare_rows
+    from tomostar_b200.rays import RayKernels, step_km
+
+    inv, s = _model()
+    rng = np.random.default_rng(7)
+    lon = lambda f: inv.min_lon + f * (inv.max_lon - inv.min_lon)  # noqa: E731
+    lat = lambda f: inv.min_lat + f * (inv.max_lat - inv.min_lat)  # noqa: E731
+    stations = np.array([[lon(0.2), lat(0.3), 0.0], [lon(0.8), lat(0.6), 0.0], [lon(0.5), lat(0.9), 0.0],
+                         [lon(1.35), lat(0.5), 0.0], [lon(0.4), lat(-0.3), 0.0]])
+    events = np.array([[lon(f), lat(g), d] for f, g, d in rng.uniform([0.1, 0.1, 3], [0.9, 0.9, 16], (6, 3))] +
+                      [[lon(1.25), lat(0.2), 8.0], [lon(-0.3), lat(1.2), 12.0], [lon(0.5), lat(0.5), 28.0]])
+    fwd, ext, _ = domain.covering(inv, 2, np.concatenate([stations, events]))
+    assert ext
+    bg = domain.Background(np.array([0.0, 12.0, 12.0, 40.0]), np.array([5.3, 6.0, 6.4, 7.8]),
+                           np.array([3.05, 3.45, 3.7, 4.5]))
+    slow = O.resample(O.Grid.of(fwd), O.Grid.of(inv), s, (bg.depth_km, bg.vp, bg.vs))
+    arrivals = np.array([[e, k, p] for e in range(len(events)) for k in range(len(stations)) for p in (0, 1)],
+                        np.int32)
+    domain.set_background(solver, bg)
+    try:
+        gpu = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64)
+    finally:
+        domain.set_background(solver, None)
+    og = O.Grid.of(fwd)
+    tables, index = [], {}
+    for p in (0, 1):
+        for k in range(len(stations)):
+            idx, t = point_source(fwd, slow[p], *stations[k])
+            f, ok, _ = O.relax(og, slow[p], idx, t)
+            assert ok
+            index[(p, k)] = len(tables)
+            tables.append(O.to_table(f))
+    tab_of = np.array([index[(p, k)] for _, k, p in arrivals], np.int32)
+    tab_phase = np.array([p for (p, _k) in sorted(index, key=index.get)], np.int32)
+    nnz, nodes, lens, tg, outside = O.ray_rows_many_bg(og, np.stack(tables), tab_of, tab_phase,
+                                                       stations[arrivals[:, 1]], O.Grid.of(inv), events[arrivals[:, 0]],
+                                                       step_km(fwd, inv), (bg.depth_km, bg.vp, bg.vs))
+    compare_rows(gpu, nnz, nodes, lens, tg)
+    ok = nnz >= 0
+    assert (outside[ok] > 0).sum() >= 10 and (outside[ok] == 0).sum() >= 10
+    assert np.max(np.abs(gpu.outside[ok] - outside[ok])) <= 1e-9 * max(1.0, float(outside.max()))
+    # Without the background the same rays keep every piece (outside time 0).
+    plain = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64)
+    assert not plain.outside.any() and plain.nnz > gpu.nnz

@@ -137,6 +137,8 @@ SIGNATURES = {
     "ts_domain_covering": (C.c_int, [_gp, _i32, _i32, _P(C.c_double), _i64, _gp, _P(_i32), _P(C.c_double)]),
     "ts_model_put_resampled": (C.c_int, [_vp, _gp, _gp, _P(C.c_double), _i32, _P(Background), _i32, _P(_i32)]),
     "ts_model_copy_slowness": (C.c_int, [_vp, _i32, _i32, _P(C.c_double)]),
+    "ts_set_background": (C.c_int, [_vp, _P(Background)]),
+    "ts_rows_outside": (C.c_int, [_vp, _P(C.c_double)]),
     "ts_tables_build": (C.c_int, [_vp, _gp, _dp, _i32, _i32, _dp, _ip, _i32, _P(_vp), _P(EikStats)]),
     "ts_tables_upload": (C.c_int, [_vp, _gp, _i32, _fp, _P(_vp)]),
     "ts_tables_info": (C.c_int, [_vp, _P(_i32), _P(_i64)]),

@@ -26,6 +26,9 @@ struct ts_ctx {
     int tile_f64 = 0, tile_f32 = 0;       // engine tile shape per precision
     int scheduler = 0;                    // engine scheduler: 0 lockstep diagonals, 1 flow (per field)
     double epoch_budget_ms = 0;           // flow epochs: fields pause at the first round end after this
+    // The extended domain's 1-D background for the rays' outside time (ts_set_background): node count,
+    // the nodes in the "rays.background" buffer (depths, Vp, Vs).
+    int bg_n = 0;
     // LSQR's onIteration (Numerics/Lsqr.cs:43,140): called after every iteration with its ‖r‖.
     void (*lsqr_on_iteration)(int32_t iteration, double rnorm, void* user) = nullptr;
     void* lsqr_user = nullptr;

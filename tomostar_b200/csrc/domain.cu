@@ -22,26 +22,6 @@ namespace domain {
 
 using geo::RGrid;
 
-// VelocityModel1D.Evaluate (Model/VelocityModel1D.cs:31-45): piecewise linear in depth, the upper
-// value on an interface, the first node's above it and the last node's below the last.
-__host__ __device__ __forceinline__ double background(const double* depth, const double* v, int n, double d) {
-    if (d <= depth[0]) return v[0];
-    for (int i = 1; i < n; i++) {
-        if (d > depth[i]) continue;
-        if (depth[i] - depth[i - 1] <= 1e-12) continue;  // discontinuity: move below it
-        const double t = (d - depth[i - 1]) / (depth[i] - depth[i - 1]);
-        return v[i - 1] + t * (v[i] - v[i - 1]);
-    }
-    return v[n - 1];
-}
-
-// SphericalGrid.Contains (Geo/SphericalGrid.cs:186-192).
-__device__ __forceinline__ bool contains(const RGrid& g, double lon, double lat, double dep, double tol) {
-    double fx, fy, fz;
-    geo::fractional(g, lon, lat, dep, fx, fy, fz);
-    return fx >= -tol && fx <= g.nx - 1 + tol && fy >= -tol && fy <= g.ny - 1 + tol && fz >= -tol && fz <= g.nz - 1 + tol;
-}
-
 // ForwardModel.FromInversionGrid (TravelTimeTable.cs:217-241) per forward node and phase: the
 // velocity 1/s of the inversion grid interpolated at the node (SphericalGrid.Interpolate, all eight
 // terms), the background's where the node lies outside the inversion grid (tolerance 1e-6), then 1/v.
@@ -54,7 +34,7 @@ __global__ void resample_kernel(const RGrid fg, const RGrid ig, const double* __
          idx += int64_t(gridDim.x) * blockDim.x) {
         const int i = int(idx % fg.nx), j = int((idx / fg.nx) % fg.ny), k = int(idx / (int64_t(fg.nx) * fg.ny));
         const double lon = fg.min_lon + i * fg.dlon, lat = fg.min_lat + j * fg.dlat, dep = fg.min_dep + k * fg.ddep;
-        const bool outside = nbg > 0 && !contains(ig, lon, lat, dep, 1e-6);
+        const bool outside = nbg > 0 && !geo::contains(ig, lon, lat, dep, 1e-6);
         double fx, fy, fz;
         geo::fractional(ig, lon, lat, dep, fx, fy, fz);
         int i0, j0, k0;
@@ -65,7 +45,7 @@ __global__ void resample_kernel(const RGrid fg, const RGrid ig, const double* __
         for (int p = 0; p < n_phases; p++) {
             double v;
             if (outside) {
-                v = background(bg_depth, bg_v + p * nbg, nbg, dep);
+                v = geo::background_1d(bg_depth, bg_v + p * nbg, nbg, dep);
             } else {
                 const double* s = inv_s + p * inv_n;
                 double sum = 0;
@@ -276,6 +256,31 @@ int ts_model_copy_slowness(ts_ctx* ctx, int32_t model_id, int32_t phase, double*
                                     cudaMemcpyDeviceToHost));
         for (size_t q = 0; q < n; q++) out[q] = tmp[q];
     }
+    return TS_OK;
+}
+
+int ts_set_background(ts_ctx* ctx, const ts_background* bg) {
+    if (!ctx) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!bg || bg->n == 0) {
+        ctx->bg_n = 0;
+        return TS_OK;
+    }
+    if (bg->n < 0 || !bg->depth_km || !bg->vp || !bg->vs) return ctx->fail(TS_E_ARG, "bad background model");
+    for (int q = 0; q < bg->n; q++)
+        if (!(bg->vp[q] > 0) || !(bg->vs[q] > 0) || (q > 0 && bg->depth_km[q] < bg->depth_km[q - 1]))
+            return ctx->fail(TS_E_ARG, "background velocities must be positive and depths non-decreasing");
+    std::vector<double> v(3 * size_t(bg->n));
+    for (int q = 0; q < bg->n; q++) {
+        v[q] = bg->depth_km[q];
+        v[bg->n + q] = bg->vp[q];
+        v[2 * bg->n + q] = bg->vs[q];
+    }
+    double* d = static_cast<double*>(ctx->buf("rays.background", sizeof(double) * v.size()));
+    if (!d) return TS_E_NOMEM;
+    TS_CUDA_TRY(ctx, cudaMemcpy(d, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    ctx->bg_n = bg->n;
     return TS_OK;
 }
 

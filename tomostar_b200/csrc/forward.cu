@@ -171,8 +171,10 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
         for (int c = 0; c < 3; c++) ev[3 * a + c] = events[3 * arr_event[a] + c];
     }
     if (!(step_km > 0)) step_km = 0.5 * std::min(g.min_spacing_km(), gi.min_spacing_km());  // RayKernels.cs:62
+    std::vector<int32_t> table_phase(std::max(1, nt));
+    for (int t = 0; t < nt; t++) table_phase[t] = tables[t].first;
     return rays::trace_on_device(ctx, g, tab, std::max(1, nt), table_station.data(), gi, n_arr, table_of.data(),
-                                 ev.data(), step_km, out, nullptr);
+                                 ev.data(), step_km, out, nullptr, table_phase.data());
 }
 
 }  // namespace fwd

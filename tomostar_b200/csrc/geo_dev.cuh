@@ -135,5 +135,25 @@ TS_DEVINL void table_gradient(const RGrid& g, const float* tb, double lon, doubl
     gz = tz / hz;
 }
 
+// SphericalGrid.Contains (Geo/SphericalGrid.cs:186-192).
+TS_DEVINL bool contains(const RGrid& g, double lon, double lat, double dep, double tol) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    return fx >= -tol && fx <= g.nx - 1 + tol && fy >= -tol && fy <= g.ny - 1 + tol && fz >= -tol && fz <= g.nz - 1 + tol;
+}
+
+// VelocityModel1D.Evaluate (Model/VelocityModel1D.cs:31-45): piecewise linear in depth, the upper
+// value on an interface, the first node's value above it and the last node's below the last.
+TS_HDINL double background_1d(const double* depth, const double* v, int n, double d) {
+    if (d <= depth[0]) return v[0];
+    for (int i = 1; i < n; i++) {
+        if (d > depth[i]) continue;
+        if (depth[i] - depth[i - 1] <= 1e-12) continue;  // discontinuity: move below it
+        const double t = (d - depth[i - 1]) / (depth[i] - depth[i - 1]);
+        return v[i - 1] + t * (v[i] - v[i - 1]);
+    }
+    return v[n - 1];
+}
+
 }  // namespace geo
 }  // namespace ts

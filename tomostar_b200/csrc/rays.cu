@@ -45,6 +45,10 @@ struct TraceArgs {
     double* rec_val;
     int* rec_count;               // per chunk ray
     double* tcg;                  // 4 per ray (global index)
+    double* outside;              // per ray (global index): time outside the inversion grid
+    int bg_n;                     // > 0: the extended domain's background (depths, Vp, Vs at bg)
+    const double* bg;
+    const int* table_phase;       // per table: 0 P (Vp), 1 S (Vs)
 };
 
 // Per-ray record writer with the current inversion cell's eight accumulators.
@@ -54,6 +58,8 @@ struct Recorder {
     double acc[8];
     int count = 0;
     bool overflow = false;
+    double outside = 0;           // RayRow.OutsideTime
+    const double* bgv = nullptr;  // the background's velocity of the ray's phase
 
     TS_DEVINL void flush(const TraceArgs& a, int r) {
         if (ci < 0 || !touched) return;
@@ -86,6 +92,12 @@ struct Recorder {
         double dl = len / pieces;
         for (int q = 0; q < pieces; q++) {
             GeoPt mid = geo::from_cartesian(geo::add(A, geo::scale(d, (q + 0.5) / pieces)));
+            // The extended domain (RayTracing.cs:141-145): a piece outside the inversion grid is
+            // not attributed; its length times the background's slowness is time outside.
+            if (a.bg_n > 0 && !geo::contains(a.inv, mid.lon, mid.lat, mid.dep, 1e-6)) {
+                outside += dl * (1 / geo::background_1d(a.bg, bgv, a.bg_n, mid.dep));
+                continue;
+            }
             double fx, fy, fz;
             geo::fractional(a.inv, mid.lon, mid.lat, mid.dep, fx, fy, fz);
             int i0, j0, k0;
@@ -118,6 +130,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     const double st_dep = fmin(fmax(a.table_station[3 * tab + 2], g.min_dep), g.dep_last);
     const GeoPt ev{a.events[3 * ray], a.events[3 * ray + 1], a.events[3 * ray + 2]};
     double* tcg = a.tcg + 4 * int64_t(ray);
+    a.outside[ray] = 0;
 
     // Backtrack (RayTracing.cs:75-110).
     V3 station = geo::to_cartesian(st_lon, st_lat, st_dep);
@@ -134,6 +147,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     double last_t = t0;
     int stalls = 0;
     Recorder rec;
+    if (a.bg_n > 0) rec.bgv = a.bg + (a.table_phase[tab] == 0 ? 1 : 2) * a.bg_n;
     GeoPt prev = ev;
     for (int s = 0; s < max_steps; s++) {
         if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
@@ -176,6 +190,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     }
     rec.segment(a, r, prev, GeoPt{st_lon, st_lat, st_dep});
     rec.flush(a, r);
+    a.outside[ray] = rec.outside;
     a.rec_count[r] = rec.overflow ? kOverflow : rec.count;
 }
 
@@ -331,11 +346,12 @@ struct ts_rows {
     float* len = nullptr;
     double* tcg = nullptr;    // device, 4 per row
     uint8_t* ok = nullptr;
+    double* outside = nullptr;  // device, per row: RayRow.OutsideTime
     // Stream-ordered frees: no device-wide synchronisation while other work runs (serving).
     ~ts_rows() {
         cudaStream_t s = ctx ? ctx->stream : nullptr;
         for (void* p : {static_cast<void*>(row_ptr), static_cast<void*>(col), static_cast<void*>(len),
-                        static_cast<void*>(tcg), static_cast<void*>(ok)})
+                        static_cast<void*>(tcg), static_cast<void*>(ok), static_cast<void*>(outside)})
             if (p) cudaFreeAsync(p, s);
     }
 };
@@ -346,7 +362,7 @@ namespace rays {
 static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, const float* const* table_ptrs_host,
                       int n_tables, const double* table_station_host, const host::Grid& inv, int n_rays,
                       const int32_t* table_of_host, const double* events_host, double step_km, ts_rows** out,
-                      RayStats* st) {
+                      RayStats* st, const int32_t* table_phase_host) {
     cudaStream_t s = ctx->stream;
     const int64_t n = fwd.count();
     for (int a = 0; a < n_rays; a++)
@@ -362,7 +378,9 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     };
     if (cudaMallocAsync(reinterpret_cast<void**>(&rows->row_ptr), sizeof(int) * (n_rays + 1), s) != cudaSuccess ||
         cudaMallocAsync(reinterpret_cast<void**>(&rows->tcg), sizeof(double) * 4 * std::max(1, n_rays), s) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&rows->ok), std::max(1, n_rays), s) != cudaSuccess) {
+        cudaMallocAsync(reinterpret_cast<void**>(&rows->ok), std::max(1, n_rays), s) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&rows->outside), sizeof(double) * std::max(1, n_rays), s) !=
+            cudaSuccess) {
         cudaGetLastError();
         ctx->fail(TS_E_NOMEM, "row buffers");
         return bail(TS_E_NOMEM);
@@ -392,6 +410,17 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     a.step_km = step_km;
     a.piece_km = 0.5 * inv.min_spacing_km();  // RayTracing.cs:130
     a.tcg = rows->tcg;
+    a.outside = rows->outside;
+    // The extended domain's background (ts_set_background) and each table's phase.
+    a.bg_n = ctx->bg_n;
+    a.bg = a.bg_n > 0 ? static_cast<const double*>(ctx->buf("rays.background", sizeof(double) * 3 * a.bg_n))
+                      : nullptr;
+    std::vector<int32_t> phases(std::max(1, n_tables), 0);
+    if (table_phase_host)
+        for (int t = 0; t < n_tables; t++) phases[t] = table_phase_host[t] == 1 ? 1 : 0;
+    TS_BUF(ctx, d_phase, int, "rays.table_phase", std::max(1, n_tables));
+    TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_phase, phases.data(), sizeof(int) * phases.size(), cudaMemcpyHostToDevice, s));
+    a.table_phase = d_phase;
 
     // Record capacity: one record per node per inversion cell crossed, with room for a path
     // three times the straight length; a ray that needs more is traced again with more room.
@@ -506,16 +535,17 @@ namespace rays {
 
 int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
                     const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
-                    const double* events_host, double step_km, ts_rows** out, RayStats* st) {
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st,
+                    const int32_t* table_phase_host) {
     return trace_impl(ctx, fwd, tables_dev, nullptr, n_tables, table_station_host, inv, n_rays, table_of_host,
-                      events_host, step_km, out, st);
+                      events_host, step_km, out, st, table_phase_host);
 }
 
 int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const std::vector<const float*>& tables, const double* table_station_host,
                     const host::Grid& inv, int n_rays, const int32_t* table_of_host, const double* events_host,
-                    double step_km, ts_rows** out, RayStats* st) {
+                    double step_km, ts_rows** out, RayStats* st, const int32_t* table_phase_host) {
     return trace_impl(ctx, fwd, nullptr, tables.data(), int(tables.size()), table_station_host, inv, n_rays,
-                      table_of_host, events_host, step_km, out, st);
+                      table_of_host, events_host, step_km, out, st, table_phase_host);
 }
 
 int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begin, std::vector<ts_rows*>& parts) {
@@ -545,6 +575,7 @@ int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begi
         if (cudaMallocAsync(reinterpret_cast<void**>(&p->row_ptr), sizeof(int) * (n + 1), s) != cudaSuccess ||
             cudaMallocAsync(reinterpret_cast<void**>(&p->tcg), sizeof(double) * 4 * std::max(1, n), s) != cudaSuccess ||
             cudaMallocAsync(reinterpret_cast<void**>(&p->ok), std::max(1, n), s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&p->outside), sizeof(double) * std::max(1, n), s) != cudaSuccess ||
             cudaMallocAsync(reinterpret_cast<void**>(&p->col), sizeof(int) * std::max<int64_t>(1, nnz), s) != cudaSuccess ||
             cudaMallocAsync(reinterpret_cast<void**>(&p->len), sizeof(float) * std::max<int64_t>(1, nnz), s) != cudaSuccess)
             return fail();
@@ -554,6 +585,8 @@ int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begi
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->tcg, all->tcg + 4 * int64_t(r0), sizeof(double) * 4 * n,
                                              cudaMemcpyDeviceToDevice, s));
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->ok, all->ok + r0, size_t(n), cudaMemcpyDeviceToDevice, s));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->outside, all->outside + r0, sizeof(double) * n,
+                                             cudaMemcpyDeviceToDevice, s));
         }
         if (nnz) {
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->col, all->col + z0, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
@@ -619,6 +652,18 @@ int ts_rows_copy(ts_rows* rows, int32_t* row_ptr, int32_t* col, float* len, doub
     if (tcalc_grad && n) TS_CUDA_TRY(ctx, cudaMemcpyAsync(tcalc_grad, rows->tcg, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
     if (ok && n) TS_CUDA_TRY(ctx, cudaMemcpyAsync(ok, rows->ok, size_t(n), cudaMemcpyDeviceToHost, s));
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return TS_OK;
+}
+
+int ts_rows_outside(ts_rows* rows, double* outside) {
+    if (!rows || !outside) return TS_E_ARG;
+    ts_ctx* ctx = rows->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (rows->n_rows > 0)
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(outside, rows->outside, sizeof(double) * rows->n_rows, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return TS_OK;
 }
 

@@ -16,14 +16,18 @@ struct RayStats {
 
 // Traces n_rays rays on device-resident float32 tables (n_tables fields on fwd) and builds their
 // CSR rows on the inversion grid; host arrays: table_station (3 per table), table_of and events.
+// With a background set on the context (ts_set_background) pieces outside the inversion grid give
+// time outside instead of row entries, at the Vp (table phase 0) or Vs (1) of the background.
 int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const float* tables_dev, int n_tables,
                     const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
-                    const double* events_host, double step_km, ts_rows** out, RayStats* st);
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st,
+                    const int32_t* table_phase_host = nullptr);
 
 // The same with each table in a buffer of its own (tables[t] on the device).
 int trace_on_device(ts_ctx* ctx, const host::Grid& fwd, const std::vector<const float*>& tables,
                     const double* table_station_host, const host::Grid& inv, int n_rays, const int32_t* table_of_host,
-                    const double* events_host, double step_km, ts_rows** out, RayStats* st);
+                    const double* events_host, double step_km, ts_rows** out, RayStats* st,
+                    const int32_t* table_phase_host = nullptr);
 
 // Cuts a result into consecutive row ranges [row_begin[k], row_begin[k+1]), each a result of its
 // own (stream-ordered copies on the context's stream).

@@ -79,3 +79,11 @@ def copy_slowness(solver, model_id: int, phase: int, count: int) -> np.ndarray:
     if rc != L.TS_OK:
         raise L.TsError(rc, solver.last_error)
     return out
+
+
+def set_background(solver, background: Background | None) -> None:
+    """The extended domain's background for the rays' outside time (RayKernels.cs:63-65); None clears it."""
+    b = background.struct() if background is not None else None
+    rc = L.load().ts_set_background(solver.handle, C.byref(b) if b is not None else None)
+    if rc != L.TS_OK:
+        raise L.TsError(rc, solver.last_error)

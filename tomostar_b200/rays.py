@@ -43,6 +43,7 @@ class Rows:
     len: np.ndarray          # float32 (nnz) km
     tcalc_grad: np.ndarray   # float64 (n_rows, 4): TCalc, Ge, Gn, Gz
     ok: np.ndarray           # bool (n_rows)
+    outside: np.ndarray | None = None  # float64 (n_rows): RayRow.OutsideTime (0 without a background)
 
     @property
     def n_rows(self) -> int:
@@ -81,10 +82,13 @@ def _fetch(handle) -> Rows:
     rc = lib.ts_rows_copy(handle, rp.ctypes.data_as(P(C.c_int32)), col.ctypes.data_as(P(C.c_int32)),
                           ln.ctypes.data_as(P(C.c_float)), tg.ctypes.data_as(P(C.c_double)),
                           ok.ctypes.data_as(P(C.c_uint8)))
+    out = np.empty(n.value)
+    if rc == L.TS_OK:
+        rc = lib.ts_rows_outside(handle, out.ctypes.data_as(P(C.c_double)))
     lib.ts_rows_free(handle)
     if rc != L.TS_OK:
         raise L.TsError(rc, "copying rows")
-    return Rows(rp, col, ln, tg, ok.astype(bool))
+    return Rows(rp, col, ln, tg, ok.astype(bool), out)
 
 
 def step_km(forward: GridDef, inversion: GridDef) -> float:
