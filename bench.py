@@ -249,6 +249,44 @@ def location_job(device: int, n_events: int, cpu_events: int, threads: int) -> d
     }
 
 
+def resample_job(device: int) -> dict:
+    """ForwardModel.FromInversionGrid on the device for the 401x401x121 model: P and S slowness of
+    the 19.46 M forward nodes from the 201x201x61 inversion grid (ts_model_put_resampled, end to end:
+    inversion slowness from the host, the model left resident), against the C++ restatement on one core."""
+    from oracle import oracle as O
+    from tomostar_b200 import _lib as L
+    from tomostar_b200 import domain
+    from tomostar_b200 import synthetic as syn
+    from tomostar_b200.eikonal import EikonalCuda
+
+    g = syn.regular_grid(401, 401, 121, 0.25)
+    inv = g.coarsened(2)
+    rng = np.random.default_rng(21)
+    vp = 5.0 + 0.04 * np.repeat(inv.depth(), inv.nx * inv.ny) + 0.2 * rng.standard_normal(inv.count)
+    s_inv = np.stack([1 / vp, 1.73 / vp])
+    times = []
+    with EikonalCuda.create(device, 64) as s:
+        for rep in range(4):
+            t0 = time.perf_counter()
+            mid = domain.put_resampled(s, g, inv, s_inv)
+            times.append(time.perf_counter() - t0)
+            if rep == 0:
+                got = domain.copy_slowness(s, mid, 0, g.count)
+            L.load().ts_model_drop(s.handle, mid)
+    t_dev = min(times[1:])
+    t1 = time.perf_counter()
+    want = O.resample(O.Grid.of(g), O.Grid.of(inv), s_inv)
+    cpu_s = time.perf_counter() - t1
+    out_gb = 2 * g.count * 8 / 1e9
+    return {"workload": "401x401x121 forward nodes (19.46 M) x P,S from the 201x201x61 inversion grid, FP64",
+            "wall_s": t_dev, "nodes_per_s": 2 * g.count / t_dev, "slowness_gbs_written": out_gb / t_dev,
+            "bitwise_equal_restatement": bool(np.array_equal(got, want[0])),
+            "cpu_baseline": {"wall_s": cpu_s, "cores": 1, "kind": "port",
+                             "sample": "the whole grid, the C++ restatement"},
+            "speedup_vs_cpu": cpu_s / t_dev,
+            "note": "end to end per call: 39 MB of inversion slowness uploaded, 311 MB model allocated and written"}
+
+
 def run_reference(args, problem_fn):
     # The CPU arm needs no process group: rank 0 alone runs it and prints the line.
     if int(os.environ.get("RANK", "0")) != 0:
@@ -462,9 +500,17 @@ def run_ours(args, problem_fn):
                             "note": "setup = transpose built on the device from the resident rows, column order as the host transpose"}}
         del rows
         fsolver.close()
-    location = None
+    location = resample = None
     if world == 1 and not args.no_location:
-        location = location_job(local, args.location_events, args.location_cpu_events, os.cpu_count() or 1)
+        # Sections beside the headline: a failure is reported in the line, not fatal to it.
+        try:
+            location = location_job(local, args.location_events, args.location_cpu_events, os.cpu_count() or 1)
+        except Exception as exc:  # noqa: BLE001
+            location = {"error": repr(exc)[:300]}
+        try:
+            resample = resample_job(local)
+        except Exception as exc:  # noqa: BLE001
+            resample = {"error": repr(exc)[:300]}
     # The serving load (Poisson stream of mixed requests) on one GPU, after the batch job's buffers
     # are released; at N = 1 only (the scaling runs measure the batch job).
     serving = None
@@ -500,6 +546,7 @@ def run_ours(args, problem_fn):
             "plain_gpu": plain,
             "forward_step": forward,
             "location": location,
+            "resample": resample,
             "serving": serving,
             "node_updates_per_step": updates // args.steps,
             "wall_s_timed": t_wall,
