@@ -1,13 +1,18 @@
 // ORACLE — TEST INFRASTRUCTURE ONLY.
 //
-// A CPU restatement of TomoSTAR's forward path, used by the tests, by the smoke check and by
-// bench.py's CPU-baseline leg as the checker and baseline. The product (tomostar_b200/) never
-// links, loads or calls this file.
+// A CPU restatement of TomoSTAR's forward path and of its callers on either side (LSQR, event
+// location, the forward domain and model), used by the tests, by the smoke check and by bench.py's
+// CPU-baseline legs as the checker and baseline. The product (tomostar_b200/) never links, loads or
+// calls this file.
 //
 // Parity status: the reference is C# (.NET 10) and cannot be built or run here, so no bitwise
-// reference output exists. This restatement is pinned by the reference's own known-answer tests
-// (tests/TomoStar.Tests/NumericsTests.cs:88-123) and by the analytic cases of its validation
-// exporter (validation/TomoStar.Validation/Program.cs:107-143); tests/test_oracle.py runs them.
+// reference output exists. The forward path is pinned by the reference's own known-answer tests
+// (tests/TomoStar.Tests/NumericsTests.cs:88-123) and the analytic cases of its validation exporter
+// (validation/TomoStar.Validation/Program.cs:107-143); LSQR by SciPy's lsqr (the SOL kernel
+// Lsqr.cs follows); location by PipelineTests.RelocationMovesEventsTowardsTheTruth
+// (tests/TomoStar.Tests/PipelineTests.cs:95-107) and hand-worked medians and gaps; the forward
+// domain and the 1-D background by hand-worked cases. tests/test_oracle.py and tests/test_domain.py
+// run them.
 //
 // Every function cites the reference lines it follows. Arithmetic is kept in the reference's
 // expression order and the file is compiled with -ffp-contract=off, so a double result is the

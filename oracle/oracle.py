@@ -1,8 +1,10 @@
 """ctypes front end of the C++ oracle (oracle.cpp) — TEST INFRASTRUCTURE ONLY.
 
 The oracle restates the reference's CPU solvers (Forward/SphericalEikonal.cs, Forward/RayTracing.cs,
-Forward/TravelTimeTable.cs, Tomography/RayKernels.cs). Parity status: pinned by the reference's own
-known-answer tests, not by bitwise reference output (the reference is C#/.NET and cannot run here).
+Forward/TravelTimeTable.cs, Tomography/RayKernels.cs) and the callers beside them (Numerics/Lsqr.cs,
+Location/EventLocator.cs, Forward/ForwardDomain.cs). Parity status: pinned by the reference's own
+known-answer tests and, for LSQR, by SciPy's lsqr; not by bitwise reference output (the reference is
+C#/.NET and cannot run here).
 """
 from __future__ import annotations
 
