@@ -482,8 +482,9 @@ def run_ours(args, problem_fn):
         n_rows = int(rows.n_rows)
         nnz = int(rows.nnz)
         # Algorithmic bytes of one LSQR iteration: A·v and Aᵀ·u each read every non-zero's column
-        # index and value (4 + 8 B) and read and write their output vector.
-        it_bytes = 2 * nnz * 12 + 16 * (n_rows + p.inv.count)
+        # index and float32 length (4 + 4 B, the rows as the rays leave them) and read and write their
+        # output vector.
+        it_bytes = 2 * nnz * 8 + 16 * (n_rows + p.inv.count)
         it_ms = lres.device_ms / max(1, lres.iterations)
         lsqr_gbs = it_bytes / (it_ms / 1e3) / 1e9
         peak, _ = measured_hbm_peak()

@@ -114,6 +114,21 @@ struct ts_ctx {
     type* var = static_cast<type*>((ctx)->buf((key), sizeof(type) * size_t(count))); \
     if (!var) return TS_E_NOMEM
 
+// Two timing events destroyed on every return path.
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EventPair() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+};
+
 // The error text of calls made without a context (ts_last_error(NULL)), per host thread.
 std::string& ts_thread_error();
 

@@ -971,9 +971,8 @@ extern "C" int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settin
     host::Grid g(tables->def);
     const RGrid rg = rays::make_rgrid(g);
     const int fix = set->fix_depth ? 1 : 0;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     cudaEventRecord(e0, s);
     // Observations (their tables as device pointers), their events, and the per-event state.
     std::vector<ObsD> oall(std::max(1, n_obs));
@@ -1108,8 +1107,6 @@ extern "C" int ts_locate(ts_ctx* ctx, ts_tables* tables, const ts_locator_settin
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     const double nan = std::nan("");
     for (int e = 0; e < n_events; e++) {
         const EvState& v = st[e];

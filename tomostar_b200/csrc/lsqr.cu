@@ -95,14 +95,9 @@ __global__ void reduce_partials(const double* __restrict__ partial, int count, d
 }
 
 __global__ void gather_values(int64_t nnz, const int* __restrict__ perm, const float* __restrict__ len,
-                              double* __restrict__ out) {
+                              float* __restrict__ out) {
     for (int64_t p = blockIdx.x * int64_t(kThreads) + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * kThreads)
-        out[p] = double(len[perm[p]]);
-}
-
-__global__ void widen(int64_t nnz, const float* __restrict__ len, double* __restrict__ out) {
-    for (int64_t p = blockIdx.x * int64_t(kThreads) + threadIdx.x; p < nnz; p += int64_t(gridDim.x) * kThreads)
-        out[p] = double(len[p]);
+        out[p] = len[perm[p]];
 }
 
 // ---- the transpose on the device, in the reference's order -------------------------------------
@@ -168,12 +163,27 @@ static void transpose_host(int m, int n, const int* rs, const int* ci, std::vect
         }
 }
 
+// A and its transpose on the device: values as FP64 (a host matrix), or as the float32 lengths a ray
+// call leaves (widened on load: the same FP64 products, a third less traffic per non-zero).
 struct System {
     int m = 0, n = 0;
     int64_t nnz = 0;
     const int *rs = nullptr, *ci = nullptr, *trs = nullptr, *tci = nullptr;
     const double *va = nullptr, *tva = nullptr;
+    const float *vaf = nullptr, *tvaf = nullptr;
 };
+
+// A·x or Aᵀ·x fused with the update, on whichever value type the system holds.
+static void spmv(const System& A, bool transpose, const double* x, double a, double* y, double* part,
+                 cudaStream_t s) {
+    const int rows = transpose ? A.n : A.m;
+    const int* rs = transpose ? A.trs : A.rs;
+    const int* ci = transpose ? A.tci : A.ci;
+    if (A.vaf)
+        spmv_update<float><<<kBlocks, kThreads, 0, s>>>(rows, rs, ci, transpose ? A.tvaf : A.vaf, x, a, y, part);
+    else
+        spmv_update<double><<<kBlocks, kThreads, 0, s>>>(rows, rs, ci, transpose ? A.tva : A.va, x, a, y, part);
+}
 
 // The LSQR iteration on a system already on the device (Lsqr.cs:50-150, term for term). Two reads
 // per iteration: ‖u‖² (with the ‖w‖² of the previous update) and ‖v‖².
@@ -197,17 +207,14 @@ static int run(ts_ctx* ctx, const System& A, const double* b, double damp, int m
         TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
         return TS_OK;
     };
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     cudaEventRecord(e0, s);
     auto finish = [&](int stop, int it, double bnorm, double rnorm, double acond) -> int {
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         TS_CUDA_TRY(ctx, cudaMemcpy(x_out, x, sizeof(double) * n, cudaMemcpyDeviceToHost));
         if (info) {
             info->iterations = it;
@@ -230,7 +237,7 @@ static int run(ts_ctx* ctx, const System& A, const double* b, double damp, int m
     scale<<<kBlocks, kThreads, 0, s>>>(m, u, 1.0 / beta);
     // α v = Aᵀ u (v starts at zero, so the update term vanishes)
     TS_CUDA_TRY(ctx, cudaMemsetAsync(v, 0, sizeof(double) * n, s));
-    spmv_update<double><<<kBlocks, kThreads, 0, s>>>(n, A.trs, A.tci, A.tva, u, 0.0, v, part);
+    spmv(A, true, u, 0.0, v, part, s);
     sum_to(part, 1);
     if (int rc = fetch(2)) return rc;
     double alpha = std::sqrt(hs[1]);
@@ -248,7 +255,7 @@ static int run(ts_ctx* ctx, const System& A, const double* b, double damp, int m
         iterations = it + 1;
         if (ctx->cancel_host && *ctx->cancel_host) return ctx->fail(TS_E_CANCELLED, "cancelled");
         // β u ← A v − α u
-        spmv_update<double><<<kBlocks, kThreads, 0, s>>>(m, A.rs, A.ci, A.va, v, alpha, u, part);
+        spmv(A, false, v, alpha, u, part, s);
         sum_to(part, 0);
         if (int rc = fetch(3)) return rc;
         beta = std::sqrt(hs[0]);
@@ -257,7 +264,7 @@ static int run(ts_ctx* ctx, const System& A, const double* b, double damp, int m
             scale<<<kBlocks, kThreads, 0, s>>>(m, u, 1.0 / beta);
             anorm2 += alpha * alpha + beta * beta + damp * damp;
             // α v ← Aᵀ u − β v
-            spmv_update<double><<<kBlocks, kThreads, 0, s>>>(n, A.trs, A.tci, A.tva, u, beta, v, part);
+            spmv(A, true, u, beta, v, part, s);
             sum_to(part, 1);
             if (int rc = fetch(2)) return rc;
             alpha = std::sqrt(hs[1]);
@@ -337,6 +344,7 @@ int ts_lsqr_solve(ts_ctx* ctx, int32_t m, int32_t n, const int32_t* row_ptr, con
     cudaStream_t s = ctx->stream;
     TS_BUF(ctx, d_rs, int, "lsqr.rs", m + 1);
     TS_BUF(ctx, d_ci, int, "lsqr.ci", std::max<int64_t>(1, nnz));
+    ctx->release("lsqr.tvaf");  // float values of earlier device rows are not needed here
     TS_BUF(ctx, d_va, double, "lsqr.va", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_trs, int, "lsqr.trs", n + 1);
     TS_BUF(ctx, d_tci, int, "lsqr.tci", std::max<int64_t>(1, nnz));
@@ -366,10 +374,11 @@ int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, d
     if (n <= 0 || m == 0 || !b || !x_out) return ctx->fail(TS_E_ARG, "empty system or null array");
     cudaStream_t s = ctx->stream;
     // The transpose built on the device in the reference's order; its values gathered there too.
-    TS_BUF(ctx, d_va, double, "lsqr.va", std::max<int64_t>(1, nnz));
+    ctx->release("lsqr.va");  // FP64 values of an earlier host matrix are not needed here
+    ctx->release("lsqr.tva");
     TS_BUF(ctx, d_trs, int, "lsqr.trs", n + 1);
     TS_BUF(ctx, d_tci, int, "lsqr.tci", std::max<int64_t>(1, nnz));
-    TS_BUF(ctx, d_tva, double, "lsqr.tva", std::max<int64_t>(1, nnz));
+    TS_BUF(ctx, d_tva, float, "lsqr.tvaf", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_perm, int, "lsqr.perm", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_trow, int, "lsqr.trow", std::max<int64_t>(1, nnz));
     TS_BUF(ctx, d_tsrc, int, "lsqr.tsrc", std::max<int64_t>(1, nnz));
@@ -390,7 +399,6 @@ int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, d
     TS_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(int) * n, s));
     scatter_columns<<<kBlocks * 8, kThreads, 0, s>>>(m, n, rs, ci, d_trs, d_cnt, d_trow, d_tsrc);
     order_columns<<<std::min(n, 262140), kThreads, 0, s>>>(n, d_trs, d_trow, d_tsrc, d_tci, d_perm);
-    widen<<<kBlocks * 4, kThreads, 0, s>>>(nnz, len, d_va);
     gather_values<<<kBlocks * 4, kThreads, 0, s>>>(nnz, d_perm, len, d_tva);
     TS_CUDA_TRY(ctx, cudaGetLastError());
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
@@ -398,7 +406,7 @@ int ts_lsqr_solve_rows(ts_ctx* ctx, ts_rows* rows, int32_t n, const double* b, d
     ctx->release("lsqr.trow");
     ctx->release("lsqr.tsrc");
     ctx->release("lsqr.cnt");
-    System A{m, n, nnz, rs, ci, d_trs, d_tci, d_va, d_tva};
+    System A{m, n, nnz, rs, ci, d_trs, d_tci, nullptr, nullptr, len, d_tva};
     return run(ctx, A, b, damp, max_iterations, atol, btol, conlim, x_out, info);
 }
 
