@@ -320,7 +320,7 @@ constexpr int kWarpCands = 8;
 constexpr int kBlockCands = kWarpCands * (kSearchThreads / 32);
 
 template <int E>
-__global__ void __launch_bounds__(kSearchThreads) search_warp_kernel(const SearchTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kSearchThreads, 4) search_warp_kernel(const SearchTask* __restrict__ tasks,
                                                                      int n_tasks, const int* __restrict__ off,
                                                                      const EvState* __restrict__ st,
                                                                      const ObsD* __restrict__ olist, int nx, int ny,
