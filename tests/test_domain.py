@@ -55,3 +55,16 @@ def test_background_model_known_answers():
     vp = 5.0 + np.arange(g.count) % 7 * 0.01
     bg = domain.Background.layer_mean(g, vp, vp / 1.73)
     assert len(bg.depth_km) == g.nz + 1 and bg.depth_km[-1] == 6370.0 and bg.vp[-1] == bg.vp[-2]
+
+
+def test_covering_across_the_antimeridian():
+    """Points east of 180° are unwrapped to the grid's side (GeoMath.UnwrapLon) before the box grows."""
+    from tomostar_b200.grid import GridDef
+
+    inv = GridDef(178.5, 179.5, -17.0, -16.0, 0.0, 20.0, 11, 11, 9)
+    pts = [[-179.6, -16.5, 5.0], [179.0, -16.2, 3.0]]
+    fwd, ext, fac = domain.covering(inv, 2, pts)
+    want, ext_o, fac_o = O.covering(O.Grid.of(inv), 2, pts)
+    assert (fwd.min_lon, fwd.max_lon, fwd.min_lat, fwd.max_lat, fwd.nx, fwd.ny, fwd.nz) == \
+        (want[0], want[1], want[2], want[3], want[6], want[7], want[8])
+    assert ext and fwd.max_lon > 180.0 and fwd.min_lon < inv.min_lon  # the margin applies on every side

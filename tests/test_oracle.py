@@ -264,3 +264,20 @@ def test_location_oracle_moves_events_towards_the_truth():
     assert out["rejected"].sum() > 0 and np.median(out["rms"]) < 0.05
     assert (out["used"] + out["rejected"] == np.diff(picks.offsets)).all()
     assert np.isfinite(res).all() and (out["gap_deg"] > 0).all() and (out["gap_deg"] <= 360).all()
+
+
+def test_location_oracle_fixed_depth_and_local_search():
+    """FixDepth keeps every event at its start depth (EventLocator.cs:140, 150-153, 184); a local
+    search (GlobalSearch off) from starts a few km off still moves the events towards the truth."""
+    job = syn.relocation_small()
+    g, tabs = _oracle_tables(job)
+    picks = syn.relocation_picks(job, tabs)
+    ts_ = np.ascontiguousarray(job.table_source[:, :2])
+    args = (job.start, picks.offsets, picks.table, picks.seconds, picks.weight, picks.correction)
+    fixed, _ = O.locate_many(g, tabs, ts_, O.LocatorSettings(fix_depth=1), *args)
+    assert (fixed["status"] == 0).all() and np.array_equal(fixed["depth_km"], job.start[:, 2])
+    assert (fixed["err_depth_km"] == 0).all()
+    local, _ = O.locate_many(g, tabs, ts_, O.LocatorSettings(global_search=0), *args)
+    before = syn.surface_distance_km(job.start[:, 0], job.start[:, 1], job.truth[:, 0], job.truth[:, 1])
+    after = syn.surface_distance_km(local["lon"], local["lat"], job.truth[:, 0], job.truth[:, 1])
+    assert (local["status"] == 0).all() and np.median(after) < 0.5 * np.median(before)

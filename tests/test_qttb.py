@@ -41,3 +41,13 @@ def test_model_key_composition():
     assert len(k) == 32 and k == k.upper()
     assert k == hashlib.sha256(s.astype("<f8").tobytes() + qttb.grid_json(job.grid)).hexdigest().upper()[:32]
     assert k != qttb.model_key(job.grid, job.slowness[1])
+
+
+def test_header_escapes_and_numbers():
+    """The default encoder's escapes (HTML-sensitive and non-ASCII characters as \\uXXXX, control
+    characters short) and .NET's number layout for negatives and exponents."""
+    g = GridDef(-1.0, 1.0, -1.0, 1.0, 0.0, 5.0, 3, 3, 3)
+    h = qttb.header_json('A"B<é>\n', "P", -0.000012, -1e16, 0.5, g).decode()
+    assert '"StationId": "A\\u0022B\\u003C\\u00E9\\u003E\\n"' in h
+    assert '"Lon": -1.2E-05' in h and '"Lat": -1E+16' in h and '"DepthKm": 0.5' in h
+    assert '"MinLon": -1' in h and '"Nz": 3\n  }' in h
