@@ -334,7 +334,8 @@ int ts_set_background(ts_ctx* ctx, const ts_background* bg);
 int ts_model_copy_slowness(ts_ctx* ctx, int32_t model_id, int32_t phase, double* out);
 
 /* ---- Travel-time tables kept on the device (TravelTimeTableSet, Forward/TravelTimeTable.cs:247-412) ----
- * n_tables float32 fields on one uniform grid, node-major per table as a .qttb file holds them. */
+ * n_tables float32 fields on one uniform grid, node-major per table as a .qttb file holds them. A table
+ * set belongs to the context that made it: free it (ts_tables_free) before ts_cuda_destroy. */
 typedef struct ts_tables ts_tables;
 /* TravelTimeTableSet.Build (:264-308): table t is the field of the source sources[3t..3t+2] (lon, lat,
  * depth km; seeds by PointSource, :373) for the slowness of phase source_phase[t] (slowness holds
