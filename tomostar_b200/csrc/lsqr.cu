@@ -38,6 +38,9 @@ __global__ void spmv_update(int rows, const int* __restrict__ rs, const int* __r
     double acc2 = 0.0;
     for (int i = gw; i < rows; i += nw) {
         double s = 0.0;
+        // Unrolled so that several gathers of x are in flight per lane; each lane still adds its
+        // terms in order.
+#pragma unroll 4
         for (int k = rs[i] + lane; k < rs[i + 1]; k += 32) s += double(va[k]) * x[ci[k]];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) {
