@@ -129,12 +129,13 @@ def max_over_ranks(dist, local, x: float) -> float:
     return float(t.item())
 
 
-def rank_problem(rank: int):
+def rank_problem(rank: int, dims=(401, 401, 121)):
     """Weak scaling with no collective on the data path: rank r solves its own job of the same shape
-    (the workload generated with seed 5 + r: its own stations, events and velocity bodies)."""
+    (the workload generated with seed 5 + r: its own stations, events and velocity bodies).
+    `dims` smaller than 401x401x121 is only for profiling captures that must stay small."""
     from tomostar_b200 import synthetic as syn
 
-    return syn.regional_401(seed=5 + rank)
+    return syn.regional_401(seed=5 + rank, dims=dims)
 
 
 def job_throughput(dist, local, world: int, fields_per_rank_step: int, steps: int, dev_ms: float):
@@ -581,11 +582,15 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-tile", type=int, default=2)
     ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
+    ap.add_argument("--dims", default="401,401,121",
+                    help="grid of the regional job (smaller only for profiling captures; the bench line is 401,401,121)")
     args = ap.parse_args()
+    dims = tuple(int(v) for v in args.dims.split(","))
+    problem_fn = lambda rank: rank_problem(rank, dims)  # noqa: E731
 
     if args.impl == "reference":
-        return run_reference(args, rank_problem)
-    return run_ours(args, rank_problem)
+        return run_reference(args, problem_fn)
+    return run_ours(args, problem_fn)
 
 
 if __name__ == "__main__":

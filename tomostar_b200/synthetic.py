@@ -150,22 +150,26 @@ def ellipsoid_bodies(grid: GridDef, h_km: float, rng, n: int = 3, amplitude: flo
     return out.reshape(-1)
 
 
-def regional_401(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000, seed: int = 5) -> Problem:
+def regional_401(n_stations: int = 400, n_events: int = 5000, n_rays: int = 1_500_000, seed: int = 5,
+                 dims: tuple = (401, 401, 121)) -> Problem:
     """401×401×121 at 0.25 km (19.46 M nodes): Vp = 5 + 0.04 z km/s plus three ellipsoidal ±8 % bodies,
     Vs = Vp / 1.73; 400 surface stations and 5,000 events (2–25 km deep) → 800 P and S fields;
     1.5 M (event, station, phase) arrivals drawn uniformly without replacement. One generator,
-    seed 5, in that order."""
+    seed 5, in that order. `dims` other than 401×401×121 gives the same model law on a smaller
+    grid (profiling captures that must stay a few GB on the device); events stay within its depth.
+    The grid stays square in x and y (stations and events are drawn over one span)."""
+    assert dims[0] == dims[1], "regional grids are square in x and y"
     h = 0.25
-    g = regular_grid(401, 401, 121, h)
+    g = regular_grid(*dims, h)
     rng = np.random.default_rng(seed)
     vp = vp_linear(g, 5.0, 0.04) * (1 + ellipsoid_bodies(g, h, rng))
     vs = vp / 1.73
-    span = 400 * h
+    span = (dims[0] - 1) * h
     sxy = rng.uniform(0, span, size=(n_stations, 2))
     slon, slat = km_to_geo(g, sxy[:, 0], sxy[:, 1], h)
     stations = np.stack([slon, slat, np.zeros(n_stations)], axis=1)
     exyz = np.column_stack([rng.uniform(0, span, n_events), rng.uniform(0, span, n_events),
-                            rng.uniform(2, 25, n_events)])
+                            rng.uniform(2, min(25.0, (dims[2] - 1) * h), n_events)])
     elon, elat = km_to_geo(g, exyz[:, 0], exyz[:, 1], h)
     events = np.stack([elon, elat, exyz[:, 2]], axis=1)
     pick = rng.choice(n_events * n_stations * 2, size=min(n_rays, n_events * n_stations * 2), replace=False)
