@@ -671,6 +671,74 @@ int32_t or_relax(const or_grid_def* d, const double* slowness, int32_t n_seeds, 
     return settled_all;
 }
 
+// One round of eight sweeps of one field (the body of Relax's round loop); true when a node dropped
+// from +inf or by more than tol.
+static bool relax_round(const Grid& g, const Metric& m, const double* slowness, double* out,
+                        const std::vector<uint8_t>& fixed, int phase, double tol) {
+    int nx = g.nx, ny = g.ny, nz = g.nz;
+    bool changed = false;
+    for (int dir = 0; dir < 8; dir++)
+        for (int p = 0; p < nx + ny + nz - 2; p++) {
+            int i0, i1, k0, k1;
+            plane_bounds(nx, ny, nz, p, i0, i1, k0, k1);
+            for (int kp = k0; kp <= k1; kp++)
+                for (int ip = i0; ip <= i1; ip++) {
+                    int jp = p - ip - kp;
+                    if (jp < 0 || jp >= ny) continue;
+                    int i = (dir & 1) ? nx - 1 - ip : ip;
+                    int j = (dir & 2) ? ny - 1 - jp : jp;
+                    int k = (dir & 4) ? nz - 1 - kp : kp;
+                    int idx = g.index(i, j, k);
+                    if (fixed[idx]) continue;
+                    double cur = out[idx];
+                    double cand = relax_node(m, slowness, out, idx, i, j, k, phase == 1);
+                    if (!(cand < cur)) continue;
+                    out[idx] = cand;
+                    if (!std::isfinite(cur) || cur - cand > tol) changed = true;
+                }
+        }
+    return changed;
+}
+
+// A batch of fields on one slowness as EikonalOpenCl.Sweep solves it (EikonalOpenCl.cs:215-270): one
+// `changed` flag for the whole batch, so every field is swept until no field of the batch moved by
+// more than tol in a round, and the batch enters phase 1 together. A field that settled early keeps
+// being swept, which can move it below tol: its bits may differ from a solve on its own (Relax, and
+// the per-field settling of the CUDA engine) by a few ulps. Seeds of field e are
+// seed_idx/seed_t[seed_off[e] .. seed_off[e+1]); out is field-major. Returns 1 when settled.
+int32_t or_relax_batch(const or_grid_def* d, const double* slowness, int32_t batch, const int32_t* seed_off,
+                       const int32_t* seed_idx, const double* seed_t, int32_t max_rounds, double tol, double* out,
+                       int32_t* rounds_out) {
+    Grid g(*d);
+    Metric m(g);
+    const int n = g.count();
+    std::vector<std::vector<uint8_t>> fixed(batch, std::vector<uint8_t>(n, 0));
+    for (int e = 0; e < batch; e++) {
+        double* f = out + int64_t(e) * n;
+        std::fill(f, f + n, kInf);
+        for (int q = seed_off[e]; q < seed_off[e + 1]; q++) {
+            int s = seed_idx[q];
+            if (unsigned(s) >= unsigned(n)) continue;
+            f[s] = std::min(f[s], seed_t[q]);
+            fixed[e][s] = 1;
+        }
+    }
+    const int cap = max_rounds > 0 ? max_rounds : sweep_round_cap(g);
+    for (int phase = 0; phase < 2; phase++) {
+        bool settled = false;
+        int round = 0;
+        for (round = 0; round < cap && !settled; round++) {
+            bool changed = false;
+            for (int e = 0; e < batch; e++)
+                if (relax_round(g, m, slowness, out + int64_t(e) * n, fixed[e], phase, tol)) changed = true;
+            settled = !changed;
+        }
+        if (rounds_out) rounds_out[phase] = round;
+        if (!settled) return 0;
+    }
+    return 1;
+}
+
 // SphericalEikonal.Solve (SphericalEikonal.cs:102-152): fast marching, the reference's production CPU
 // solver (and the timed CPU baseline). Seeds are imposed; neighbours are updated from Alive nodes only.
 int32_t or_fmm(const or_grid_def* d, const double* slowness, int32_t n_seeds, const int32_t* seed_idx,
@@ -1050,6 +1118,32 @@ static void csr_mul(int32_t rows, const int32_t* rs, const int32_t* ci, const do
         for (int32_t k = rs[i]; k < rs[i + 1]; k++) s += va[k] * x[ci[k]];
         y[i] = s;
     }
+}
+
+// The products or_lsqr forms (CsrMatrix.MultiplyInto, SparseMatrix.cs:55-72: one sequential sum per
+// row), exported for the comparison with the reference's own spmv kernel (LsqrOpenCl.cs:45-53).
+void or_csr_mul(int32_t rows, const int32_t* rs, const int32_t* ci, const double* va, const double* x, double* y) {
+    for (int32_t i = 0; i < rows; i++) {
+        double s = 0;
+        for (int32_t k = rs[i]; k < rs[i + 1]; k++) s += va[k] * x[ci[k]];
+        y[i] = s;
+    }
+}
+
+// CsrMatrix.Transpose (SparseMatrix.cs:79-96) as or_lsqr builds it: a stable counting sort by column.
+void or_csr_transpose(int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                      int32_t* trs, int32_t* tci, double* tva) {
+    const int64_t nnz = row_ptr[m];
+    for (int32_t c = 0; c <= n; c++) trs[c] = 0;
+    for (int64_t k = 0; k < nnz; k++) trs[col[k] + 1]++;
+    for (int32_t c = 0; c < n; c++) trs[c + 1] += trs[c];
+    std::vector<int32_t> next(trs, trs + n);
+    for (int32_t i = 0; i < m; i++)
+        for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; k++) {
+            int32_t p = next[col[k]]++;
+            tci[p] = i;
+            tva[p] = val[k];
+        }
 }
 
 int32_t or_lsqr(int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val, const double* b,

@@ -2,9 +2,11 @@
 
 The oracle restates the reference's CPU solvers (Forward/SphericalEikonal.cs, Forward/RayTracing.cs,
 Forward/TravelTimeTable.cs, Tomography/RayKernels.cs) and the callers beside them (Numerics/Lsqr.cs,
-Location/EventLocator.cs, Forward/ForwardDomain.cs). Parity status: pinned by the reference's own
-known-answer tests and, for LSQR, by SciPy's lsqr; not by bitwise reference output (the reference is
-C#/.NET and cannot run here).
+Location/EventLocator.cs, Forward/ForwardDomain.cs). Parity status: the sweeping solver (or_relax,
+or_relax_batch) and the LSQR products are pinned bit for bit to the reference's own device kernels
+compiled for the CPU (oracle/ref.py, tests/test_ref_pin.py); fast marching, rays and location by the
+reference's known-answer tests, LSQR also by SciPy's lsqr. The C# host code itself cannot run here
+(no .NET).
 """
 from __future__ import annotations
 
@@ -73,6 +75,9 @@ def lib():
             "or_ray_rows_many": (None, [g, fp, ip, dp, g, dp, i32, d, i32, ip, ip, fp, dp, i32]),
             "or_relax_wake": (i32, [g, dp, i32, ip, dp, d, d, i32, dp, ip, P(C.c_int64)]),
             "or_lsqr": (i32, [i32, i32, ip, ip, dp, dp, d, i32, d, d, d, dp, dp]),
+            "or_csr_mul": (None, [i32, ip, ip, dp, dp, dp]),
+            "or_relax_batch": (i32, [g, dp, i32, ip, ip, dp, i32, d, dp, ip]),
+            "or_csr_transpose": (None, [i32, i32, ip, ip, dp, ip, ip, dp]),
             "or_locate_many": (None, [g, fp, i32, dp, C.c_void_p, i32, dp, ip, ip, dp, dp, dp, i32, C.c_void_p,
                                       dp]),
             "or_weighted_median": (d, [i32, dp, dp]),
@@ -181,6 +186,18 @@ def relax(g: Grid, slowness, seed_idx, seed_t, tol=1e-7, max_rounds=0):
     rounds = np.zeros(2, np.int32)
     ok = lib().or_relax(g.ref, _p(s, C.c_double), len(si), _p(si, C.c_int32), _p(st, C.c_double), max_rounds, tol,
                         _p(out, C.c_double), _p(rounds, C.c_int32))
+    return out, bool(ok), rounds
+
+
+def relax_batch(g: Grid, slowness, seed_sets, tol=1e-7, max_rounds=0):
+    """A batch on one slowness as EikonalOpenCl.Sweep solves it: one round flag for the whole batch.
+    Returns (fields (batch, n), settled, rounds[2])."""
+    s = np.ascontiguousarray(slowness, np.float64)
+    off, idx, t = _seed_arrays(seed_sets)
+    out = np.empty((len(seed_sets), g.count))
+    rounds = np.zeros(2, np.int32)
+    ok = lib().or_relax_batch(g.ref, _p(s, C.c_double), len(seed_sets), _p(off, C.c_int32), _p(idx, C.c_int32),
+                              _p(t, C.c_double), max_rounds, tol, _p(out, C.c_double), _p(rounds, C.c_int32))
     return out, bool(ok), rounds
 
 
@@ -346,6 +363,31 @@ def lsqr(m, n, row_ptr, col, val, b, damp=0.0, max_iterations=500, atol=1e-8, bt
     code = lib().or_lsqr(m, n, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(va, C.c_double), _p(bb, C.c_double), damp,
                          max_iterations, atol, btol, conlim, _p(x, C.c_double), _p(info, C.c_double))
     return x, int(code), {"iterations": int(info[0]), "bnorm": info[1], "rnorm": info[2], "acond": info[3]}
+
+
+def csr_mul(row_ptr, col, val, x):
+    """The product or_lsqr forms (CsrMatrix.MultiplyInto: one sequential sum per row)."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col, np.int32)
+    va = np.ascontiguousarray(val, np.float64)
+    xv = np.ascontiguousarray(x, np.float64)
+    y = np.empty(len(rp) - 1)
+    lib().or_csr_mul(len(rp) - 1, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(va, C.c_double), _p(xv, C.c_double),
+                     _p(y, C.c_double))
+    return y
+
+
+def csr_transpose(m, n, row_ptr, col, val):
+    """CsrMatrix.Transpose as or_lsqr builds it: (row_ptr, col, val) of Aᵀ."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col, np.int32)
+    va = np.ascontiguousarray(val, np.float64)
+    trs = np.empty(n + 1, np.int32)
+    tci = np.empty(len(ci), np.int32)
+    tva = np.empty(len(ci))
+    lib().or_csr_transpose(m, n, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(va, C.c_double), _p(trs, C.c_int32),
+                           _p(tci, C.c_int32), _p(tva, C.c_double))
+    return trs, tci, tva
 
 
 class LocatorSettings(C.Structure):
