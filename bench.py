@@ -461,16 +461,27 @@ def run_ours(args, problem_fn):
         ar = np.ascontiguousarray(p.arrivals, np.int32)
         ae, ast, aph = (np.ascontiguousarray(ar[:, q]) for q in range(3))
         fstats = L.EikStats()
-        h = C.c_void_p()
-        t0 = time.perf_counter()
-        rc = lib.ts_forward(fsolver.handle, C.byref(fs), s_all.ctypes.data_as(P(C.c_double)), len(s_all),
-                            C.byref(is_), len(st), st.ctypes.data_as(P(C.c_double)), len(ev),
-                            ev.ctypes.data_as(P(C.c_double)), len(ar), ae.ctypes.data_as(P(C.c_int32)),
-                            ast.ctypes.data_as(P(C.c_int32)), aph.ctypes.data_as(P(C.c_int32)), 64, 0.0,
-                            C.byref(h), C.byref(fstats))
-        fwd_s = time.perf_counter() - t0
-        if rc:
-            raise SystemExit(f"forward step failed: {fsolver.last_error}")
+
+        def forward_call(mode):
+            hh = C.c_void_p()
+            t = time.perf_counter()
+            rc = lib.ts_forward(fsolver.handle, C.byref(fs), s_all.ctypes.data_as(P(C.c_double)), len(s_all),
+                                C.byref(is_), len(st), st.ctypes.data_as(P(C.c_double)), len(ev),
+                                ev.ctypes.data_as(P(C.c_double)), len(ar), ae.ctypes.data_as(P(C.c_int32)),
+                                ast.ctypes.data_as(P(C.c_int32)), aph.ctypes.data_as(P(C.c_int32)), 64, mode, 0.0,
+                                C.byref(hh), C.byref(fstats))
+            if rc:
+                raise SystemExit(f"forward step failed: {fsolver.last_error}")
+            return hh, time.perf_counter() - t
+
+        # The bitwise mode first (its tables only are reported), then the default fast mode.
+        exact = None
+        if not args.no_forward_exact:
+            hx, fwd_x = forward_call(L.MODE_ENGINE)
+            exact = {"mode": "engine (the reference's fields to the bit)", "wall_s": fwd_x,
+                     "tables_s": fstats.device_ms / 1e3, "node_updates": int(fstats.node_updates)}
+            lib.ts_rows_free(hx)
+        h, fwd_s = forward_call(args.mode)
         fields_s = fstats.device_ms / 1e3
         # LSQR (Lsqr.Solve) on the rows where they lie: 100 iterations, no early stop (fixed work).
         b = np.random.default_rng(11).standard_normal(len(ar)) * 0.05
@@ -494,7 +505,9 @@ def run_ours(args, problem_fn):
                    "rays_and_copy_s": fwd_s - fields_s + copy_s,
                    "rays_rows_per_s": n_rows / max(1e-9, fwd_s - fields_s + copy_s), "nnz": nnz,
                    "nnz_per_row": nnz / max(1, int(rows.ok.sum())), "kept_rows": int(rows.ok.sum()),
-                   "mode": "engine (bitwise) tables, float32, rays FP64",
+                   "mode": ("fast" if args.mode == L.MODE_FAST else "engine (bitwise)") +
+                           " tables (FP64 fields as float32), rays FP64",
+                   "exact_mode": exact,
                    "lsqr": {"iterations": lres.iterations, "columns": p.inv.count, "damp": 0.1,
                             "wall_s": lsqr_wall, "device_ms": lres.device_ms, "ms_per_iteration": it_ms,
                             "achieved_gbs": lsqr_gbs, "hbm_frac": lsqr_gbs / peak,
@@ -575,6 +588,7 @@ def main():
     ap.add_argument("--scheduler", type=int, default=0, help="0 lockstep diagonals, 1 flow (per field)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-load measurement")
     ap.add_argument("--no-forward", action="store_true", help="skip the forward step (tables + rays)")
+    ap.add_argument("--no-forward-exact", action="store_true", help="skip the bitwise-mode forward step")
     ap.add_argument("--no-location", action="store_true", help="skip the relocation measurement")
     ap.add_argument("--location-events", type=int, default=4000)
     ap.add_argument("--location-cpu-events", type=int, default=256, help="events the CPU baseline locates")

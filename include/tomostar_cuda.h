@@ -262,11 +262,13 @@ int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float
  * seeded by PointSource at the station and rounded to float32 as TravelTimeTable.Write does, then
  * every arrival traced on its table. slowness: n_phases fields on fwd (ForwardModel, phase p at
  * p*n). stations/events: 3 doubles each. Arrival a: (arr_event[a], arr_station[a], arr_phase[a]).
- * step_km <= 0 uses the RayKernels step. */
+ * mode: TS_MODE_FAST (the recommended default: fields within 1e-10 relative of the reference's, about
+ * half the work) or TS_MODE_ENGINE (the reference's fields to the bit). step_km <= 0 uses the
+ * RayKernels step. */
 int ts_forward(ts_ctx* ctx, const ts_grid* fwd, const double* slowness, int32_t n_phases, const ts_grid* inv,
                int32_t n_stations, const double* stations, int32_t n_events, const double* events,
                int32_t n_arrivals, const int32_t* arr_event, const int32_t* arr_station, const int32_t* arr_phase,
-               int32_t precision, double step_km, ts_rows** out, ts_eik_stats* stats);
+               int32_t precision, int32_t mode, double step_km, ts_rows** out, ts_eik_stats* stats);
 
 /* ---- LSQR on the device (Numerics/Lsqr.cs:33-152, LsqrOpenCl.cs) ----
  * Damped LSQR, min ‖A x − b‖² + damp² ‖x‖², with the reference's stopping rules (atol, btol,

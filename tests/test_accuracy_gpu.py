@@ -5,7 +5,8 @@ the largest absolute error in seconds.
 * FP64 engine (exact rule): equal to the oracle's Relax (0).
 * FP64 fast mode, delivered as float32 tables (the headline): within 2e-5 relative (in fact the
   float32 rounding, ~6e-8).
-* FP32 arithmetic: p99 within 2e-5; single nodes on promotion flips may exceed it (bounded 2e-4).
+* FP32 arithmetic (the reference's paired-float scheme, times as hi + lo floats): within 2e-5
+  relative at every node (measured: a few 1e-6 at most).
 """
 import numpy as np
 import pytest
@@ -49,7 +50,7 @@ def check(solver, name, cases):
     r = dict(rows)
     assert r["fp64 engine"][0] == 0.0
     assert r["fp64 fast -> float32 tables"][0] <= 2e-5
-    assert r["fp32 arithmetic"][1] <= 2e-5 and r["fp32 arithmetic"][0] <= 2e-4
+    assert r["fp32 arithmetic"][0] <= 2e-5
 
 
 def test_accuracy_single_source_61(solver):
@@ -83,4 +84,4 @@ def test_accuracy_regional_401_one_field(solver):
     rows = [("fp64 fast -> float32 tables", errors(tables, ref)), ("fp32 arithmetic", errors(f32, ref))]
     report("401x401x121 at 0.25 km (one P field)", rows)
     assert rows[0][1][0] <= 2e-5
-    assert rows[1][1][1] <= 2e-5 and rows[1][1][0] <= 2e-4
+    assert rows[1][1][0] <= 2e-5

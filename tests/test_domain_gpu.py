@@ -93,7 +93,8 @@ def test_forward_step_extended_domain_outside_time(solver):
                         np.int32)
     domain.set_background(solver, bg)
     try:
-        gpu = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64)
+        gpu = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64,
+                                                   mode=L.MODE_ENGINE)
     finally:
         domain.set_background(solver, None)
     og = O.Grid.of(fwd)
@@ -115,5 +116,6 @@ def test_forward_step_extended_domain_outside_time(solver):
     assert (outside[ok] > 0).sum() >= 10 and (outside[ok] == 0).sum() >= 10
     assert np.max(np.abs(gpu.outside[ok] - outside[ok])) <= 1e-9 * max(1.0, float(outside.max()))
     # Without the background the same rays keep every piece (outside time 0).
-    plain = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64)
+    plain = RayKernels(inv, fwd, solver).compute(slow, stations, events, arrivals, precision=64,
+                                                 mode=L.MODE_ENGINE)
     assert not plain.outside.any() and plain.nnz > gpu.nnz

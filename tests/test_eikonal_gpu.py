@@ -145,10 +145,9 @@ def test_f64_tables_inversion_step_121_subset(solver):
 
 
 def test_f32_compute_error_profile_inversion_step_121(solver):
-    """FP32 arithmetic and float32 storage: the error against the FP64 oracle is float rounding
-    (p99 under 2e-6) except along the lines of nodes where two neighbour times differ by about one
-    float ulp and the reference's second-order promotion test (t2 <= first, SphericalEikonal.cs:391)
-    flips; those reach a few 1e-5 relative. This mode is the fast option, not the headline."""
+    """FP32 arithmetic (the reference's paired-float scheme: times as hi + lo floats, the update in
+    float offsets from the smallest upwind neighbour): within 2e-5 relative of the FP64 oracle at
+    every node, p99 near the float32 table rounding."""
     p = syn.inversion_step_121()
     for ph in (0, 1):
         seeds = [point_source(p.grid, p.slowness[ph], *p.stations[q]) for q in (0, 7, 19)]
@@ -157,8 +156,8 @@ def test_f32_compute_error_profile_inversion_step_121(solver):
         for f in range(3):
             fin = np.isfinite(ref[f])
             rel = np.abs(out[f][fin] - ref[f][fin]) / np.maximum(ref[f][fin], 1e-9)
-            assert np.percentile(rel, 99) <= 2e-6, (ph, f)
-            assert rel.max() <= 2e-4, (ph, f, rel.max())
+            assert np.percentile(rel, 99) <= 2e-7, (ph, f)
+            assert rel.max() <= F32_REL_TOL, (ph, f, rel.max())
 
 
 def test_f32_output_float32(solver):

@@ -95,7 +95,7 @@ def test_lsqr_on_device_resident_rays(solver):
     rc = lib.ts_forward(solver.handle, C.byref(fs), s.ctypes.data_as(P(C.c_double)), len(s), C.byref(is_), len(st),
                         st.ctypes.data_as(P(C.c_double)), len(ev), ev.ctypes.data_as(P(C.c_double)), len(ar),
                         ae.ctypes.data_as(P(C.c_int32)), ast.ctypes.data_as(P(C.c_int32)),
-                        ap.ctypes.data_as(P(C.c_int32)), 64, 0.0, C.byref(h), C.byref(stats))
+                        ap.ctypes.data_as(P(C.c_int32)), 64, L.MODE_ENGINE, 0.0, C.byref(h), C.byref(stats))
     assert rc == 0, solver.last_error
     n = p.inv.count
     b = np.random.default_rng(9).standard_normal(len(ar)) * 0.05

@@ -107,8 +107,8 @@ def test_multi_grid_fp32_within_tolerance(solver, batch):
         fin = np.isfinite(ref)
         assert np.array_equal(fin, np.isfinite(fields[q]))
         worst = max(worst, float(np.max(np.abs(fields[q][fin] - ref[fin]) / np.maximum(ref[fin], 1e-9))))
-    # FP32 arithmetic: most nodes within 2e-5; promotion flips at valley lines may exceed it locally.
-    assert worst <= 2e-4, worst
+    # FP32 arithmetic (paired floats): within 2e-5 at every node, variable depth spacing included.
+    assert worst <= F32_REL_TOL, worst
 
 
 def test_graph_replay_repeats_the_job(solver, batch):

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from tomostar_b200 import _lib as L
 from tomostar_b200 import synthetic as syn
 from tomostar_b200.eikonal import point_source
 from tomostar_b200.rays import RayKernels, trace_rows
@@ -119,7 +120,7 @@ def test_forward_step_single_source_61_f64(solver):
     """RayKernels.Compute on the device (tables + rays) against the oracle pipeline, FP64."""
     p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
-    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64)
+    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64, mode=L.MODE_ENGINE)
     nnz, nodes, lens, tg = O.ray_rows_many(O.Grid.of(p.grid), tb[None, :], np.zeros(25, np.int32),
                                            np.repeat(p.stations, 25, axis=0), O.Grid.of(p.inv), p.events, p.step_km)
     compare_rows(gpu, nnz, nodes, lens, tg)
@@ -131,7 +132,7 @@ def test_forward_step_f32_close(solver):
     """The FP32 forward step: rows close to the FP64 oracle's (tables differ by the FP32 error)."""
     p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
-    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=32)
+    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=32, mode=L.MODE_ENGINE)
     nnz, nodes, lens, tg = O.ray_rows_many(O.Grid.of(p.grid), tb[None, :], np.zeros(25, np.int32),
                                            np.repeat(p.stations, 25, axis=0), O.Grid.of(p.inv), p.events, p.step_km)
     assert np.array_equal(gpu.ok, nnz >= 0)
@@ -145,7 +146,7 @@ def test_row_time_consistency(solver):
     """Σ length·slowness of each row is close to TCalc (the reference's 'rays' validation, <5 %)."""
     p, tb = single_source_61_tables()
     rk = RayKernels(p.inv, p.grid, solver)
-    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64)
+    gpu = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=64, mode=L.MODE_ENGINE)
     s_inv = p.slowness[0].reshape(p.grid.shape)[::2, ::2, ::2].reshape(-1)  # inversion nodes are every other
     for row in gpu.rows():
         kt = float(np.sum(row.length * s_inv[row.nodes]))

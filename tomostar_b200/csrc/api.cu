@@ -104,7 +104,8 @@ void ts_set_cancel(ts_ctx* ctx, int32_t cancel) {
 
 int32_t ts_eik_suggest_batch(ts_ctx* ctx, int64_t nodes, int32_t precision) {
     if (!ctx || nodes <= 0) return 0;
-    const int64_t real = precision == TS_PRECISION_F64 ? 8 : 4;
+    const int64_t real = 8;  // a double, or the FP32 precision's float pair (EikonalOpenCl.Real)
+    (void)precision;
     size_t free_b = 0, total_b = 0;
     cudaSetDevice(ctx->device);
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {

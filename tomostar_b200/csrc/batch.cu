@@ -19,7 +19,7 @@ static int solve_multi_impl(ts_ctx* ctx, int n_grids, const ts_grid* grids, cons
                             int n_fields, const int32_t* field_grid, const int32_t* seed_offsets,
                             const int32_t* seed_index, const double* seed_time, int mode, double tol, int max_rounds,
                             void* out, int out_type, ts_eik_stats* stats) {
-    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    const int precision = precision_of<Real>();
     std::vector<std::unique_ptr<host::Grid>> g(n_grids);
     std::vector<std::unique_ptr<host::Metric>> m(n_grids);
     EngineJob job;
@@ -129,7 +129,7 @@ int ts_eik_solve_multi(ts_ctx* ctx, int32_t n_grids, const ts_grid* grids, const
         return ts::eik::solve_multi_impl<double>(ctx, n_grids, grids, slowness, n_fields, field_grid, seed_offsets,
                                                  seed_index, seed_time, mode, tol, max_rounds, out, out_type, stats);
     if (precision == TS_PRECISION_F32)
-        return ts::eik::solve_multi_impl<float>(ctx, n_grids, grids, slowness, n_fields, field_grid, seed_offsets,
+        return ts::eik::solve_multi_impl<ts::Pair>(ctx, n_grids, grids, slowness, n_fields, field_grid, seed_offsets,
                                                 seed_index, seed_time, mode, tol, max_rounds, out, out_type, stats);
     return ctx->fail(TS_E_ARG, "precision must be 64 or 32");
 }

@@ -194,7 +194,7 @@ int ts_model_put_resampled(ts_ctx* ctx, const ts_grid* forward, const ts_grid* i
     m->n_phases = n_phases;
     const host::Grid ig(*inversion);
     const int64_t fn = m->grid->count(), in = ig.count();
-    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t esz = 8;  // a double, or the float pair of the FP32 precision
     if (cudaMalloc(&m->slowness, size_t(fn) * n_phases * esz) != cudaSuccess) {
         cudaGetLastError();
         m->slowness = nullptr;
@@ -226,8 +226,8 @@ int ts_model_put_resampled(ts_ctx* ctx, const ts_grid* forward, const ts_grid* i
             domain::resample_kernel<double><<<blocks, 256, 0, s>>>(fg, rg, s_d, in, n_phases, nbg, bg_d, bg_d + nbg,
                                                                    static_cast<double*>(m->slowness));
         else
-            domain::resample_kernel<float><<<blocks, 256, 0, s>>>(fg, rg, s_d, in, n_phases, nbg, bg_d, bg_d + nbg,
-                                                                  static_cast<float*>(m->slowness));
+            domain::resample_kernel<Pair><<<blocks, 256, 0, s>>>(fg, rg, s_d, in, n_phases, nbg, bg_d, bg_d + nbg,
+                                                                 static_cast<Pair*>(m->slowness));
         if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) rc = TS_E_CUDA;
     }
     if (rc) {
@@ -251,10 +251,11 @@ int ts_model_copy_slowness(ts_ctx* ctx, int32_t model_id, int32_t phase, double*
     if (m->precision == TS_PRECISION_F64) {
         TS_CUDA_TRY(ctx, cudaMemcpy(out, static_cast<double*>(m->slowness) + n * phase, n * 8, cudaMemcpyDeviceToHost));
     } else {
-        std::vector<float> tmp(n);
-        TS_CUDA_TRY(ctx, cudaMemcpy(tmp.data(), static_cast<float*>(m->slowness) + n * phase, n * 4,
+        // The FP32 precision's slowness is the float the paired kernel reads (the pair's hi).
+        std::vector<Pair> tmp(n);
+        TS_CUDA_TRY(ctx, cudaMemcpy(tmp.data(), static_cast<Pair*>(m->slowness) + n * phase, n * sizeof(Pair),
                                     cudaMemcpyDeviceToHost));
-        for (size_t q = 0; q < n; q++) out[q] = tmp[q];
+        for (size_t q = 0; q < n; q++) out[q] = tmp[q].hi;
     }
     return TS_OK;
 }

@@ -78,7 +78,7 @@ __global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_s
     for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < rows * nx; q += int64_t(gridDim.x) * blockDim.x) {
         int64_t r = q / nx;
         From v = src[r * pitch + xoff + (q - r * nx)];
-        dst[q] = isfinite(v) ? To(v) : To(__int_as_float(0x7f800000));
+        dst[q] = finite_r(v) ? To(v) : To(__int_as_float(0x7f800000));
     }
 }
 
@@ -122,9 +122,9 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
             for (int b = 0; b < ty[gi]; b++)
                 for (int a = 0; a < tx[gi]; a++) dt[pos[a + b + c]++] = uint32_t(a) | (uint32_t(b) << 10) | (uint32_t(c) << 20);
         o_wx[gi] = A.add(sizeof(Real) * m.wx.size());
-        for (size_t q = 0; q < m.wx.size(); q++) A.at<Real>(o_wx[gi])[q] = Real(m.wx[q]);
+        for (size_t q = 0; q < m.wx.size(); q++) A.at<Real>(o_wx[gi])[q] = Real(weight_of<Real>(m.wx[q], m.wx32[q]));
         o_wy[gi] = A.add(sizeof(Real) * m.wy.size());
-        for (size_t q = 0; q < m.wy.size(); q++) A.at<Real>(o_wy[gi])[q] = Real(m.wy[q]);
+        for (size_t q = 0; q < m.wy.size(); q++) A.at<Real>(o_wy[gi])[q] = Real(weight_of<Real>(m.wy[q], m.wy32[q]));
         o_zc[gi] = A.add(sizeof(Real) * std::max<size_t>(1, m.zc.size()));
         for (size_t q = 0; q < m.zc.size(); q++) A.at<Real>(o_zc[gi])[q] = Real(m.zc[q]);
     }
@@ -302,8 +302,8 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
         gd.wx = D + o_wx[gi];
         gd.wy = D + o_wy[gi];
         gd.zc = D + o_zc[gi];
-        gd.wz1 = metrics[gi]->wz1;
-        gd.wz2 = metrics[gi]->wz2;
+        gd.wz1 = weight_of<Real>(metrics[gi]->wz1, metrics[gi]->wz1_32);
+        gd.wz2 = weight_of<Real>(metrics[gi]->wz2, metrics[gi]->wz2_32);
         gd.pitch = Layout<Real>::pitch(tx[gi], BX);
         A.at<GridDesc>(o_grids)[gi] = gd;
     }
@@ -489,27 +489,31 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
 // Fields of the job in dense grid order: same precision → strided copies; otherwise converted on the
 // device in blocks of fields, then copied.
 int fields_to_dense_host(ts_ctx* ctx, const EngineJob& job, int precision, void* out, int out_type) {
-    const size_t rsz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t rsz = 8;  // a double, or the FP32 precision's float pair
     const size_t osz = out_type == TS_OUT_F64 ? 8 : 4;
+    const bool same = precision == TS_PRECISION_F64 && out_type == TS_OUT_F64;
     char* dst = static_cast<char*>(out);
     for (size_t f = 0; f < job.fields.size(); f++) {
         const host::Grid& g = *job.grids[job.fields[f].grid];
         const int pitch = job.pitch[job.fields[f].grid];
         const int64_t rows = int64_t(g.ny) * g.nz, n = rows * g.nx;
         const char* src = static_cast<const char*>(job.fields[f].T);
-        if (rsz == osz) {
+        if (same) {
             TS_CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, g.nx * osz, src + job.xoff * rsz, pitch * rsz, g.nx * rsz, rows,
                                                cudaMemcpyDeviceToHost, ctx->stream));
         } else {
             void* stage = ctx->buf("out.stage", size_t(n) * osz);
             if (!stage) return TS_E_NOMEM;
             int blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
-            if (rsz == 8)
+            if (precision == TS_PRECISION_F64)
                 dense_convert_kernel<double, float><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
                     reinterpret_cast<const double*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<float*>(stage));
+            else if (osz == 8)
+                dense_convert_kernel<Pair, double><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
+                    reinterpret_cast<const Pair*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<double*>(stage));
             else
-                dense_convert_kernel<float, double><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
-                    reinterpret_cast<const float*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<double*>(stage));
+                dense_convert_kernel<Pair, float><<<dim3(blocks, 1), 256, 0, ctx->stream>>>(
+                    reinterpret_cast<const Pair*>(src), 0, pitch, job.xoff, g.nx, rows, static_cast<float*>(stage));
             TS_CUDA_TRY(ctx, cudaGetLastError());
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(dst, stage, size_t(n) * osz, cudaMemcpyDeviceToHost, ctx->stream));
             TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -529,8 +533,8 @@ int field_to_dense_f32_device(ts_ctx* ctx, const host::Grid& g, const FieldLayou
         dense_convert_kernel<double, float><<<dim3(blocks, 1), 256, 0, s>>>(static_cast<const double*>(T), 0, L.pitch,
                                                                             L.xoff, g.nx, rows, out);
     else
-        dense_convert_kernel<float, float><<<dim3(blocks, 1), 256, 0, s>>>(static_cast<const float*>(T), 0, L.pitch,
-                                                                           L.xoff, g.nx, rows, out);
+        dense_convert_kernel<Pair, float><<<dim3(blocks, 1), 256, 0, s>>>(static_cast<const Pair*>(T), 0, L.pitch,
+                                                                          L.xoff, g.nx, rows, out);
     TS_CUDA_TRY(ctx, cudaGetLastError());
     return TS_OK;
 }
@@ -553,7 +557,7 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
                  double tol, double wake_rel, int tile, int max_rounds, ts_eik_stats* stats, cudaStream_t s) {
     if (fields.empty()) return TS_OK;
     // Warps per block sized so that two or three blocks fill an SM's shared memory.
-    constexpr bool F64 = sizeof(Real) == 8;
+    constexpr bool F64 = sizeof(Real) == 8;  // 8-byte values: shared memory as FP64 (Pair too)
     switch (tile) {
         case 1: return launch_epoch<Real, 16, 8, 4, F64 ? 5 : 8, 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 2: return launch_epoch<Real, 8, 8, 4, F64 ? 6 : 8, F64 ? 3 : 2>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
@@ -569,7 +573,8 @@ FieldLayout field_layout(const host::Grid& g, int tile, int precision) {
     int bx = 8, by = 8, bz = 8;
     for (const auto& t : tile_shapes())
         if (t.id == tile) { bx = t.bx; by = t.by; bz = t.bz; }
-    const int hx = precision == TS_PRECISION_F64 ? 2 : 4;
+    const int hx = 2;  // 16 bytes of 8-byte values (a double, or the FP32 precision's float pair)
+    (void)precision;
     const int tx = (g.nx + bx - 1) / bx, ty = (g.ny + by - 1) / by, tz = (g.nz + bz - 1) / bz;
     FieldLayout L;
     L.pitch = hx + tx * bx + hx;
@@ -585,12 +590,14 @@ int64_t FieldLayout::elems() const { return int64_t(pitch) * rows_; }
 static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 
 int64_t FieldLayout::bytes(int precision) const {
-    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t esz = 8;
+    (void)precision;
     return int64_t(up256(size_t(elems()) * esz) + up256(size_t(tiles)) + up256(4 * size_t(mask_words)) + 256);
 }
 
 void engine_field_place(EngineField& f, const FieldLayout& L, int precision, void* block) {
-    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t esz = 8;
+    (void)precision;
     char* p = static_cast<char*>(block);
     f.T = p;
     p += up256(size_t(L.elems()) * esz);
@@ -604,7 +611,7 @@ void engine_field_place(EngineField& f, const FieldLayout& L, int precision, voi
 template <typename Real>
 int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     if (job.fields.empty()) return TS_OK;
-    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    const int precision = precision_of<Real>();
     // Every field's buffers from one pooled block of the context.
     std::vector<FieldLayout> layouts;
     for (auto* g : job.grids) layouts.push_back(field_layout(*g, job.tile, precision));
@@ -626,9 +633,9 @@ int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     return engine_epoch<Real>(ctx, job.grids, job.metrics, fl, job.tol, job.wake_rel, job.tile, 0, stats, ctx->stream);
 }
 
-template int engine_run<float>(ts_ctx*, EngineJob&, ts_eik_stats*);
+template int engine_run<Pair>(ts_ctx*, EngineJob&, ts_eik_stats*);
 template int engine_run<double>(ts_ctx*, EngineJob&, ts_eik_stats*);
-template int engine_epoch<float>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
+template int engine_epoch<Pair>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
                                  const std::vector<EngineField*>&, double, double, int, int, ts_eik_stats*, cudaStream_t);
 template int engine_epoch<double>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
                                   const std::vector<EngineField*>&, double, double, int, int, ts_eik_stats*, cudaStream_t);

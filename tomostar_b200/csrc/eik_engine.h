@@ -10,6 +10,7 @@
 
 #include "ctx.h"
 #include "host_geo.h"
+#include "ts_common.cuh"
 
 namespace ts {
 namespace eik {

@@ -45,9 +45,10 @@ static void merge_seeds(const int32_t* idx, const double* t, int count, int64_t 
 }
 
 template <typename Real>
-static int upload_real(ts_ctx* ctx, const std::string& key, const double* src, size_t count, Real** dst) {
+static int upload_real(ts_ctx* ctx, const std::string& key, const double* src, size_t count, Real** dst,
+                       const float* src32 = nullptr) {
     std::vector<Real> tmp(count);
-    for (size_t q = 0; q < count; q++) tmp[q] = Real(src[q]);
+    for (size_t q = 0; q < count; q++) tmp[q] = src32 ? Real(weight_of<Real>(src[q], src32[q])) : Real(src[q]);
     TS_BUF(ctx, d, Real, key, count);
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(d, tmp.data(), count * sizeof(Real), cudaMemcpyHostToDevice, ctx->stream));
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -67,8 +68,8 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
     const int64_t n = g.count();
     Real *wx, *wy, *zc = nullptr;
     int rc;
-    if ((rc = upload_real<Real>(ctx, "plain.wx", m.wx.data(), m.wx.size(), &wx))) return rc;
-    if ((rc = upload_real<Real>(ctx, "plain.wy", m.wy.data(), m.wy.size(), &wy))) return rc;
+    if ((rc = upload_real<Real>(ctx, "plain.wx", m.wx.data(), m.wx.size(), &wx, m.wx32.data()))) return rc;
+    if ((rc = upload_real<Real>(ctx, "plain.wy", m.wy.data(), m.wy.size(), &wy, m.wy32.data()))) return rc;
     if (g.variable && (rc = upload_real<Real>(ctx, "plain.zc", m.zc.data(), m.zc.size(), &zc))) return rc;
     TS_BUF(ctx, fixed, uint8_t, "plain.fixed", n);
     TS_BUF(ctx, dirty, uint8_t, "plain.dirty", n);
@@ -86,6 +87,7 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
     seed_kernel<Real><<<(int(sidx.size()) + 127) / 128, 128, 0, s>>>(T, fixed, at, tv, int(sidx.size()));
     TS_CUDA_TRY(ctx, cudaGetLastError());
     const int planes = nx + ny + nz - 2;
+    const Real wz1 = Real(weight_of<Real>(m.wz1, m.wz1_32)), wz2 = Real(weight_of<Real>(m.wz2, m.wz2_32));
     int launches = 0;
     struct Ev {  // events bracketing each round's plane launches
         cudaEvent_t e;
@@ -107,11 +109,11 @@ static int plain_solve(ts_ctx* ctx, const host::Grid& g, const host::Metric& m, 
                     dim3 grid((i1 - i0 + 1 + 127) / 128, k1 - k0 + 1);
                     if (g.variable)
                         plain_sweep_kernel<Real, true><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, wx, wy,
-                                                                              Real(m.wz1), Real(m.wz2), zc, nx, ny, nz, phase,
+                                                                              wz1, wz2, zc, nx, ny, nz, phase,
                                                                               changed, dir, p, Real(tol), updates);
                     else
                         plain_sweep_kernel<Real, false><<<grid, 128, 0, s>>>(T, slow_d, fixed, dirty, wx, wy,
-                                                                               Real(m.wz1), Real(m.wz2), zc, nx, ny, nz, phase,
+                                                                               wz1, wz2, zc, nx, ny, nz, phase,
                                                                                changed, dir, p, Real(tol), updates);
                     launches++;
                 }
@@ -163,7 +165,7 @@ int model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int n_ph
     m->precision = precision;
     m->n_phases = n_phases;
     const size_t count = size_t(m->grid->count()) * n_phases;
-    const size_t esz = precision == TS_PRECISION_F64 ? 8 : 4;
+    const size_t esz = 8;  // a double, or the FP32 precision's float pair (hi = the float slowness)
     if (cudaMalloc(&m->slowness, count * esz) != cudaSuccess) {
         cudaGetLastError();
         m->slowness = nullptr;
@@ -174,9 +176,10 @@ int model_put(ts_ctx* ctx, const ts_grid* grid, const double* slowness, int n_ph
     if (precision == TS_PRECISION_F64) {
         if (cudaMemcpy(m->slowness, slowness, count * 8, cudaMemcpyHostToDevice) != cudaSuccess) rc = TS_E_CUDA;
     } else {
-        std::vector<float> tmp(count);
-        for (size_t q = 0; q < count; q++) tmp[q] = float(slowness[q]);
-        if (cudaMemcpy(m->slowness, tmp.data(), count * 4, cudaMemcpyHostToDevice) != cudaSuccess) rc = TS_E_CUDA;
+        std::vector<Pair> tmp(count);
+        for (size_t q = 0; q < count; q++) tmp[q] = Pair(slowness[q]);
+        if (cudaMemcpy(m->slowness, tmp.data(), count * sizeof(Pair), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = TS_E_CUDA;
     }
     if (rc) {
         delete m;
@@ -260,7 +263,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
         job.metrics.push_back(&m);
         job.tol = in.tol;
         job.wake_rel = in.mode == TS_MODE_FAST ? TS_WAKE_REL : 0.0;
-        job.tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
+        job.tile = is_f64<Real>() ? ctx->tile_f64 : ctx->tile_f32;
         for (int f = 0; f < nf; f++) {
             EngineField ef;
             ef.grid = 0;
@@ -296,7 +299,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
     }
     ctx->stats = std::to_string(rounds_max[0]) + "+" + std::to_string(rounds_max[1]) + " rounds of 8 sweeps";
     if (rc) return rc;
-    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
+    const int precision = precision_of<Real>();
     if (out_type == TS_OUT_NONE) return TS_OK;  // the fields stay on the device
     if (in.mode == TS_MODE_PLAIN) return copy_fields_out(ctx, T, precision, int64_t(nf) * n, out, out_type);
     return fields_to_dense_host(ctx, job, precision, out, out_type);
@@ -305,7 +308,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
 int solve(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, ts_eik_stats* stats) {
     if (stats) std::memset(stats, 0, sizeof(*stats));
     if (in.precision == TS_PRECISION_F64) return solve_impl<double>(ctx, in, out, out_type, stats);
-    if (in.precision == TS_PRECISION_F32) return solve_impl<float>(ctx, in, out, out_type, stats);
+    if (in.precision == TS_PRECISION_F32) return solve_impl<Pair>(ctx, in, out, out_type, stats);
     return ctx->fail(TS_E_ARG, "precision must be 64 or 32");
 }
 
@@ -314,7 +317,7 @@ int copy_fields_out(ts_ctx* ctx, const void* fields_dev, int precision, int64_t 
     const bool src64 = precision == TS_PRECISION_F64;
     const bool dst64 = out_type == TS_OUT_F64;
     const size_t esz = dst64 ? 8 : 4;
-    if (src64 == dst64) {
+    if (src64 && dst64) {
         TS_CUDA_TRY(ctx, cudaMemcpyAsync(out, fields_dev, size_t(count) * esz, cudaMemcpyDeviceToHost, ctx->stream));
         TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         return TS_OK;
@@ -327,9 +330,12 @@ int copy_fields_out(ts_ctx* ctx, const void* fields_dev, int precision, int64_t 
         if (src64)
             convert_kernel<double, float><<<fill_blocks(len), 256, 0, ctx->stream>>>(
                 static_cast<const double*>(fields_dev) + o, static_cast<float*>(stage), len);
+        else if (dst64)
+            convert_kernel<Pair, double><<<fill_blocks(len), 256, 0, ctx->stream>>>(
+                static_cast<const Pair*>(fields_dev) + o, static_cast<double*>(stage), len);
         else
-            convert_kernel<float, double><<<fill_blocks(len), 256, 0, ctx->stream>>>(
-                static_cast<const float*>(fields_dev) + o, static_cast<double*>(stage), len);
+            convert_kernel<Pair, float><<<fill_blocks(len), 256, 0, ctx->stream>>>(
+                static_cast<const Pair*>(fields_dev) + o, static_cast<float*>(stage), len);
         TS_CUDA_TRY(ctx, cudaGetLastError());
         TS_CUDA_TRY(ctx, cudaMemcpyAsync(static_cast<char*>(out) + o * esz, stage, size_t(len) * esz,
                                          cudaMemcpyDeviceToHost, ctx->stream));

@@ -326,14 +326,14 @@ TS_DEVINL int process_tile(const Args<Real>& a, const GridDesc& g, const FieldDe
     const Real* wy = static_cast<const Real*>(g.wy);
     for (int q = lane; q < 2 * S::BY * S::BZ; q += 32) {
         int r = q >> 1, j = y0 + r % S::BY, k = z0 + r / S::BY;
-        mwx[q] = (j < ny && k < nz) ? __ldg(&wx[2 * (int64_t(k) * ny + j) + (q & 1)]) : Real(1);
+        mwx[q] = (j < ny && k < nz) ? ldg_r(&wx[2 * (int64_t(k) * ny + j) + (q & 1)]) : Real(1);
     }
-    for (int q = lane; q < 2 * S::BZ; q += 32) mwy[q] = (z0 + (q >> 1) < nz) ? __ldg(&wy[2 * z0 + q]) : Real(1);
+    for (int q = lane; q < 2 * S::BZ; q += 32) mwy[q] = (z0 + (q >> 1) < nz) ? ldg_r(&wy[2 * z0 + q]) : Real(1);
     if (VARZ) {
         const Real* zc = static_cast<const Real*>(g.zc);
         for (int q = lane; q < kZCoef * S::BZ; q += 32) {
             int k = z0 + q / kZCoef;
-            mzc[q] = k < nz ? __ldg(&zc[int64_t(k) * kZCoef + q % kZCoef]) : Real(1);
+            mzc[q] = k < nz ? ldg_r(&zc[int64_t(k) * kZCoef + q % kZCoef]) : Real(1);
         }
     }
     // The cube: every row segment the stencil reads (the interior rows with their x halo, and the

@@ -50,7 +50,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
 template <typename Real, int BX, bool VARZ, bool SPEC>
 TS_DEVINL int visit_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                            int tz, int dir, bool second, Real* halo, int lane) {
-    if constexpr (SPEC && sizeof(Real) == 8) {
+    if constexpr (SPEC && is_f64<Real>()) {
         switch (dir) {
 #define TS_PENCIL_DIR(d) \
     case d: return process_pencil<Real, BX, VARZ, d>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
@@ -128,10 +128,10 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     const Real* wyp = static_cast<const Real*>(g.wy);
     Real wx1 = Real(1), wx2 = Real(1), wy1 = Real(1), wy2 = Real(1);
     if (row_on) {
-        wx1 = __ldg(&wxp[2 * rowi]);
-        wx2 = __ldg(&wxp[2 * rowi + 1]);
-        wy1 = __ldg(&wyp[2 * gz]);
-        wy2 = __ldg(&wyp[2 * gz + 1]);
+        wx1 = ldg_r(&wxp[2 * rowi]);
+        wx2 = ldg_r(&wxp[2 * rowi + 1]);
+        wy1 = ldg_r(&wyp[2 * gz]);
+        wy2 = ldg_r(&wyp[2 * gz + 1]);
     }
     const Real wz1 = Real(g.wz1), wz2 = Real(g.wz2);
     const Real* zc = VARZ ? static_cast<const Real*>(g.zc) + kZCoef * (row_on ? gz : 0) : nullptr;
@@ -170,8 +170,8 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
         else return (row_on && c >= -2 && c <= BX + 1) ? ld_cg(row + ax(c)) : inf;
     };
     auto ldS = [&](int c) -> Real {
-        if constexpr (SDIR >= 0) return row_on ? __ldg(srow + max(0, min(ax(c), xlast))) : Real(0);
-        else return (row_on && c >= 0 && c < BX && x0 + ax(c) < nx) ? __ldg(srow + ax(c)) : Real(0);
+        if constexpr (SDIR >= 0) return row_on ? ldg_r(srow + max(0, min(ax(c), xlast))) : Real(0);
+        else return (row_on && c >= 0 && c < BX && x0 + ax(c) < nx) ? ldg_r(srow + ax(c)) : Real(0);
     };
     const int ip0 = -jp - kp;
     Real W0 = ldT(ip0 - 2), W1 = ldT(ip0 - 1), W2 = ldT(ip0), W3 = ldT(ip0 + 1), W4 = ldT(ip0 + 2);
@@ -202,10 +202,10 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
             if (__any_sync(FULL, is_due)) {
                 // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
                 // ahead has not (offset +1); two rows away likewise at offsets ∓2.
-                Real yb1 = __shfl_up_sync(FULL, W1, 1), ya1 = __shfl_down_sync(FULL, W3, 1);
-                Real yb2 = __shfl_up_sync(FULL, W0, 2), ya2 = __shfl_down_sync(FULL, W4, 2);
-                Real zb1 = __shfl_up_sync(FULL, W1, 8), za1 = __shfl_down_sync(FULL, W3, 8);
-                Real zb2 = __shfl_up_sync(FULL, W0, 16), za2 = __shfl_down_sync(FULL, W4, 16);
+                Real yb1 = shfl_up_r(FULL, W1, 1), ya1 = shfl_down_r(FULL, W3, 1);
+                Real yb2 = shfl_up_r(FULL, W0, 2), ya2 = shfl_down_r(FULL, W4, 2);
+                Real zb1 = shfl_up_r(FULL, W1, 8), za1 = shfl_down_r(FULL, W3, 8);
+                Real zb2 = shfl_up_r(FULL, W0, 16), za2 = shfl_down_r(FULL, W4, 16);
                 bool chg = false;
                 if (is_due) {
                     const int x = ax(ip);

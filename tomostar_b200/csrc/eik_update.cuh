@@ -5,11 +5,8 @@
 // operation is an explicit round-to-nearest intrinsic, so the compiler can neither contract a
 // multiply-add nor reorder: a result is the host's to the last bit, whichever kernel inlines it.
 //
-// FP32: the times are stored as float, and the update is solved as offsets from the smallest
-// upwind neighbour r (the scheme of the reference's paired-float kernel, EikonalOpenCl.cs:484-497,
-// 568-606): every quantity of the quadratic is then a cell crossing time, not an absolute time,
-// so float keeps the digits that survive the discriminant's subtraction. The stored time is
-// r + root rounded once to float.
+// FP32: the reference's paired-float kernel (times as hi + lo float pairs, the update in float
+// offsets from the smallest upwind neighbour; EikonalOpenCl.cs:454-497, 545-606), term for term.
 //
 // Extension (variable vertical spacing): the z axis may carry per-level coefficients instead of
 // the uniform spacing; see zcoef_* below. A uniform grid never takes that path.
@@ -134,87 +131,119 @@ TS_DEVINL double update64(double s, double xm, double xp, double xm2, double xp2
     return inf;
 }
 
-// ---- FP32, offsets from the smallest upwind neighbour -------------------------------------------
+// ---- FP32: times as float pairs hi + lo, the update in float offsets -----------------------------
+//
+// The reference's paired-float kernel term for term (EikonalOpenCl.cs:454-497 df_sub, df_add,
+// df_less, eik_pick, eik_term; 545-606 the root and the acceptance): each axis's upwind neighbour is
+// chosen by the lexicographic order of (hi, lo), the reference time r is the smallest of them, every
+// term is a float offset from r (a cell crossing time, so float keeps the digits that survive the
+// discriminant's subtraction), and the result r + root is formed as a pair by Knuth's two-sum.
+// Every float operation is an explicit round-to-nearest intrinsic (the kernel's FP_CONTRACT OFF),
+// so the result equals the reference kernel's to the bit on the same inputs.
 
-// Explicit intrinsics here too, so that two kernels inlining this update round identically.
 TS_DEVINL float fmul(float a, float b) { return __fmul_rn(a, b); }
 TS_DEVINL float fadd(float a, float b) { return __fadd_rn(a, b); }
 TS_DEVINL float fsub(float a, float b) { return __fadd_rn(a, -b); }
 TS_DEVINL float fdiv(float a, float b) { return __fdiv_rn(a, b); }
-TS_DEVINL float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
-struct Pick32 {
-    float first, t2;
+// df_sub: (a.hi − b.hi) + (a.lo − b.lo).
+TS_DEVINL float psub(Pair a, Pair b) { return fadd(fsub(a.hi, b.hi), fsub(a.lo, b.lo)); }
+// df_less: lexicographic on (hi, lo).
+TS_DEVINL bool pless(Pair a, Pair b) { return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo); }
+// df_add: r + x as hi + lo (Knuth's two-sum of r.hi and r.lo + x).
+TS_DEVINL Pair padd(Pair r, float x) {
+    float b = fadd(r.lo, x);
+    float s = fadd(r.hi, b);
+    float bb = fsub(s, r.hi);
+    float e = fadd(fsub(r.hi, fsub(s, bb)), fsub(b, bb));
+    return Pair(s, e);
+}
+
+struct PickP {
+    Pair first, t2;
     bool minus_side, ok;
 };
 
-TS_DEVINL Pick32 pick32(float minus, float plus, float minus2, float plus2) {
-    Pick32 p;
-    p.minus_side = minus <= plus;
+// eik_pick: the upwind neighbour of one axis and its second-order partner (+inf when absent or when
+// the update is first order: the kernels pass +inf for nodes off the grid).
+TS_DEVINL PickP pickp(Pair minus, Pair plus, Pair minus2, Pair plus2) {
+    PickP p;
+    p.minus_side = !pless(plus, minus);
     p.first = p.minus_side ? minus : plus;
     p.t2 = p.minus_side ? minus2 : plus2;
-    p.ok = p.first <= 3.4028234663852886e38f;
+    p.ok = finite_r(p.first.hi);
     return p;
 }
 
+// eik_term: the axis's term as offsets from r. Extension (variable depth spacing): the second-order
+// term takes the level's coefficient c/a in place of 1/3.
 template <bool VARZ>
-TS_DEVINL void term32(const Pick32& p, float r, float w1, float w2, const float* zc, bool second, float& te, float& we,
-                      float& tn) {
-    float of = fsub(p.first, r);
-    bool promote = second && (p.t2 <= 3.4028234663852886e38f) && p.t2 <= p.first;
+TS_DEVINL void termp(const PickP& p, Pair r, float w1, float w2, const Pair* zc, bool second, float& te, float& we,
+                     float& tn) {
+    const float of = psub(p.first, r);
+    const bool promote = second && finite_r(p.t2.hi) && !pless(p.first, p.t2);
     if (!VARZ) {
-        if (promote) { te = ffma(fsub(p.first, p.t2), 0.333333343f, of); we = w2; }
+        if (promote) { te = fadd(of, fdiv(psub(p.first, p.t2), 3.0f)); we = w2; }
         else { te = of; we = w1; }
     } else {
-        const float* c = zc + (p.minus_side ? 0 : 8);
-        if (promote) { te = ffma(fsub(p.first, p.t2), c[5], of); we = c[1]; }
-        else { te = of; we = c[0]; }
+        const Pair* c = zc + (p.minus_side ? 0 : 8);
+        if (promote) { te = fadd(of, fmul(psub(p.first, p.t2), c[5].hi)); we = c[1].hi; }
+        else { te = of; we = c[0].hi; }
     }
     tn = of;
 }
 
-TS_DEVINL bool root32(int terms, const float* t, const float* w, const float* n, float s, float& root) {
-    float base = t[0];
+// The root over the first `terms` sorted terms, as offsets from base = te[0] (EikonalOpenCl.cs:575-597).
+TS_DEVINL bool rootp(int terms, const float* t, const float* w, const float* n, float s, float& root) {
+    const float base = t[0];
     float sw = 0.f, swd = 0.f, swd2 = 0.f;
 #pragma unroll
-    for (int r = 0; r < 3; r++) {
-        if (r < terms) {
-            float d = fsub(t[r], base);
-            sw = fadd(sw, w[r]);
-            float wd = fmul(w[r], d);
-            swd = fadd(swd, wd);
-            swd2 = ffma(wd, d, swd2);
+    for (int q = 0; q < 3; q++) {
+        if (q < terms) {
+            const float d = fsub(t[q], base);
+            sw = fadd(sw, w[q]);
+            swd = fadd(swd, fmul(w[q], d));
+            swd2 = fadd(swd2, fmul(fmul(w[q], d), d));
         }
     }
-    float disc = ffma(swd, swd, -fmul(sw, ffma(-s, s, swd2)));
+    const float disc = fsub(fmul(swd, swd), fmul(sw, fsub(swd2, fmul(s, s))));
     if (disc < 0.f) return false;
     root = fadd(base, fdiv(fadd(swd, __fsqrt_rn(disc)), sw));
 #pragma unroll
-    for (int r = 0; r < 3; r++)
-        if (r < terms && root < n[r]) return false;
+    for (int q = 0; q < 3; q++)
+        if (q < terms && root < n[q]) return false;
     return true;
 }
 
-// The FP32 candidate time of a node (same inputs as update64).
+// The paired candidate time of a node (same inputs as update64; slowness and weights in hi).
 template <bool VARZ>
-TS_DEVINL float update32(float s, float xm, float xp, float xm2, float xp2, float ym, float yp, float ym2, float yp2,
-                         float zm, float zp, float zm2, float zp2, float wx1, float wx2, float wy1, float wy2,
-                         float wz1, float wz2, const float* zc, bool second) {
-    const float inf = real_inf<float>();
+TS_DEVINL Pair updatep(Pair sp, Pair xm, Pair xp, Pair xm2, Pair xp2, Pair ym, Pair yp, Pair ym2, Pair yp2, Pair zm,
+                       Pair zp, Pair zm2, Pair zp2, Pair wx1, Pair wx2, Pair wy1, Pair wy2, Pair wz1, Pair wz2,
+                       const Pair* zc, bool second) {
+    const Pair inf = real_inf<Pair>();
+    const float s = sp.hi;
     if (!(s > 0.f)) return inf;
-    Pick32 px = pick32(xm, xp, xm2, xp2), py = pick32(ym, yp, ym2, yp2), pz = pick32(zm, zp, zm2, zp2);
-    int used = int(px.ok) + int(py.ok) + int(pz.ok);
-    if (used == 0) return inf;
-    float r = fminf(px.ok ? px.first : inf, fminf(py.ok ? py.first : inf, pz.ok ? pz.first : inf));
-    float t[3] = {inf, inf, inf}, w[3] = {1.f, 1.f, 1.f}, n[3] = {inf, inf, inf};
-    if (px.ok) term32<false>(px, r, wx1, wx2, nullptr, second, t[0], w[0], n[0]);
-    if (py.ok) term32<false>(py, r, wy1, wy2, nullptr, second, t[1], w[1], n[1]);
-    if (pz.ok) term32<VARZ>(pz, r, wz1, wz2, zc, second, t[2], w[2], n[2]);
+    const Pair pinf = inf;
+    PickP px = pickp(xm, xp, second ? xm2 : pinf, second ? xp2 : pinf);
+    PickP py = pickp(ym, yp, second ? ym2 : pinf, second ? yp2 : pinf);
+    PickP pz = pickp(zm, zp, second ? zm2 : pinf, second ? zp2 : pinf);
+    if (!(px.ok || py.ok || pz.ok)) return inf;
+    Pair r = inf;
+    if (px.ok && pless(px.first, r)) r = px.first;
+    if (py.ok && pless(py.first, r)) r = py.first;
+    if (pz.ok && pless(pz.first, r)) r = pz.first;
+    const float finf = __builtin_huge_valf();
+    float t[3] = {finf, finf, finf}, w[3] = {1.f, 1.f, 1.f}, n[3] = {finf, finf, finf};
+    int used = 0;
+    if (px.ok) { termp<false>(px, r, wx1.hi, wx2.hi, nullptr, second, t[0], w[0], n[0]); used++; }
+    if (py.ok) { termp<false>(py, r, wy1.hi, wy2.hi, nullptr, second, t[1], w[1], n[1]); used++; }
+    if (pz.ok) { termp<VARZ>(pz, r, wz1.hi, wz2.hi, zc, second, t[2], w[2], n[2]); used++; }
     sort3(t, w, n);
     float root;
-    bool found = (used >= 3 && root32(3, t, w, n, s, root)) || (used >= 2 && root32(2, t, w, n, s, root)) ||
-                 root32(1, t, w, n, s, root);
-    return found ? fadd(r, root) : inf;
+    const bool found = (used >= 3 && rootp(3, t, w, n, s, root)) || (used >= 2 && rootp(2, t, w, n, s, root)) ||
+                       rootp(1, t, w, n, s, root);
+    if (!found || !finite_r(root)) return inf;
+    return padd(r, root);
 }
 
 // Generic front ends used by the kernels.
@@ -233,12 +262,12 @@ struct Update<double, VARZ> {
 };
 
 template <bool VARZ>
-struct Update<float, VARZ> {
-    TS_DEVINL static float eval(float s, float xm, float xp, float xm2, float xp2, float ym, float yp, float ym2,
-                                float yp2, float zm, float zp, float zm2, float zp2, float wx1, float wx2, float wy1,
-                                float wy2, float wz1, float wz2, const float* zc, bool second) {
-        return update32<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
-                              zc, second);
+struct Update<Pair, VARZ> {
+    TS_DEVINL static Pair eval(Pair s, Pair xm, Pair xp, Pair xm2, Pair xp2, Pair ym, Pair yp, Pair ym2, Pair yp2,
+                               Pair zm, Pair zp, Pair zm2, Pair zp2, Pair wx1, Pair wx2, Pair wy1, Pair wy2, Pair wz1,
+                               Pair wz2, const Pair* zc, bool second) {
+        return updatep<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
+                             zc, second);
     }
 };
 
@@ -251,18 +280,21 @@ TS_DEVINL bool wakes<double>(double cur, double cand, double wake_rel) {
     return !(cur <= 1.7976931348623157e308) || dsub(cur, cand) > dmul(wake_rel, cand);
 }
 template <>
-TS_DEVINL bool wakes<float>(float cur, float cand, float wake_rel) {
-    return !(cur <= 3.4028234663852886e38f) || fsub(cur, cand) > fmul(wake_rel, cand);
+TS_DEVINL bool wakes<Pair>(Pair cur, Pair cand, Pair wake_rel) {
+    return !finite_r(cur.hi) || psub(cur, cand) > fmul(wake_rel.hi, cand.hi);
 }
 
-// Whether a drop counts towards "the round changed something" (SphericalEikonal.cs:319).
+// Whether a drop counts towards "the round changed something" (SphericalEikonal.cs:319; the paired
+// kernel's `drop > TOL`, EikonalOpenCl.cs:604).
 template <typename Real>
-TS_DEVINL bool counts_as_change(Real cur, Real cand, Real tol) {
-    return !(cur <= Real(3.4028234663852886e38)) || (cur - cand) > tol;
-}
+TS_DEVINL bool counts_as_change(Real cur, Real cand, Real tol);
 template <>
 TS_DEVINL bool counts_as_change<double>(double cur, double cand, double tol) {
     return !(cur <= 1.7976931348623157e308) || dsub(cur, cand) > tol;
+}
+template <>
+TS_DEVINL bool counts_as_change<Pair>(Pair cur, Pair cand, Pair tol) {
+    return psub(cur, cand) > tol.hi;
 }
 
 }  // namespace ts

@@ -27,9 +27,10 @@ static int upload_slowness(ts_ctx* ctx, const double* src, size_t count, Real* d
 // The float32 tables of `tables` ((phase, source) pairs; sources hold lon, lat, depth) on g, solved
 // by the engine in batches that fit the device next to the tables, each rounded to float32 into its
 // slot of `tab` (n_nodes floats per table): TravelTimeTableSet.Build (Forward/TravelTimeTable.cs:264-308)
-// with the seeds of PointSource at the source (:373).
+// with the seeds of PointSource at the source (:373). mode: TS_MODE_ENGINE (the reference's fields to
+// the bit) or TS_MODE_FAST (within 1e-10 relative of them, about half the node evaluations).
 template <typename Real>
-int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n_phases,
+int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n_phases, int mode,
                  const std::vector<std::pair<int, int>>& tables, const double* sources, float* tab,
                  ts_eik_stats* stats) {
     host::Metric m(g);
@@ -59,8 +60,8 @@ int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n
         st[t].assign(tv.begin(), tv.begin() + c);
         if (c == 0) return ctx->fail(TS_E_NOSEEDS, "no seed nodes for source " + std::to_string(tables[t].second));
     }
-    const int precision = sizeof(Real) == 8 ? TS_PRECISION_F64 : TS_PRECISION_F32;
-    const int tile = sizeof(Real) == 8 ? ctx->tile_f64 : ctx->tile_f32;
+    const int precision = precision_of<Real>();
+    const int tile = is_f64<Real>() ? ctx->tile_f64 : ctx->tile_f32;
     const size_t per_field = size_t(eik::field_layout(g, tile, precision).bytes(precision));
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -77,6 +78,7 @@ int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n
         job.grids.push_back(&g);
         job.metrics.push_back(&m);
         job.tol = 1e-7;  // SphericalEikonal.SettleTolerance
+        job.wake_rel = mode == TS_MODE_FAST ? TS_WAKE_REL : 0.0;
         job.tile = tile;
         for (int t = t0; t < t1; t++) {
             eik::EngineField ef;
@@ -127,13 +129,13 @@ int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n
     return TS_OK;
 }
 
-template int solve_tables<double>(ts_ctx*, const host::Grid&, const double*, int, const std::vector<std::pair<int, int>>&,
+template int solve_tables<double>(ts_ctx*, const host::Grid&, const double*, int, int, const std::vector<std::pair<int, int>>&,
                                   const double*, float*, ts_eik_stats*);
-template int solve_tables<float>(ts_ctx*, const host::Grid&, const double*, int, const std::vector<std::pair<int, int>>&,
+template int solve_tables<Pair>(ts_ctx*, const host::Grid&, const double*, int, int, const std::vector<std::pair<int, int>>&,
                                  const double*, float*, ts_eik_stats*);
 
 template <typename Real>
-static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slowness, int n_phases,
+static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slowness, int n_phases, int mode,
                         const ts_grid* inv_def, int n_stations, const double* stations, int n_events,
                         const double* events, int n_arr, const int32_t* arr_event, const int32_t* arr_station,
                         const int32_t* arr_phase, double step_km, ts_rows** out, ts_eik_stats* stats) {
@@ -161,7 +163,7 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
         tab = static_cast<float*>(ctx->buf("fwd.tables", sizeof(float) * size_t(n) * nt));
         if (!tab) return TS_E_NOMEM;
     }
-    int rc = solve_tables<Real>(ctx, g, slowness, n_phases, tables, stations, tab, stats);
+    int rc = solve_tables<Real>(ctx, g, slowness, n_phases, mode, tables, stations, tab, stats);
     if (rc) return rc;
     // Arrivals → rays (the engine's field buffers were released for the rows).
     std::vector<int32_t> table_of(std::max(1, n_arr));
@@ -183,8 +185,8 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
 extern "C" int ts_forward(ts_ctx* ctx, const ts_grid* fwd, const double* slowness, int32_t n_phases,
                           const ts_grid* inv, int32_t n_stations, const double* stations, int32_t n_events,
                           const double* events, int32_t n_arrivals, const int32_t* arr_event,
-                          const int32_t* arr_station, const int32_t* arr_phase, int32_t precision, double step_km,
-                          ts_rows** out, ts_eik_stats* stats) {
+                          const int32_t* arr_station, const int32_t* arr_phase, int32_t precision, int32_t mode,
+                          double step_km, ts_rows** out, ts_eik_stats* stats) {
     if (!ctx || !out) return TS_E_ARG;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
@@ -198,11 +200,12 @@ extern "C" int ts_forward(ts_ctx* ctx, const ts_grid* fwd, const double* slownes
         return ctx->fail(TS_E_ARG, "bad sizes");
     if (n_arrivals > 0 && (!stations || !events || !arr_event || !arr_station || !arr_phase))
         return ctx->fail(TS_E_ARG, "null arrival arrays");
+    if (mode != TS_MODE_ENGINE && mode != TS_MODE_FAST) return ctx->fail(TS_E_ARG, "mode must be engine or fast");
     if (precision == TS_PRECISION_F64)
-        return ts::fwd::forward_impl<double>(ctx, fwd, slowness, n_phases, inv, n_stations, stations, n_events, events,
+        return ts::fwd::forward_impl<double>(ctx, fwd, slowness, n_phases, mode, inv, n_stations, stations, n_events, events,
                                              n_arrivals, arr_event, arr_station, arr_phase, step_km, out, stats);
     if (precision == TS_PRECISION_F32)
-        return ts::fwd::forward_impl<float>(ctx, fwd, slowness, n_phases, inv, n_stations, stations, n_events, events,
+        return ts::fwd::forward_impl<ts::Pair>(ctx, fwd, slowness, n_phases, mode, inv, n_stations, stations, n_events, events,
                                             n_arrivals, arr_event, arr_station, arr_phase, step_km, out, stats);
     return ctx->fail(TS_E_ARG, "precision must be 64 or 32");
 }

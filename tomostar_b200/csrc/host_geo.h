@@ -150,27 +150,42 @@ struct Metric {
     std::vector<double> wx;  // 2 per (k, j): w1, w2 of the longitude axis
     std::vector<double> wy;  // 2 per k: latitude axis
     double hr = 0, wz1 = 1, wz2 = 1;
+    // The same weights as the paired-float kernel forms them, in float from the spacing narrowed to
+    // float (eik_term: he = 2.0f * h / 3.0f, we = 1.0f / (he * he); EikonalOpenCl.cs:490-495).
+    std::vector<float> wx32, wy32;
+    float wz1_32 = 1, wz2_32 = 1;
     static void weights(double h, double& w1, double& w2) {
         w1 = 1.0 / (h * h);
         double he = 2 * h / 3;
         w2 = 1.0 / (he * he);
+    }
+    static void weights32(double h64, float& w1, float& w2) {
+        const float h = float(h64);
+        w1 = 1.0f / (h * h);
+        const float he = 2.0f * h / 3.0f;
+        w2 = 1.0f / (he * he);
     }
     explicit Metric(const Grid& g) {
         hlon.resize(size_t(g.ny) * g.nz);
         hlat.resize(g.nz);
         wx.resize(2 * hlon.size());
         wy.resize(2 * size_t(g.nz));
+        wx32.resize(wx.size());
+        wy32.resize(wy.size());
         for (int k = 0; k < g.nz; k++) {
             hlat[k] = g.rad[k] * g.dlat_rad;
             weights(hlat[k], wy[2 * k], wy[2 * k + 1]);
+            weights32(hlat[k], wy32[2 * k], wy32[2 * k + 1]);
             for (int j = 0; j < g.ny; j++) {
                 size_t q = size_t(k) * g.ny + j;
                 hlon[q] = std::max(1e-9, g.rad[k] * g.coslat[j] * g.dlon_rad);
                 weights(hlon[q], wx[2 * q], wx[2 * q + 1]);
+                weights32(hlon[q], wx32[2 * q], wx32[2 * q + 1]);
             }
         }
         hr = g.ddep;
         weights(hr, wz1, wz2);
+        weights32(hr, wz1_32, wz2_32);
         if (g.variable) {
             zc.assign(size_t(16) * g.nz, 1.0);
             auto side = [&](double* c, double h1, double h2) {

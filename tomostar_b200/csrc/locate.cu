@@ -900,9 +900,9 @@ int ts_tables_build(ts_ctx* ctx, const ts_grid* grid, const double* slowness, in
     }
     host::Grid g(*grid);
     int rc = precision == TS_PRECISION_F32
-                 ? fwd::solve_tables<float>(ctx, g, slowness, n_phases, list, sources, tb->dev, stats)
+                 ? fwd::solve_tables<ts::Pair>(ctx, g, slowness, n_phases, TS_MODE_ENGINE, list, sources, tb->dev, stats)
              : precision == TS_PRECISION_F64
-                 ? fwd::solve_tables<double>(ctx, g, slowness, n_phases, list, sources, tb->dev, stats)
+                 ? fwd::solve_tables<double>(ctx, g, slowness, n_phases, TS_MODE_ENGINE, list, sources, tb->dev, stats)
                  : ctx->fail(TS_E_ARG, "precision must be 64 or 32");
     if (rc) {
         cudaFree(tb->dev);

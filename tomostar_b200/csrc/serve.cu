@@ -159,7 +159,7 @@ void admit(ts_server* sv) {
         const ts::eik::FieldLayout L = ts::eik::field_layout(*m.grid, sv->tile, sv->precision);
         const size_t fb = (size_t(L.bytes(sv->precision)) + 255) / 256 * 256;
         char* p = static_cast<char*>(block);  // the fields' buffers, then their float32 tables
-        const size_t esz = sv->precision == TS_PRECISION_F64 ? 8 : 4;
+        const size_t esz = 8;  // model slowness: a double, or the FP32 precision's float pair
         r->fields.resize(r->n_fields);
         for (int f = 0; f < r->n_fields; f++) {
             EngineField& ef = r->fields[f];
@@ -348,7 +348,7 @@ void serve_loop(ts_server* sv) {
             rc = sv->precision == TS_PRECISION_F64
                      ? ts::eik::engine_epoch<double>(ctx, grids, metrics, fl, ts::kSettleTolerance, wake_rel, sv->tile,
                                                      sv->rounds_per_epoch, &st, ctx->stream)
-                     : ts::eik::engine_epoch<float>(ctx, grids, metrics, fl, ts::kSettleTolerance, wake_rel, sv->tile,
+                     : ts::eik::engine_epoch<ts::Pair>(ctx, grids, metrics, fl, ts::kSettleTolerance, wake_rel, sv->tile,
                                                     sv->rounds_per_epoch, &st, ctx->stream);
         }
         const auto te1 = Clock::now();

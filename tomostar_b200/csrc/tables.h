@@ -23,7 +23,7 @@ namespace fwd {
 // The tables of `tables` ((phase, source) pairs; sources: lon, lat, depth) solved by the engine into
 // tab (nodes floats per table) with the .qttb float32 rounding (TravelTimeTable.cs:264-308, :373).
 template <typename Real>
-int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n_phases,
+int solve_tables(ts_ctx* ctx, const host::Grid& g, const double* slowness, int n_phases, int mode,
                  const std::vector<std::pair<int, int>>& tables, const double* sources, float* tab,
                  ts_eik_stats* stats);
 

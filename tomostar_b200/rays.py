@@ -127,9 +127,10 @@ class RayKernels:
         self.last_stats = L.EikStats()
 
     def compute(self, slowness_fwd: np.ndarray, stations: np.ndarray, events: np.ndarray, arrivals: np.ndarray,
-                precision: int | None = None, step: float | None = None) -> Rows:
+                precision: int | None = None, step: float | None = None, mode: int = L.MODE_FAST) -> Rows:
         """slowness_fwd: (n_phases, n) on the forward grid (ForwardModel); stations/events (k, 3)
-        lon, lat, depth; arrivals (m, 3) int (event, station, phase)."""
+        lon, lat, depth; arrivals (m, 3) int (event, station, phase). mode: L.MODE_FAST (tables within
+        1e-10 relative of the reference's fields) or L.MODE_ENGINE (the reference's to the bit)."""
         lib = L.load()
         s = np.ascontiguousarray(slowness_fwd, np.float64).reshape(-1, self.forward.count)
         st = np.ascontiguousarray(stations, np.float64).reshape(-1, 3)
@@ -143,7 +144,8 @@ class RayKernels:
         rc = lib.ts_forward(self.solver.handle, C.byref(fs), s.ctypes.data_as(P(C.c_double)), len(s), C.byref(is_),
                             len(st), st.ctypes.data_as(P(C.c_double)), len(ev), ev.ctypes.data_as(P(C.c_double)),
                             len(ar), ae.ctypes.data_as(P(C.c_int32)), ast.ctypes.data_as(P(C.c_int32)),
-                            ap.ctypes.data_as(P(C.c_int32)), prec, step or 0.0, C.byref(h), C.byref(self.last_stats))
+                            ap.ctypes.data_as(P(C.c_int32)), prec, mode, step or 0.0, C.byref(h),
+                            C.byref(self.last_stats))
         if rc != L.TS_OK:
             raise L.TsError(rc, self.solver.last_error)
         return _fetch(h)
