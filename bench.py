@@ -6,9 +6,10 @@
 One step = every field of the job solved once by the batched engine (two launches: the P and the
 S fields). `value` is fields/s with the velocity model resident in HBM and the fields left on the
 device; `e2e` is the same job through the C-ABI entry point a host calls (ts_eik_solve: slowness and
-seeds from host memory, float32 tables read back into pinned host memory). Under torchrun every rank
-solves its own job of 800 fields (different stations; weak scaling, no collective on the data path);
-rank 0 prints one JSON line with the max-over-ranks time. At N = 1 the line also carries the
+seeds from host memory, float32 tables read back into pinned host memory). Under torchrun the N
+ranks split one job of 400·N stations by station (station i on rank i % N, as the reference's MPI
+session does; 800 fields per rank: weak scaling, no collective on the data path); rank 0 prints one
+JSON line with the max-over-ranks time. At N = 1 the line also carries the
 serving load (`serving`: Poisson arrivals at 200 requests/s of mixed eikonal, ray and resolution
 requests on three grid sizes, p50/p99 latency and fields/s). `--impl reference` times the
 reference's CPU solver (fast marching, restated in oracle/) on the host cores on a bounded sample of
@@ -129,13 +130,21 @@ def max_over_ranks(dist, local, x: float) -> float:
     return float(t.item())
 
 
-def rank_problem(rank: int, dims=(401, 401, 121)):
-    """Weak scaling with no collective on the data path: rank r solves its own job of the same shape
-    (the workload generated with seed 5 + r: its own stations, events and velocity bodies).
-    `dims` smaller than 401x401x121 is only for profiling captures that must stay small."""
+def job_problem(world: int, dims=(401, 401, 121)):
+    """The regional job for `world` GPUs: 400 surface stations per GPU on one model (seed 5), so that
+    each GPU's share is the size of the 1-GPU job (weak scaling). `dims` smaller than 401x401x121 is
+    only for profiling captures that must stay small."""
     from tomostar_b200 import synthetic as syn
 
-    return syn.regional_401(seed=5 + rank, dims=dims)
+    return syn.regional_401(n_stations=400 * world, dims=dims)
+
+
+def rank_stations(problem, rank: int, world: int):
+    """The stations rank `rank` solves: station i goes to rank i % world (Compute/MpiSession.cs:97), so
+    the ranks split one job by station with no collective on the data path."""
+    from tomostar_b200 import shard
+
+    return problem.stations[shard.station_share(len(problem.stations), rank, world)]
 
 
 def job_throughput(dist, local, world: int, fields_per_rank_step: int, steps: int, dev_ms: float):
@@ -293,7 +302,7 @@ def run_reference(args, problem_fn):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     threads = os.cpu_count() or 1
-    p = problem_fn(0)
+    p = problem_fn(1)
     n = threads  # one field per host thread: ~one fast-marching solve of time per step
     rates = []
     for step in range(args.warmup + args.steps):
@@ -321,10 +330,11 @@ def run_ours(args, problem_fn):
     from tomostar_b200.eikonal import EikonalCuda, pack_seeds, point_source
 
     lib = L.load()
-    p = problem_fn(rank)
+    p = problem_fn(world)
     g = p.grid
     n = g.count
-    n_st = min(len(p.stations), args.fields) if args.fields > 0 else len(p.stations)
+    my_st = rank_stations(p, rank, world)
+    n_st = min(len(my_st), args.fields) if args.fields > 0 else len(my_st)
     solver = EikonalCuda.create(local, 64)
     rel, msg = solver.self_test()
     if not (rel <= 1e-6):
@@ -332,7 +342,7 @@ def run_ours(args, problem_fn):
     lib.ts_engine_set_tile(solver.handle, 64, args.tile)
     lib.ts_engine_set_scheduler(solver.handle, args.scheduler)
     # Seeds of every (station, phase) field, on the host before timing (PointSource, C ABI).
-    seeds = {ph: [point_source(g, p.slowness[ph], *p.stations[q]) for q in range(n_st)] for ph in (0, 1)}
+    seeds = {ph: [point_source(g, p.slowness[ph], *my_st[q]) for q in range(n_st)] for ph in (0, 1)}
     packed = {ph: pack_seeds(seeds[ph]) for ph in (0, 1)}
     gs = g.struct()
     mid = C.c_int32()
@@ -600,7 +610,7 @@ def main():
                     help="grid of the regional job (smaller only for profiling captures; the bench line is 401,401,121)")
     args = ap.parse_args()
     dims = tuple(int(v) for v in args.dims.split(","))
-    problem_fn = lambda rank: rank_problem(rank, dims)  # noqa: E731
+    problem_fn = lambda world: job_problem(world, dims)  # noqa: E731
 
     if args.impl == "reference":
         return run_reference(args, problem_fn)

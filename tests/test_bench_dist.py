@@ -1,6 +1,6 @@
-"""The multi-GPU path of bench.py on CPU ranks (gloo, world size 2): each rank solves a job of its
-own (no collective on the data path) and the whole-job throughput divides every rank's fields by
-the slowest rank's time, reduced with one all-reduce."""
+"""The multi-GPU path of bench.py on CPU ranks (gloo, world size 2): the ranks split one job by
+station (station i on rank i % N; no collective on the data path) and the whole-job throughput
+divides every rank's fields by the slowest rank's time, reduced with one all-reduce."""
 import os
 import socket
 import sys
@@ -30,8 +30,8 @@ def _rank(rank, world, port, out):
     try:
         dev_ms = [1000.0, 1250.0][rank]  # the second rank is slower
         value, dev_max = bench.job_throughput(dist, 0, world, 800, 3, dev_ms)
-        p = bench.rank_problem(rank)
-        out[rank] = (value, dev_max, p.stations[:3].tolist())
+        p = bench.job_problem(world, dims=(41, 41, 21))
+        out[rank] = (value, dev_max, bench.rank_stations(p, rank, world).tolist(), p.stations.tolist())
     finally:
         dist.destroy_process_group()
 
@@ -50,7 +50,11 @@ def test_weak_scaling_throughput_two_ranks():
             assert p.exitcode == 0
         res = dict(out)
     for r in range(world):
-        value, dev_max, _ = res[r]
+        value, dev_max, _, _ = res[r]
         assert dev_max == 1250.0
         assert value == pytest.approx(800 * 2 * 3 / 1.25)
-    assert res[0][2] != res[1][2]  # each rank has its own stations
+    # One job (the same stations on both ranks), split by station: 400 per rank, disjoint, complete.
+    allst = res[0][3]
+    assert res[1][3] == allst and len(allst) == 800
+    assert len(res[0][2]) == len(res[1][2]) == 400
+    assert sorted(map(tuple, res[0][2] + res[1][2])) == sorted(map(tuple, allst))
