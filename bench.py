@@ -297,6 +297,180 @@ def resample_job(device: int) -> dict:
             "note": "end to end per call: 39 MB of inversion slowness uploaded, 311 MB model allocated and written"}
 
 
+def _fmm_sample_fields_per_s(grids, slownesses, seed_sets, threads: int):
+    """The reference's CPU solver (SphericalEikonal.Solve, fast marching, restated in oracle/) on the
+    given fields, one field per host thread; returns (fields/s, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+
+    def one(q):
+        return O.fmm(O.Grid.of(grids[q]), slownesses[q], *seed_sets[q])
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(one, range(len(grids))))
+    dt = time.perf_counter() - t0
+    return len(grids) / dt, dt
+
+
+def inversion_job(device: int, threads: int) -> dict:
+    """The forward step of a synthetic inversion (121x121x61 at 0.5 km, 25 stations x P,S = 50 fields,
+    7,500 rays) in FP64 and FP32 (the paired-float scheme): engine fields/s with the model resident,
+    its roofline, the forward step through ts_forward (tables + Jacobian rows), the plain per-plane
+    GPU path on one field and the CPU solver on a sample of fields."""
+    from oracle import oracle as O
+    from tomostar_b200 import _lib as L
+    from tomostar_b200 import synthetic as syn
+    from tomostar_b200.eikonal import EikonalCuda, pack_seeds, point_source
+    from tomostar_b200.rays import RayKernels
+
+    p = syn.inversion_step_121()
+    g = p.grid
+    lib = L.load()
+    P = C.POINTER
+    peak, _ = measured_hbm_peak()
+    seeds = {ph: [point_source(g, p.slowness[ph], *p.stations[q]) for q in range(len(p.stations))] for ph in (0, 1)}
+    out = {"workload": "inversion_step_121: 121x121x61 at 0.5 km (0.89 M nodes), 25 stations x P,S = 50 fields, "
+                       "150 events, 7,500 P+S rays into a CSR Jacobian"}
+    with EikonalCuda.create(device, 64) as s:
+        for prec in (64, 32):
+            gs = g.struct()
+            mid = C.c_int32()
+            s_all = np.ascontiguousarray(p.slowness)
+            L.check(lib.ts_model_put(s.handle, C.byref(gs), s_all.ctypes.data_as(P(C.c_double)), 2, prec,
+                                     C.byref(mid)), s)
+            stats = L.EikStats()
+
+            def step():
+                dev = kern = 0.0
+                upd = 0
+                for ph in (0, 1):
+                    off, idx, t = pack_seeds(seeds[ph])
+                    L.check(lib.ts_eik_solve_model(s.handle, mid.value, ph, len(seeds[ph]),
+                                                   off.ctypes.data_as(P(C.c_int32)), idx.ctypes.data_as(P(C.c_int32)),
+                                                   t.ctypes.data_as(P(C.c_double)), L.MODE_FAST, 1e-7, 0, None,
+                                                   L.OUT_NONE, C.byref(stats)), s)
+                    dev += stats.device_ms
+                    kern += stats.kernel_ms
+                    upd += stats.node_updates
+                return dev, kern, upd
+
+            for _ in range(3):
+                step()
+            runs = [step() for _ in range(5)]
+            dev = sum(r[0] for r in runs) / 5
+            kern = sum(r[1] for r in runs) / 5
+            upd = runs[-1][2]
+            ach = upd * 24 / (kern / 1e3) / 1e9
+            rk = RayKernels(p.inv, g, s)
+            rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=prec)  # warm-up
+            t0 = time.perf_counter()
+            rows = rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=prec)
+            fwd_s = time.perf_counter() - t0
+            tables_s = rk.last_stats.device_ms / 1e3
+            out[f"fp{prec}"] = {
+                "fields_per_s": 50 / (dev / 1e3), "ms_per_50_fields": dev, "node_updates": upd,
+                "updates_per_s": upd / (kern / 1e3),
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                             "bytes_per_update": 24},
+                "forward_step": {"wall_s": fwd_s, "tables_s": tables_s, "rows": int(rows.n_rows),
+                                 "kept_rows": int(rows.ok.sum()), "nnz": int(rows.nnz),
+                                 "rows_per_s": rows.n_rows / fwd_s,
+                                 "rays_rows_per_s": rows.n_rows / max(1e-9, fwd_s - tables_s)},
+            }
+            lib.ts_model_drop(s.handle, mid.value)
+        # FP32 against the FP64 fields on two of the fields (the bitwise engine is the FP64 oracle).
+        sub_seeds = [seeds[0][0], seeds[1][7]]
+        worst = 0.0
+        for q, ph in enumerate((0, 1)):
+            f64 = s.solve(g, p.slowness[ph], [sub_seeds[q]], precision=64, mode=L.MODE_ENGINE)[0]
+            f32 = s.solve(g, p.slowness[ph], [sub_seeds[q]], precision=32, mode=L.MODE_ENGINE)[0]
+            fin = np.isfinite(f64) & (f64 > 0)
+            worst = max(worst, float(np.max(np.abs(f32[fin] - f64[fin]) / f64[fin])))
+        out["fp32_max_rel_err_vs_fp64"] = worst
+        # Plain per-plane GPU path, one field.
+        t0 = time.perf_counter()
+        s.solve(g, p.slowness[0], [seeds[0][0]], precision=64, mode=L.MODE_PLAIN)
+        out["plain_gpu"] = {"fields_per_s": 1 / (time.perf_counter() - t0), "sample": "1 P field, one launch per plane"}
+    n_cpu = min(threads, 50)
+    gl = [g] * n_cpu
+    sl = [p.slowness[q % 2] for q in range(n_cpu)]
+    ss = [seeds[q % 2][q // 2 % 25] for q in range(n_cpu)]
+    r, dt = _fmm_sample_fields_per_s(gl, sl, ss, threads)
+    out["cpu_baseline"] = {"fields_per_s": r, "cores": threads, "kind": "port",
+                           "sample": f"{n_cpu} of the 50 fields, fast marching one field per thread"}
+    out["speedup_fp64_vs_cpu"] = out["fp64"]["fields_per_s"] / r
+    out["speedup_fp64_vs_plain_gpu"] = out["fp64"]["fields_per_s"] / out["plain_gpu"]["fields_per_s"]
+    return out
+
+
+def uneven_job(device: int, threads: int) -> dict:
+    """200 sources each on its own grid (48-192 x 48-192 x 32-96 nodes, half with geometric depth
+    spacing) solved in one persistent engine launch, the tile shape and scheduler picked by the
+    autotuner on a 40-grid sample, the job captured as a CUDA graph and replayed; FP32 (the named
+    precision: paired floats) and FP64. Baselines: the plain per-plane GPU path and the CPU solver on
+    samples of the grids."""
+    from tomostar_b200 import _lib as L
+    from tomostar_b200 import synthetic as syn
+    from tomostar_b200.eikonal import EikonalCuda, point_source
+
+    b = syn.uneven_grids(200)
+    seeds = [point_source(g, s, *src) for g, s, src in zip(b.grids, b.slowness, b.sources)]
+    fg = list(range(len(b.grids)))
+    nodes = sum(g.count for g in b.grids)
+    peak, _ = measured_hbm_peak()
+    out = {"workload": f"uneven_grids: 200 grids ({nodes / 1e6:.1f} M nodes in all, {sum(g.depth_km is not None for g in b.grids)} "
+                       "with geometric depth spacing), one source each, seed 3"}
+    with EikonalCuda.create(device, 64) as s:
+        lib = L.load()
+        for prec in (32, 64):
+            sample = list(range(0, 200, 5))
+            best, sched, table = s.autotune([b.grids[q] for q in sample], [b.slowness[q] for q in sample],
+                                            list(range(len(sample))), [seeds[q] for q in sample], mode=L.MODE_FAST,
+                                            precision=prec)
+            lib.ts_engine_set_tile(s.handle, prec, best)
+            lib.ts_engine_set_scheduler(s.handle, sched)
+            s.set_graph(True)
+            times, kern, upd = [], [], 0
+            for rep in range(4):
+                s.solve_multi(b.grids, b.slowness, fg, seeds, out_dtype=None, mode=L.MODE_FAST, precision=prec)
+                st = s.last_stats_struct
+                if rep >= 1:  # the first call captures the graph
+                    times.append(st.device_ms)
+                    kern.append(st.kernel_ms)
+                    upd = st.node_updates
+            replays = s.graph_replays
+            s.set_graph(False)
+            ms = float(np.median(times))
+            shape = {sid: f"{bx}x{by}x{bz}" for sid, bx, by, bz in L.engine_shapes()}[best]
+            k_ms = float(np.median(kern)) if any(k > 0 for k in kern) else ms
+            ach = upd * 24 / (k_ms / 1e3) / 1e9
+            out[f"fp{prec}"] = {"fields_per_s": 200 / (ms / 1e3), "ms_per_job": ms, "node_updates": int(upd),
+                                "updates_per_s": upd / (ms / 1e3), "graph_replays": int(replays),
+                                "autotuned": {"shape": shape, "scheduler": ["lockstep", "flow"][sched]},
+                                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                                             "frac": ach / peak, "bytes_per_update": 24}}
+        lib.ts_engine_set_tile(s.handle, 64, 0)
+        lib.ts_engine_set_tile(s.handle, 32, 0)
+        lib.ts_engine_set_scheduler(s.handle, 0)
+        # Plain per-plane GPU path on four of the grids (one field each).
+        t0 = time.perf_counter()
+        for q in (0, 50, 100, 150):
+            s.solve(b.grids[q], b.slowness[q], [seeds[q]], precision=64, mode=L.MODE_PLAIN)
+        plain = 4 / (time.perf_counter() - t0)
+    out["plain_gpu"] = {"fields_per_s": plain, "sample": "grids 0, 50, 100, 150 one at a time, one launch per plane"}
+    n_cpu = min(threads, 32)
+    q = list(range(0, 200, 200 // n_cpu))[:n_cpu]
+    r, dt = _fmm_sample_fields_per_s([b.grids[i] for i in q], [b.slowness[i] for i in q], [seeds[i] for i in q],
+                                     threads)
+    out["cpu_baseline"] = {"fields_per_s": r, "cores": threads, "kind": "port",
+                           "sample": f"{n_cpu} of the 200 grids, fast marching one grid per thread"}
+    out["speedup_vs_plain_gpu"] = out["fp32"]["fields_per_s"] / plain
+    out["speedup_vs_cpu"] = out["fp32"]["fields_per_s"] / r
+    return out
+
+
 def run_reference(args, problem_fn):
     # The CPU arm needs no process group: rank 0 alone runs it and prints the line.
     if int(os.environ.get("RANK", "0")) != 0:
@@ -536,6 +710,16 @@ def run_ours(args, problem_fn):
             resample = resample_job(local)
         except Exception as exc:  # noqa: BLE001
             resample = {"error": repr(exc)[:300]}
+    inversion = uneven = None
+    if world == 1 and not args.no_configs:
+        try:
+            inversion = inversion_job(local, os.cpu_count() or 1)
+        except Exception as exc:  # noqa: BLE001
+            inversion = {"error": repr(exc)[:300]}
+        try:
+            uneven = uneven_job(local, os.cpu_count() or 1)
+        except Exception as exc:  # noqa: BLE001
+            uneven = {"error": repr(exc)[:300]}
     # The serving load (Poisson stream of mixed requests) on one GPU, after the batch job's buffers
     # are released; at N = 1 only (the scaling runs measure the batch job).
     serving = None
@@ -572,6 +756,8 @@ def run_ours(args, problem_fn):
             "forward_step": forward,
             "location": location,
             "resample": resample,
+            "inversion_step_121": inversion,
+            "uneven_grids": uneven,
             "serving": serving,
             "node_updates_per_step": updates // args.steps,
             "wall_s_timed": t_wall,
@@ -590,7 +776,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tile", type=int, default=5)
     ap.add_argument("--mode", type=int, default=2, help="0 engine (bitwise), 2 fast (wake threshold 1e-13)")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-baselines", action="store_true")
     ap.add_argument("--fields", type=int, default=0, help="stations per step (default all 400; fewer = a small case)")
@@ -600,6 +786,8 @@ def main():
     ap.add_argument("--no-forward", action="store_true", help="skip the forward step (tables + rays)")
     ap.add_argument("--no-forward-exact", action="store_true", help="skip the bitwise-mode forward step")
     ap.add_argument("--no-location", action="store_true", help="skip the relocation measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 121x121x61 inversion step and the 200 uneven grids sections")
     ap.add_argument("--location-events", type=int, default=4000)
     ap.add_argument("--location-cpu-events", type=int, default=256, help="events the CPU baseline locates")
     ap.add_argument("--serve-scheduler", type=int, default=1)

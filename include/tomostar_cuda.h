@@ -125,14 +125,16 @@ int ts_eik_solve_model(ts_ctx* ctx, int32_t model_id, int32_t phase, int32_t n_f
  * by another allocator (a framework's caching pool, a serving budget reserved at start-up), a plug-in
  * host that forbids device allocation after initialisation, or a latency-critical path that cannot
  * take an allocation's implicit synchronisation. The caller passes its own device buffers:
- * slowness_dev (nx*ny*nz doubles, grid order) and field_dev (the same size, written); seeds are host
+ * slowness_dev (nx*ny*nz doubles, grid order) and field_dev (the same size, written), both device memory
+ * of the calling thread's current device (anything else is refused with TS_E_ARG); seeds are host
  * arrays as in ts_eik_solve. The function allocates no device memory: its working memory (due and
  * fixed-node flags, axis weights, seeds, the round flag) is one static __device__ array of about
  * 13 MB that every GPU which loads the library holds until the process exits. Limits: uniform grids
  * (depth_km NULL), nx*ny*nz <= TS_NOALLOC_MAX_NODES, ny*nz <= TS_NOALLOC_MAX_ROWS,
  * nz <= TS_NOALLOC_MAX_LEVELS, at most TS_NOALLOC_MAX_SEEDS distinct seed nodes; larger inputs
- * return TS_E_CAPACITY. The first call on a device looks up the array's address
- * (cudaGetSymbolAddress) with that device current; make that first call before any stream capture.
+ * return TS_E_CAPACITY. Every call looks up the array's address (cudaGetSymbolAddress) on the current
+ * device, so a device reset leaves no stale address behind; the first call on a device is also where
+ * the library's device code is loaded there: make that first call before any stream capture.
  * All calls share the one array, so calls that overlap on the GPU (other host threads, other
  * streams) race: serialise them. The result equals SphericalEikonal.Relax to the bit (the reference
  * scheme, one launch per diagonal plane, on `stream`, NULL for the default stream). rounds_out[2]

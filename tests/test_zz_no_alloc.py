@@ -22,7 +22,9 @@ pytestmark = pytest.mark.gpu
 P = C.POINTER
 
 
-def no_alloc_solve(grid, slowness, seeds):
+def no_alloc_solve(grid, slowness, seeds, stream=None):
+    """The caller's buffers are made here (torch), as a caller would bring its own; `stream` is a torch
+    stream the call runs on (its handle passed through the C ABI), None for the default stream."""
     import torch
 
     lib = L.load()
@@ -33,10 +35,13 @@ def no_alloc_solve(grid, slowness, seeds):
     st = np.ascontiguousarray(seeds[1], np.float64)
     gs = grid.struct()
     rounds = np.zeros(2, np.int32)
+    handle = C.c_void_p(stream.cuda_stream) if stream is not None else None
     rc = lib.ts_eik_solve_noalloc(C.byref(gs), C.c_void_p(s_dev.data_ptr()), len(si), si.ctypes.data_as(P(C.c_int32)),
-                                  st.ctypes.data_as(P(C.c_double)), C.c_void_p(out.data_ptr()), 1e-7, 0, None,
+                                  st.ctypes.data_as(P(C.c_double)), C.c_void_p(out.data_ptr()), 1e-7, 0, handle,
                                   rounds.ctypes.data_as(P(C.c_int32)))
     assert rc == L.TS_OK, lib.ts_last_error(None).decode()
+    if stream is not None:
+        stream.synchronize()
     return out.cpu().numpy(), rounds
 
 
@@ -70,3 +75,39 @@ def test_no_alloc_rejects_grids_beyond_its_limit():
                                   st.ctypes.data_as(P(C.c_double)), C.c_void_p(16), 1e-7, 0, None, None)
     assert rc == L.TS_E_CAPACITY
     assert "limits" in lib.ts_last_error(None).decode()
+
+
+def test_no_alloc_merges_seeds_on_a_side_stream(solver):
+    """Duplicate seeds (the smallest time kept) and seeds off the grid (dropped), as TrySolve merges
+    them, on a caller's non-default stream: bitwise against ts_eik_solve on the same seed list."""
+    import torch
+
+    g = GridDef(10.0, 10.2, 42.0, 42.18, -1.0, 11.0, 21, 19, 13)
+    rng = np.random.default_rng(44)
+    s = 1 / (5.2 + rng.uniform(-0.3, 0.3, g.count))
+    si, st = point_source(g, s, 10.07, 42.1, 3.0)
+    si = np.concatenate([si, si[:3], [g.count, g.count + 7, -1]]).astype(np.int32)
+    st = np.concatenate([st, st[:3] - 0.002, [0.0, 0.0, 0.0]])
+    side = torch.cuda.Stream()
+    got, _ = no_alloc_solve(g, s, (si, st), stream=side)
+    want = solver.solve(g, s, [(si, st)], precision=64, mode=L.MODE_PLAIN)[0]
+    assert np.array_equal(got, want)
+
+
+def test_no_alloc_refuses_host_buffers():
+    """Buffers that are not device memory of the current device are refused before any launch."""
+    import torch
+
+    torch.cuda.init()
+    lib = L.load()
+    g = GridDef(10.0, 10.1, 42.0, 42.1, 0.0, 5.0, 9, 9, 6)
+    host_s = np.full(g.count, 0.2)
+    host_out = np.empty(g.count)
+    si = np.array([40], np.int32)
+    st = np.zeros(1)
+    gs = g.struct()
+    rc = lib.ts_eik_solve_noalloc(C.byref(gs), host_s.ctypes.data_as(C.c_void_p), 1, si.ctypes.data_as(P(C.c_int32)),
+                                  st.ctypes.data_as(P(C.c_double)), host_out.ctypes.data_as(C.c_void_p), 1e-7, 0,
+                                  None, None)
+    assert rc == L.TS_E_ARG
+    assert "device memory" in lib.ts_last_error(None).decode()

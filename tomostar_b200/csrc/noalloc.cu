@@ -14,7 +14,6 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -44,17 +43,10 @@ constexpr size_t kScratchBytes = kOffFlags + 256;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// The scratch array's device address, looked up once per device (with that device current).
-std::mutex g_mu;
-std::map<int, unsigned char*> g_addr;
-
-int scratch_address(int device, unsigned char** out) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    auto it = g_addr.find(device);
-    if (it != g_addr.end()) {
-        *out = it->second;
-        return TS_OK;
-    }
+// The scratch array's device address on the current device. Looked up on every call (a host-side
+// query, cheap next to a solve): an address kept from an earlier call would be stale after the
+// device's primary context was reset and the library's device code loaded again.
+int scratch_address(unsigned char** out) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) {
@@ -62,9 +54,19 @@ int scratch_address(int device, unsigned char** out) {
         ts_thread_error() = std::string("cudaGetSymbolAddress of the scratch array: ") + cudaGetErrorString(e);
         return TS_E_CUDA;
     }
-    g_addr[device] = static_cast<unsigned char*>(p);
     *out = static_cast<unsigned char*>(p);
     return TS_OK;
+}
+
+// True when p is device (or managed) memory of `device`: a kernel given a host pointer or another
+// GPU's buffer would touch memory it cannot or must not address.
+bool on_device(const void* p, int device) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
 }
 
 __global__ void fill_f64(double* __restrict__ p, double v, int64_t n) {
@@ -115,8 +117,11 @@ int solve(const ts_grid* grid, const double* slowness_dev, int n_seeds, const in
         return fail(TS_E_CAPACITY, "more than " + std::to_string(kMaxSeeds) + " seed nodes");
     int device = 0;
     NA_TRY(cudaGetDevice(&device));
+    if (!on_device(slowness_dev, device) || !on_device(field_dev, device))
+        return fail(TS_E_ARG, "slowness_dev and field_dev must be device memory of the current device (" +
+                                  std::to_string(device) + ")");
     unsigned char* base = nullptr;
-    if (int rc = scratch_address(device, &base)) return rc;
+    if (int rc = scratch_address(&base)) return rc;
     uint8_t* fixed = base + kOffFixed;
     uint8_t* due = base + kOffDue;
     double* wx = reinterpret_cast<double*>(base + kOffWx);
