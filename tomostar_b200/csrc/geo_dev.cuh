@@ -135,6 +135,79 @@ TS_DEVINL void table_gradient(const RGrid& g, const float* tb, double lon, doubl
     gz = tz / hz;
 }
 
+// ---- the same Time and Gradient with every corner load issued before any is used ----------------
+//
+// time_fractional above loads a corner only where its weight is non-zero and stops at the first
+// non-finite one, so each load waits on the previous one's test. The forms below compute the base
+// corner first, load all eight corners of every evaluation (they lie on the grid: the base is
+// clamped to n − 2 on each axis), and then sum in the reference's order with the same skips and the
+// same +inf rule: the same values, with the loads of one step in flight together.
+
+// Base corner of the evaluation at (fx, fy, fz) (clamped as weights() clamps).
+TS_DEVINL int64_t corner_base(const RGrid& g, double fx, double fy, double fz) {
+    fx = fmin(fmax(fx, 0.0), double(g.nx - 1));
+    fy = fmin(fmax(fy, 0.0), double(g.ny - 1));
+    fz = fmin(fmax(fz, 0.0), double(g.nz - 1));
+    const int i0 = min(int(fx), g.nx - 2), j0 = min(int(fy), g.ny - 2), k0 = min(int(fz), g.nz - 2);
+    return int64_t(k0) * g.nx * g.ny + int64_t(j0) * g.nx + i0;
+}
+
+TS_DEVINL void load_corners(const RGrid& g, const float* __restrict__ tb, int64_t base, float* v) {
+    const int64_t nxy = int64_t(g.nx) * g.ny;
+#pragma unroll
+    for (int n = 0; n < 8; n++) v[n] = __ldg(&tb[base + (n >> 2) * nxy + ((n >> 1) & 1) * g.nx + (n & 1)]);
+}
+
+// TimeFractional from loaded corners.
+TS_DEVINL double sum_corners(const RGrid& g, double fx, double fy, double fz, const float* v) {
+    int i0, j0, k0;
+    double w[8];
+    weights(g, fx, fy, fz, i0, j0, k0, w);
+    double t = 0;
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+        if (w[n] != 0) {
+            if (!isfinite(v[n])) return dinf();
+            t += double(v[n]) * w[n];
+        }
+    }
+    return t;
+}
+
+TS_DEVINL double table_time_b(const RGrid& g, const float* tb, double lon, double lat, double dep) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    float v[8];
+    load_corners(g, tb, corner_base(g, fx, fy, fz), v);
+    return sum_corners(g, fx, fy, fz, v);
+}
+
+// Gradient: the six evaluations' 48 corners loaded together.
+TS_DEVINL void table_gradient_b(const RGrid& g, const float* tb, double lon, double lat, double dep, double& ge,
+                                double& gn, double& gz) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    const double d = 0.5;
+    float v[6][8];
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+        const double ex = e == 0 ? fx + d : e == 1 ? fx - d : fx;
+        const double ey = e == 2 ? fy + d : e == 3 ? fy - d : fy;
+        const double ez = e == 4 ? fz + d : e == 5 ? fz - d : fz;
+        load_corners(g, tb, corner_base(g, ex, ey, ez), v[e]);
+    }
+    const double tx = (sum_corners(g, fx + d, fy, fz, v[0]) - sum_corners(g, fx - d, fy, fz, v[1])) / (2 * d);
+    const double ty = (sum_corners(g, fx, fy + d, fz, v[2]) - sum_corners(g, fx, fy - d, fz, v[3])) / (2 * d);
+    const double tz = (sum_corners(g, fx, fy, fz + d, v[4]) - sum_corners(g, fx, fy, fz - d, v[5])) / (2 * d);
+    double r = kEarthRadiusKm - dep;
+    double hx = r * cos(lat * kDeg2Rad) * g.dlon_rad;
+    double hy = r * g.dlat_rad;
+    double hz = g.ddep;
+    ge = tx / hx;
+    gn = ty / hy;
+    gz = tz / hz;
+}
+
 // SphericalGrid.Contains (Geo/SphericalGrid.cs:186-192).
 TS_DEVINL bool contains(const RGrid& g, double lon, double lat, double dep, double tol) {
     double fx, fy, fz;

@@ -1,18 +1,25 @@
 // Rays and Jacobian rows on the device: RayTracing.Backtrack (Forward/RayTracing.cs:73-111),
 // RayTracing.Kernel (:118-159) and RayKernels' row finalisation (Tomography/RayKernels.cs:79-97).
 //
-// Three kernels per chunk of rays, none with atomics:
+// Rays are taken in order of their table (so that a table's float32 nodes stay in L2 while its rays
+// are traced) in chunks sized by a record budget; each ray's record room is its own estimate.
+// Kernels, none with atomics:
 //   trace_kernel  one thread per ray: steepest descent on the station's float32 table, each new
 //                 polyline segment integrated at once against the trilinear basis of the inversion
 //                 grid. Pieces falling in the same inversion cell are summed before a record
 //                 (node, length) is written, so a ray writes about one record per node per cell.
+//                 A step's gradient loads its six evaluations' 48 corners together (one memory
+//                 latency instead of six dependent ones).
 //   merge_kernel  one warp per ray: sorts the ray's records by node (bitonic, shared memory, the
 //                 record index breaking ties so equal nodes keep visit order), sums each node's
 //                 lengths in that order and writes the unique nodes ascending, lengths as float32.
-//   emit_kernel   one warp per ray: copies the row into the CSR arrays at its scanned offset.
+//   stage_kernel  one warp per ray: appends the chunk's rows to a staging area (chunk order).
+//   emit_kernel   one warp per ray: copies every row from the staging area into the CSR arrays at
+//                 its offset in arrival order, once all chunks are traced.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "ctx.h"
@@ -38,12 +45,14 @@ struct TraceArgs {
     const double* table_station;  // 3 per table
     const int* table_of;          // per ray
     const double* events;         // 3 per ray
-    int ray0, nrays;
+    const int* ray_of;            // global ray index of each chunk slot
+    int nrays;                    // chunk slots
     double step_km, piece_km;
-    int cap;
-    int* rec_node;                // [nrays * cap]
+    const int64_t* rec_base;      // per chunk slot: first record of its room
+    const int* rec_cap;           // per chunk slot: records it may write
+    int* rec_node;                // the chunk's records
     double* rec_val;
-    int* rec_count;               // per chunk ray
+    int* rec_count;               // per chunk slot
     double* tcg;                  // 4 per ray (global index)
     double* outside;              // per ray (global index): time outside the inversion grid
     int bg_n;                     // > 0: the extended domain's background (depths, Vp, Vs at bg)
@@ -65,15 +74,16 @@ struct Recorder {
         if (ci < 0 || !touched) return;
         const int nx = a.inv.nx;
         const int64_t nxy = int64_t(a.inv.nx) * a.inv.ny;
+        const int cap = a.rec_cap[r];
 #pragma unroll
         for (int n = 0; n < 8; n++) {
             if (!((touched >> n) & 1u)) continue;
-            if (count >= a.cap) {
+            if (count >= cap) {
                 overflow = true;
                 continue;
             }
             int di = n & 1, dj = (n >> 1) & 1, dk = n >> 2;
-            int64_t slot = int64_t(r) * a.cap + count;
+            int64_t slot = a.rec_base[r] + count;
             a.rec_node[slot] = int((ck + dk) * nxy + int64_t(cj + dj) * nx + (ci + di));
             a.rec_val[slot] = acc[n];
             count++;
@@ -122,7 +132,7 @@ struct Recorder {
 __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.nrays) return;
-    const int ray = a.ray0 + r;
+    const int ray = a.ray_of[r];
     const int tab = a.table_of[ray];
     const float* tb = a.table_ptr ? a.table_ptr[tab] : a.tables + int64_t(tab) * a.table_n;
     const RGrid& g = a.fwd;
@@ -135,13 +145,13 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     // Backtrack (RayTracing.cs:75-110).
     V3 station = geo::to_cartesian(st_lon, st_lat, st_dep);
     V3 p = geo::to_cartesian(ev.lon, ev.lat, ev.dep);
-    double t0 = geo::table_time(g, tb, ev.lon, ev.lat, ev.dep);
+    double t0 = geo::table_time_b(g, tb, ev.lon, ev.lat, ev.dep);
     tcg[0] = t0;
     if (!isfinite(t0)) {
         a.rec_count[r] = kDropped;
         return;
     }
-    geo::table_gradient(g, tb, ev.lon, ev.lat, ev.dep, tcg[1], tcg[2], tcg[3]);
+    geo::table_gradient_b(g, tb, ev.lon, ev.lat, ev.dep, tcg[1], tcg[2], tcg[3]);
     const double step = a.step_km;
     const int max_steps = 20 * int(ceil(geo::norm(geo::sub(p, station)) / step + 10));
     double last_t = t0;
@@ -153,7 +163,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
         if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
         GeoPt gp = geo::from_cartesian(p);
         double ge, gn, gz;
-        geo::table_gradient(g, tb, gp.lon, gp.lat, gp.dep, ge, gn, gz);
+        geo::table_gradient_b(g, tb, gp.lon, gp.lat, gp.dep, ge, gn, gz);
         if (!isfinite(ge) || !isfinite(gn) || !isfinite(gz)) {
             a.rec_count[r] = kDropped;
             return;
@@ -177,7 +187,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
         p = geo::to_cartesian(q.lon, q.lat, q.dep);
         rec.segment(a, r, prev, q);
         prev = q;
-        double t = geo::table_time(g, tb, q.lon, q.lat, q.dep);
+        double t = geo::table_time_b(g, tb, q.lon, q.lat, q.dep);
         if (!(t < last_t)) {
             if (++stalls > 20) {
                 a.rec_count[r] = kDropped;
@@ -199,8 +209,9 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
 // A pass handles the rays with lo < records <= P; the first pass (lo = 0) also writes the empty
 // and dropped rows and marks the rays left for a larger pass.
 __global__ void merge_kernel(const int* __restrict__ rec_node, const double* __restrict__ rec_val,
-                             const int* __restrict__ rec_count, int cap, int nrays, int P, int lo,
-                             int* __restrict__ out_node, float* __restrict__ out_len, int* __restrict__ nnz) {
+                             const int* __restrict__ rec_count, const int64_t* __restrict__ rec_base, int nrays,
+                             int P, int lo, int* __restrict__ out_node, float* __restrict__ out_len,
+                             int* __restrict__ nnz) {
     extern __shared__ unsigned long long keys_all[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     unsigned long long* keys = keys_all + size_t(warp) * P;
@@ -216,7 +227,7 @@ __global__ void merge_kernel(const int* __restrict__ rec_node, const double* __r
         }
         int n2 = 32;
         while (n2 < c) n2 <<= 1;
-        const int64_t base = int64_t(r) * cap;
+        const int64_t base = rec_base[r];
         for (int q = lane; q < n2; q += 32)
             keys[q] = q < c ? (static_cast<unsigned long long>(unsigned(rec_node[base + q])) << 32) | unsigned(q)
                             : ~0ull;
@@ -300,21 +311,46 @@ __global__ void scan_kernel(const int* __restrict__ nnz, int n, int* __restrict_
     }
 }
 
-__global__ void emit_kernel(const int* __restrict__ out_node, const float* __restrict__ out_len,
-                            const int* __restrict__ nnz, const int* __restrict__ off, int cap, int nrays, int ray0,
-                            long long base, int* __restrict__ row_ptr, int* __restrict__ col, float* __restrict__ len,
-                            uint8_t* __restrict__ ok) {
+// A chunk's merged rows appended to the staging area at stage0 + their scanned offsets; each ray's
+// place and size recorded under its global index.
+__global__ void stage_kernel(const int* __restrict__ out_node, const float* __restrict__ out_len,
+                             const int* __restrict__ nnz, const int* __restrict__ off,
+                             const int64_t* __restrict__ rec_base, const int* __restrict__ ray_of, int nrays,
+                             long long stage0, int* __restrict__ stage_col, float* __restrict__ stage_len,
+                             long long* __restrict__ stage_off, int* __restrict__ ray_nnz) {
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nrays; r += gridDim.x * wpb) {
-        int c = nnz[r];
-        long long o = base + off[r];
+        const int c = nnz[r];
+        const long long o = stage0 + off[r];
         if (lane == 0) {
-            row_ptr[ray0 + r] = int(o);
-            ok[ray0 + r] = c >= 0 ? 1 : 0;
+            stage_off[ray_of[r]] = o;
+            ray_nnz[ray_of[r]] = c;
         }
+        const int64_t b = rec_base[r];
         for (int q = lane; q < c; q += 32) {
-            col[o + q] = out_node[int64_t(r) * cap + q];
-            len[o + q] = out_len[int64_t(r) * cap + q];
+            stage_col[o + q] = out_node[b + q];
+            stage_len[o + q] = out_len[b + q];
+        }
+    }
+}
+
+// Every row from the staging area into the CSR arrays in arrival order (row_ptr from the scan).
+__global__ void emit_kernel(const int* __restrict__ stage_col, const float* __restrict__ stage_len,
+                            const long long* __restrict__ stage_off, const int* __restrict__ ray_nnz,
+                            const int* __restrict__ off, int nrays, int* __restrict__ row_ptr,
+                            int* __restrict__ col, float* __restrict__ len, uint8_t* __restrict__ ok) {
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nrays; r += gridDim.x * wpb) {
+        const int c = ray_nnz[r];
+        const long long o = off[r];
+        if (lane == 0) {
+            row_ptr[r] = int(o);
+            ok[r] = c >= 0 ? 1 : 0;
+        }
+        const long long s = stage_off[r];
+        for (int q = lane; q < c; q += 32) {
+            col[o + q] = stage_col[s + q];
+            len[o + q] = stage_len[s + q];
         }
     }
 }
@@ -369,13 +405,12 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
         if (table_of_host[a] < 0 || table_of_host[a] >= n_tables) return ctx->fail(TS_E_ARG, "table_of out of range");
     if (!(step_km > 0)) return ctx->fail(TS_E_ARG, "step must be positive");
     if (fwd.variable || inv.variable) return ctx->fail(TS_E_ARG, "rays need uniform grids");
-    auto rows = new ts_rows();
+    // The result is freed on every early return; handed to the caller at the end.
+    std::unique_ptr<ts_rows> rows_own(new ts_rows());
+    ts_rows* rows = rows_own.get();
     rows->ctx = ctx;
     rows->n_rows = n_rays;
-    auto bail = [&](int code) {
-        delete rows;
-        return code;
-    };
+    auto bail = [&](int code) { return code; };
     if (cudaMallocAsync(reinterpret_cast<void**>(&rows->row_ptr), sizeof(int) * (n_rays + 1), s) != cudaSuccess ||
         cudaMallocAsync(reinterpret_cast<void**>(&rows->tcg), sizeof(double) * 4 * std::max(1, n_rays), s) != cudaSuccess ||
         cudaMallocAsync(reinterpret_cast<void**>(&rows->ok), std::max(1, n_rays), s) != cudaSuccess ||
@@ -422,39 +457,89 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_phase, phases.data(), sizeof(int) * phases.size(), cudaMemcpyHostToDevice, s));
     a.table_phase = d_phase;
 
-    // Record capacity: one record per node per inversion cell crossed, with room for a path
-    // three times the straight length; a ray that needs more is traced again with more room.
-    const int CH = 16384;
-    int64_t csr_cap = 0;
-    int64_t total = 0;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, s);
-    for (int ray0 = 0; ray0 < n_rays; ray0 += CH) {
-        const int nr = std::min(CH, n_rays - ray0);
-        double maxd = 0;
-        for (int q = ray0; q < ray0 + nr; q++) {
-            const double* ev = events_host + 3 * q;
-            const double* stn = table_station_host + 3 * table_of_host[q];
-            host::V3 A = host::to_cartesian(ev[0], ev[1], ev[2]);
-            host::V3 B = host::to_cartesian(stn[0], stn[1], stn[2]);
-            maxd = std::max(maxd, host::dist(A, B));
+    // Record room per ray: one record per node per inversion cell crossed, with room for a path
+    // three times the straight length; a ray that needs more is traced again with four times the room.
+    constexpr int kMaxCap = 16384;  // the larger merge pass sorts up to this many in 128 KB
+    std::vector<int> cap_of(std::max(1, n_rays));
+    for (int q = 0; q < n_rays; q++) {
+        const double* ev = events_host + 3 * q;
+        const double* stn = table_station_host + 3 * table_of_host[q];
+        const double d = host::dist(host::to_cartesian(ev[0], ev[1], ev[2]), host::to_cartesian(stn[0], stn[1], stn[2]));
+        cap_of[q] = int(std::min(double(kMaxCap), 8.0 * (3.0 * d / a.piece_km + 32)));
+    }
+    // Rays in order of their table: a chunk's rays read few tables, which stay in L2.
+    std::vector<int> order(n_rays);
+    for (int q = 0; q < n_rays; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table_of_host[x] < table_of_host[y]; });
+    // Chunk budget: record slots (12 B of record + 8 B of merged output each) within a share of the
+    // free device memory, at most 8 GB of records.
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    cudaGetLastError();
+    const int64_t budget = std::max<int64_t>(int64_t(kMaxCap) * 64,
+                                             std::min<int64_t>(int64_t(400) << 20, int64_t(free_b / 4 / 20)));
+    TS_BUF(ctx, ray_nnz, int, "rays.ray_nnz", std::max(1, n_rays));
+    TS_BUF(ctx, stage_off, long long, "rays.stage_off", std::max(1, n_rays));
+    // The staging area (rows in chunk order), freed on every return.
+    struct Stage {
+        cudaStream_t s;
+        int* col = nullptr;
+        float* len = nullptr;
+        void free() {
+            if (col) cudaFreeAsync(col, s);
+            if (len) cudaFreeAsync(len, s);
+            col = nullptr;
+            len = nullptr;
         }
-        constexpr int kMaxCap = 16384;  // the larger merge pass sorts up to this many in 128 KB
-        int cap = int(std::min(double(kMaxCap), 8.0 * (3.0 * maxd / a.piece_km + 32)));
-        for (int attempt = 0;; attempt++) {
-            a.ray0 = ray0;
-            a.nrays = nr;
-            a.cap = cap;
-            TS_BUF(ctx, rec_node, int, "rays.rec_node", size_t(nr) * cap);
-            TS_BUF(ctx, rec_val, double, "rays.rec_val", size_t(nr) * cap);
+        ~Stage() { free(); }
+    } stage{s};
+    int*& stage_col = stage.col;
+    float*& stage_len = stage.len;
+    int64_t stage_cap = 0, stage_used = 0;
+    auto free_stage = [&]() { stage.free(); };
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
+    cudaEventRecord(e0, s);
+    std::vector<int> pending = order;
+    for (int pass = 0; !pending.empty(); pass++) {
+        std::vector<int> retry;
+        for (size_t c0 = 0; c0 < pending.size();) {
+            // The chunk: rays from c0 while their rooms fit the budget.
+            std::vector<int> ray_of;
+            std::vector<int64_t> base;
+            std::vector<int> caps;
+            int64_t used = 0;
+            int maxcap = 32;
+            size_t c1 = c0;
+            while (c1 < pending.size() && (ray_of.empty() || used + cap_of[pending[c1]] <= budget) &&
+                   ray_of.size() < (size_t(1) << 20)) {
+                const int q = pending[c1++];
+                ray_of.push_back(q);
+                base.push_back(used);
+                caps.push_back(cap_of[q]);
+                used += cap_of[q];
+                maxcap = std::max(maxcap, cap_of[q]);
+            }
+            c0 = c1;
+            const int nr = int(ray_of.size());
+            TS_BUF(ctx, d_ray_of, int, "rays.ray_of", nr);
+            TS_BUF(ctx, d_base, int64_t, "rays.rec_base", nr);
+            TS_BUF(ctx, d_cap, int, "rays.rec_cap", nr);
+            TS_BUF(ctx, rec_node, int, "rays.rec_node", size_t(used));
+            TS_BUF(ctx, rec_val, double, "rays.rec_val", size_t(used));
             TS_BUF(ctx, rec_count, int, "rays.rec_count", nr);
-            TS_BUF(ctx, out_node, int, "rays.out_node", size_t(nr) * cap);
-            TS_BUF(ctx, out_len, float, "rays.out_len", size_t(nr) * cap);
+            TS_BUF(ctx, out_node, int, "rays.out_node", size_t(used));
+            TS_BUF(ctx, out_len, float, "rays.out_len", size_t(used));
             TS_BUF(ctx, nnz, int, "rays.nnz", nr);
             TS_BUF(ctx, off, int, "rays.off", nr);
             TS_BUF(ctx, sums, long long, "rays.sums", 2);
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ray_of, ray_of.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_base, base.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice, s));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_cap, caps.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+            a.ray_of = d_ray_of;
+            a.nrays = nr;
+            a.rec_base = d_base;
+            a.rec_cap = d_cap;
             a.rec_node = rec_node;
             a.rec_val = rec_val;
             a.rec_count = rec_count;
@@ -463,15 +548,15 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
             // Small sort size for most rays; the rest in a second pass with one warp per block.
             const int Psmall = 2048, W = 4;
             int Pbig = Psmall;
-            while (Pbig < cap) Pbig <<= 1;
+            while (Pbig < maxcap) Pbig <<= 1;
             TS_CUDA_TRY(ctx, cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   std::max(W * Psmall, Pbig) * 8));
             merge_kernel<<<std::min((nr + W - 1) / W, ctx->sm_count * 8), W * 32, size_t(W) * Psmall * 8, s>>>(
-                rec_node, rec_val, rec_count, cap, nr, Psmall, 0, out_node, out_len, nnz);
+                rec_node, rec_val, rec_count, d_base, nr, Psmall, 0, out_node, out_len, nnz);
             TS_CUDA_TRY(ctx, cudaGetLastError());
             if (Pbig > Psmall) {
                 merge_kernel<<<std::min(nr, ctx->sm_count * 2), 32, size_t(Pbig) * 8, s>>>(
-                    rec_node, rec_val, rec_count, cap, nr, Pbig, Psmall, out_node, out_len, nnz);
+                    rec_node, rec_val, rec_count, d_base, nr, Pbig, Psmall, out_node, out_len, nnz);
                 TS_CUDA_TRY(ctx, cudaGetLastError());
             }
             scan_kernel<<<1, 1024, 0, s>>>(nnz, nr, off, sums);
@@ -479,51 +564,85 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
             TS_CUDA_TRY(ctx, cudaMemcpyAsync(h_sums, sums, sizeof h_sums, cudaMemcpyDeviceToHost, s));
             TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
             if (h_sums[1] > 0) {
-                if (cap >= kMaxCap) return bail(ctx->fail(TS_E_CAPACITY, "a ray needs more records than supported"));
-                cap = std::min(kMaxCap, cap * 4);
+                // Rays that ran out of room: traced again later with four times the room.
+                std::vector<int> hn(nr);
+                TS_CUDA_TRY(ctx, cudaMemcpy(hn.data(), nnz, sizeof(int) * nr, cudaMemcpyDeviceToHost));
+                for (int r = 0; r < nr; r++) {
+                    if (hn[r] != kOverflow) continue;
+                    const int q = ray_of[r];
+                    if (cap_of[q] >= kMaxCap) {
+                        free_stage();
+                        return bail(ctx->fail(TS_E_CAPACITY, "a ray needs more records than supported"));
+                    }
+                    cap_of[q] = std::min(kMaxCap, cap_of[q] * 4);
+                    retry.push_back(q);
+                }
                 if (st) st->retraced_chunks++;
-                continue;
             }
-            if (total + h_sums[0] > INT32_MAX) return bail(ctx->fail(TS_E_CAPACITY, "more than 2^31 non-zeros"));
-            if (total + h_sums[0] > csr_cap) {
-                int64_t want = std::max<int64_t>(total + h_sums[0], csr_cap * 2);
-                want = std::max<int64_t>(want, 1024);
+            if (stage_used + h_sums[0] > stage_cap) {
+                const int64_t want = std::max<int64_t>({stage_used + h_sums[0], stage_cap * 2, 1024});
                 int* ncol = nullptr;
                 float* nlen = nullptr;
                 if (cudaMallocAsync(reinterpret_cast<void**>(&ncol), sizeof(int) * want, s) != cudaSuccess ||
                     cudaMallocAsync(reinterpret_cast<void**>(&nlen), sizeof(float) * want, s) != cudaSuccess) {
                     cudaGetLastError();
                     if (ncol) cudaFreeAsync(ncol, s);
-                    return bail(ctx->fail(TS_E_NOMEM, "CSR arrays"));
+                    free_stage();
+                    return bail(ctx->fail(TS_E_NOMEM, "row staging arrays"));
                 }
-                if (total > 0) {
-                    cudaMemcpyAsync(ncol, rows->col, sizeof(int) * total, cudaMemcpyDeviceToDevice, s);
-                    cudaMemcpyAsync(nlen, rows->len, sizeof(float) * total, cudaMemcpyDeviceToDevice, s);
+                if (stage_used > 0) {
+                    cudaMemcpyAsync(ncol, stage_col, sizeof(int) * stage_used, cudaMemcpyDeviceToDevice, s);
+                    cudaMemcpyAsync(nlen, stage_len, sizeof(float) * stage_used, cudaMemcpyDeviceToDevice, s);
                 }
-                if (rows->col) cudaFreeAsync(rows->col, s);
-                if (rows->len) cudaFreeAsync(rows->len, s);
-                rows->col = ncol;
-                rows->len = nlen;
-                csr_cap = want;
+                free_stage();
+                stage_col = ncol;
+                stage_len = nlen;
+                stage_cap = want;
             }
-            emit_kernel<<<std::min((nr + 7) / 8, ctx->sm_count * 16), 256, 0, s>>>(
-                out_node, out_len, nnz, off, cap, nr, ray0, total, rows->row_ptr, rows->col, rows->len, rows->ok);
+            stage_kernel<<<std::min((nr + 7) / 8, ctx->sm_count * 16), 256, 0, s>>>(
+                out_node, out_len, nnz, off, d_base, d_ray_of, nr, stage_used, stage_col, stage_len, stage_off,
+                ray_nnz);
             TS_CUDA_TRY(ctx, cudaGetLastError());
-            total += h_sums[0];
-            break;
+            stage_used += h_sums[0];
         }
+        pending.swap(retry);
     }
+    // Rows in arrival order: offsets of every ray's row, then the copy into the CSR arrays.
+    int64_t total = 0;
+    if (n_rays > 0) {
+        TS_BUF(ctx, off_all, int, "rays.off_all", n_rays);
+        TS_BUF(ctx, sums_all, long long, "rays.sums_all", 2);
+        scan_kernel<<<1, 1024, 0, s>>>(ray_nnz, n_rays, off_all, sums_all);
+        long long h[2] = {0, 0};
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(h, sums_all, sizeof h, cudaMemcpyDeviceToHost, s));
+        TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        total = h[0];
+        if (total > INT32_MAX) {
+            free_stage();
+            return bail(ctx->fail(TS_E_CAPACITY, "more than 2^31 non-zeros"));
+        }
+        const int64_t alloc = std::max<int64_t>(1, total);
+        if (cudaMallocAsync(reinterpret_cast<void**>(&rows->col), sizeof(int) * alloc, s) != cudaSuccess ||
+            cudaMallocAsync(reinterpret_cast<void**>(&rows->len), sizeof(float) * alloc, s) != cudaSuccess) {
+            cudaGetLastError();
+            free_stage();
+            return bail(ctx->fail(TS_E_NOMEM, "CSR arrays"));
+        }
+        emit_kernel<<<std::min((n_rays + 7) / 8, ctx->sm_count * 16), 256, 0, s>>>(
+            stage_col, stage_len, stage_off, ray_nnz, off_all, n_rays, rows->row_ptr, rows->col, rows->len,
+            rows->ok);
+        TS_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    free_stage();
     int tot32 = int(total);
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(rows->row_ptr + n_rays, &tot32, sizeof(int), cudaMemcpyHostToDevice, s));
     cudaEventRecord(e1, s);
     TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     rows->nnz = total;
     if (st) st->device_ms += ms;
-    *out = rows;
+    *out = rows_own.release();
     return TS_OK;
 }
 
