@@ -728,7 +728,7 @@ def run_ours(args, problem_fn):
 
         serving = serve_run(seconds=args.serve_seconds, rate=200.0, tile=args.serve_tile,
                             rounds_per_epoch=args.serve_rounds, budget_bytes=120e9, device=local,
-                            scheduler=args.serve_scheduler)
+                            scheduler=args.serve_scheduler, epoch_ms=args.serve_epoch_ms)
 
     if rank == 0:
         line = {
@@ -794,6 +794,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-tile", type=int, default=2)
     ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
+    ap.add_argument("--serve-epoch-ms", type=float, default=0.0,
+                    help="flow scheduler: fields pause at their next round end after this long (0: off)")
     ap.add_argument("--dims", default="401,401,121",
                     help="grid of the regional job (smaller only for profiling captures; the bench line is 401,401,121)")
     args = ap.parse_args()

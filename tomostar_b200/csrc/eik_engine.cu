@@ -16,7 +16,8 @@ const std::vector<TileShapeInfo>& tile_shapes() {
     // 6 is 4 with room for 170 registers instead of 128: 12 warps per SM and the FP64 sweep
     // orderings specialised).
     static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4},
-                                                      {4, 32, 8, 4}, {5, 64, 8, 4}, {6, 32, 8, 4}};
+                                                      {4, 32, 8, 4}, {5, 64, 8, 4}, {6, 32, 8, 4},
+                                                      {7, 32, 8, 4}, {8, 32, 8, 4}};
     return shapes;
 }
 
@@ -82,7 +83,7 @@ __global__ void dense_convert_kernel(const From* __restrict__ a, int64_t field_s
     }
 }
 
-template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool PENCIL = false>
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool PENCIL = false, int OPT = 0>
 int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const std::vector<const host::Metric*>& metrics,
                  const std::vector<EngineField*>& fl, double tol, double wake_rel, int max_rounds, ts_eik_stats* stats,
                  cudaStream_t s) {
@@ -365,10 +366,10 @@ int launch_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids, const
     args.wake_rel = Real(wake_rel);
     args.causal = wake_rel > 0 ? 1 : 0;  // fast mode: threshold and causal wakes together
     const int smem = PENCIL ? WARPS * PencilSmem<Real, BX>::kBytes : engine_smem_bytes<Real, S>(WARPS);
-    void* kfn = flow ? (any_var ? (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
-                               : (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>)
-                     : (any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL>
-                                : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL>);
+    void* kfn = flow ? (any_var ? (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL, OPT>
+                               : (void*)flow_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL, OPT>)
+                     : (any_var ? (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, true, PENCIL, OPT>
+                                : (void*)engine_kernel<Real, BX, BY, BZ, WARPS, MINB, false, PENCIL, OPT>);
     TS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
     TS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, WARPS * 32, smem));
@@ -565,6 +566,10 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
         case 4: return launch_epoch<Real, 32, 8, 4, 4, 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 5: return launch_epoch<Real, 64, 8, 4, 4, F64 ? 2 : 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 6: return launch_epoch<Real, 32, 8, 4, 4, F64 ? 3 : 4, true>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        // 7, 8: 32-wide pencils at 16 warps per SM (128 registers), two-deep prefetch, weights read
+        // where used; 8 with the sweep ordering fixed at compile time.
+        case 7: return launch_epoch<Real, 32, 8, 4, 4, 4, true, kRing2 | kLazyW>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
+        case 8: return launch_epoch<Real, 32, 8, 4, 4, 4, true, kRing2 | kLazyW | kSpecAll>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         default: return launch_epoch<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
     }
 }

@@ -10,7 +10,7 @@ namespace eik {
 
 // PENCIL: BX×8×4 tiles swept by process_pencil (one lane per row); otherwise cube tiles swept by
 // process_tile (node planes with a plane table).
-template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool VARZ_ANY, bool PENCIL>
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool VARZ_ANY, bool PENCIL, int OPT = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) {
     using S = Shape<Real, BX, BY, BZ>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) engine_kernel(Args<Real> a) 
                         if constexpr (PENCIL) {
                             Real* halo = reinterpret_cast<Real*>(mine);
                             if (VARZ_ANY && g.varz)
-                                ev = visit_pencil<Real, BX, true, (BX == 64 || MINB <= 3)>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, true, (BX == 64 || MINB <= 3 || (OPT & kSpecAll) != 0), OPT>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                             else
-                                ev = visit_pencil<Real, BX, false, (BX == 64 || MINB <= 3)>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+                                ev = visit_pencil<Real, BX, false, (BX == 64 || MINB <= 3 || (OPT & kSpecAll) != 0), OPT>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
                         } else {
                             if (VARZ_ANY && g.varz)
                                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx,
@@ -373,7 +373,7 @@ static __global__ void flow_queue_init(unsigned long long* seq, unsigned long lo
     for (unsigned long long q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) seq[q] = q;
 }
 
-template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool VARZ_ANY, bool PENCIL>
+template <typename Real, int BX, int BY, int BZ, int WARPS, int MINB, bool VARZ_ANY, bool PENCIL, int OPT = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) flow_kernel(Args<Real> a) {
     using S = Shape<Real, BX, BY, BZ>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -466,8 +466,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) flow_kernel(Args<Real> a) {
             // No per-ordering specialisation here: warps of one launch work on fields at different
             // orderings, and eight copies of the visit would not share the instruction cache.
             Real* halo = reinterpret_cast<Real*>(mine);
-            if (VARZ_ANY && g.varz) ev = visit_pencil<Real, BX, true, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
-            else ev = visit_pencil<Real, BX, false, false>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            if (VARZ_ANY && g.varz) ev = visit_pencil<Real, BX, true, false, OPT>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
+            else ev = visit_pencil<Real, BX, false, false, OPT>(a, g, fd, ff, sx, sy, sz, dir, second, halo, lane);
         } else {
             if (VARZ_ANY && g.varz)
                 ev = process_tile<Real, S, true>(a, g, fd, ff, sx, sy, sz, dir, second, cube, ss, mwx, mwy, mzc,

@@ -40,37 +40,45 @@ TS_DEVINL uint64_t row_reverse(uint64_t m) {
     return uint64_t(__brev(uint32_t(m)));
 }
 
-template <typename Real, int BX, bool VARZ, int SDIR>
+// Variants of the visit (OPT bits): kRing2 — a two-deep prefetch ring instead of four;
+// kLazyW — axis weights read where an update uses them instead of held in registers for the visit.
+// Both only trade registers (the values computed are the same).
+// kSpecAll — the sweep ordering fixed at compile time whatever the width and occupancy (lockstep).
+constexpr int kRing2 = 1, kLazyW = 2, kSpecAll = 4;
+
+template <typename Real, int BX, bool VARZ, int SDIR, int OPT = 0>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane);
 
 // The pencil visit with the sweep ordering specialised where that pays (SPEC): FP64 pencils whose
 // launch leaves room for the extra registers (64-wide pencils, and 32-wide ones at 12 warps per SM),
 // under the lockstep scheduler, where every warp of a step runs the same ordering.
-template <typename Real, int BX, bool VARZ, bool SPEC>
+template <typename Real, int BX, bool VARZ, bool SPEC, int OPT = 0>
 TS_DEVINL int visit_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                            int tz, int dir, bool second, Real* halo, int lane) {
     if constexpr (SPEC && is_f64<Real>()) {
         switch (dir) {
 #define TS_PENCIL_DIR(d) \
-    case d: return process_pencil<Real, BX, VARZ, d>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
+    case d: return process_pencil<Real, BX, VARZ, d, OPT>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
             TS_PENCIL_DIR(0) TS_PENCIL_DIR(1) TS_PENCIL_DIR(2) TS_PENCIL_DIR(3)
             TS_PENCIL_DIR(4) TS_PENCIL_DIR(5) TS_PENCIL_DIR(6) TS_PENCIL_DIR(7)
 #undef TS_PENCIL_DIR
         }
         return 0;
     } else {
-        return process_pencil<Real, BX, VARZ, -1>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
+        return process_pencil<Real, BX, VARZ, -1, OPT>(a, g, fd, f, tx, ty, tz, dir, second, halo, lane);
     }
 }
 
 // SDIR 0..7: the sweep ordering fixed at compile time, so that the mirroring costs nothing in the
 // step loop (used for 64-wide FP64 pencils); −1: read from dir at run time (32-wide pencils, where
 // the specialised code needs more registers than the 128 their occupancy allows, and FP32).
-template <typename Real, int BX, bool VARZ, int SDIR>
+template <typename Real, int BX, bool VARZ, int SDIR, int OPT>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane) {
     static_assert(BX == 32 || BX == 64, "pencil rows are 32 or 64 nodes");
+    constexpr int RING = (OPT & kRing2) ? 2 : 4;  // prefetch depth (steps ahead)
+    constexpr bool LAZYW = (OPT & kLazyW) != 0;
     constexpr int BY = kPencilBY, BZ = kPencilBZ, HX = Layout<Real>::HX;
     constexpr int MWR = BX / 32;           // mask words per row
     constexpr int MW = BX * BY * BZ / 32;  // mask words per tile
@@ -127,7 +135,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     const Real* wxp = static_cast<const Real*>(g.wx);
     const Real* wyp = static_cast<const Real*>(g.wy);
     Real wx1 = Real(1), wx2 = Real(1), wy1 = Real(1), wy2 = Real(1);
-    if (row_on) {
+    if (row_on && !LAZYW) {
         wx1 = ldg_r(&wxp[2 * rowi]);
         wx2 = ldg_r(&wxp[2 * rowi + 1]);
         wy1 = ldg_r(&wyp[2 * gz]);
@@ -175,9 +183,9 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     };
     const int ip0 = -jp - kp;
     Real W0 = ldT(ip0 - 2), W1 = ldT(ip0 - 1), W2 = ldT(ip0), W3 = ldT(ip0 + 1), W4 = ldT(ip0 + 2);
-    Real tr[4], sr[4];
+    Real tr[RING], sr[RING];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < RING; u++) {
         tr[u] = ldT(ip0 + 3 + u);
         sr[u] = ldS(ip0 + u);
     }
@@ -193,10 +201,10 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     unsigned wxh = 0;  // bits 0..3: canonical x = −1, −2, BX, BX+1
     bool big = false;
     int evals = 0;
-    constexpr int NSTEPS = (BX + BY + BZ - 2 + 3) / 4 * 4;
-    for (int p0 = 0; p0 < NSTEPS; p0 += 4) {
+    constexpr int NSTEPS = (BX + BY + BZ - 2 + RING - 1) / RING * RING;
+    for (int p0 = 0; p0 < NSTEPS; p0 += RING) {
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < RING; u++) {
             const int ip = p0 + u + ip0;
             const bool is_due = (due >> (ip & 63)) & (unsigned(ip) < unsigned(BX));
             if (__any_sync(FULL, is_due)) {
@@ -223,6 +231,12 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     const Real xm = mx ? W3 : W1, xp = mx ? W1 : W3, xm2 = mx ? W4 : W0, xp2 = mx ? W0 : W4;
                     const Real ym = my ? ya1 : yb1, yp = my ? yb1 : ya1, ym2 = my ? ya2 : yb2, yp2 = my ? yb2 : ya2;
                     const Real zm = mz ? za1 : zb1, zp = mz ? zb1 : za1, zm2 = mz ? za2 : zb2, zp2 = mz ? zb2 : za2;
+                    if constexpr (LAZYW) {  // due lanes lie on the grid (off-grid rows are fixed)
+                        wx1 = ldg_r(&wxp[2 * rowi]);
+                        wx2 = ldg_r(&wxp[2 * rowi + 1]);
+                        wy1 = ldg_r(&wyp[2 * gz]);
+                        wy2 = ldg_r(&wyp[2 * gz + 1]);
+                    }
                     const Real cand = Update<Real, VARZ>::eval(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
                                                                zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
                     if (cand < W2) {
@@ -277,8 +291,8 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
             W2 = W3;
             W3 = W4;
             W4 = tr[u];
-            tr[u] = ldT(ip + 7);
-            sr[u] = ldS(ip + 4);
+            tr[u] = ldT(ip + 3 + RING);
+            sr[u] = ldS(ip + RING);
         }
     }
 
