@@ -634,7 +634,6 @@ def run_ours(args, problem_fn):
     forward = None
     if world == 1 and not args.no_forward:
         from tomostar_b200 import lsqr
-        from tomostar_b200.rays import _fetch
 
         fsolver = EikonalCuda.create(local, 64)
         lib.ts_engine_set_tile(fsolver.handle, 64, args.tile)
@@ -667,16 +666,31 @@ def run_ours(args, problem_fn):
             lib.ts_rows_free(hx)
         h, fwd_s = forward_call(args.mode)
         fields_s = fstats.device_ms / 1e3
+        fwd_stats = fsolver.last_stats  # the step's timing: tables, then the rays' host and device parts
         # LSQR (Lsqr.Solve) on the rows where they lie: 100 iterations, no early stop (fixed work).
         b = np.random.default_rng(11).standard_normal(len(ar)) * 0.05
         t1 = time.perf_counter()
         lres = lsqr.solve_rows(fsolver, h, p.inv.count, b, damp=0.1, max_iterations=100, atol=0, btol=0, conlim=0)
         lsqr_wall = time.perf_counter() - t1
+        # Rows to pinned host buffers (the host side of RayKernels.Compute's result), then freed.
+        import torch
+
+        n_rows_c, nnz_c = C.c_int32(), C.c_int64()
+        lib.ts_rows_info(h, C.byref(n_rows_c), C.byref(nnz_c))
+        n_rows, nnz = int(n_rows_c.value), int(nnz_c.value)
+        pin = {k: torch.empty(sz, dtype=dt, pin_memory=True)
+               for k, sz, dt in (("rp", n_rows + 1, torch.int32), ("col", max(1, nnz), torch.int32),
+                                 ("len", max(1, nnz), torch.float32), ("tg", 4 * n_rows, torch.float64),
+                                 ("ok", n_rows, torch.uint8))}
         t2 = time.perf_counter()
-        rows = _fetch(h)  # rows to the host, as RayKernels.Compute returns them
+        rc = lib.ts_rows_copy(h, C.cast(pin["rp"].data_ptr(), P(C.c_int32)), C.cast(pin["col"].data_ptr(), P(C.c_int32)),
+                              C.cast(pin["len"].data_ptr(), P(C.c_float)), C.cast(pin["tg"].data_ptr(), P(C.c_double)),
+                              C.cast(pin["ok"].data_ptr(), P(C.c_uint8)))
         copy_s = time.perf_counter() - t2
-        n_rows = int(rows.n_rows)
-        nnz = int(rows.nnz)
+        lib.ts_rows_free(h)
+        if rc:
+            raise SystemExit("row copy failed")
+        kept = int(pin["ok"].numpy().astype(bool).sum())
         # Algorithmic bytes of one LSQR iteration: A·v and Aᵀ·u each read every non-zero's column
         # index and float32 length (4 + 4 B, the rows as the rays leave them) and read and write their
         # output vector.
@@ -688,7 +702,9 @@ def run_ours(args, problem_fn):
                    "rows_per_s": n_rows / (fwd_s + copy_s), "tables_s": fields_s,
                    "rays_and_copy_s": fwd_s - fields_s + copy_s,
                    "rays_rows_per_s": n_rows / max(1e-9, fwd_s - fields_s + copy_s), "nnz": nnz,
-                   "nnz_per_row": nnz / max(1, int(rows.ok.sum())), "kept_rows": int(rows.ok.sum()),
+                   "nnz_per_row": nnz / max(1, kept), "kept_rows": kept,
+                   "copy_s": copy_s, "copy_gbs": (nnz * 8 + n_rows * 45) / copy_s / 1e9,
+                   "timing": fwd_stats,
                    "mode": ("fast" if args.mode == L.MODE_FAST else "engine (bitwise)") +
                            " tables (FP64 fields as float32), rays FP64",
                    "exact_mode": exact,
@@ -697,7 +713,7 @@ def run_ours(args, problem_fn):
                             "achieved_gbs": lsqr_gbs, "hbm_frac": lsqr_gbs / peak,
                             "setup_s": lsqr_wall - lres.device_ms / 1e3,
                             "note": "setup = transpose built on the device from the resident rows, column order as the host transpose"}}
-        del rows
+        del pin
         fsolver.close()
     location = resample = None
     if world == 1 and not args.no_location:

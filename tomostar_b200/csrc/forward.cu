@@ -4,6 +4,8 @@
 // seeds by PointSource at the station, :335/:373), rounded to float32 as TravelTimeTable.Write does
 // (:73), and every arrival is traced on its table (RayKernels.cs:67-107).
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <map>
 #include <vector>
 
@@ -141,19 +143,24 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
                         const int32_t* arr_phase, double step_km, ts_rows** out, ts_eik_stats* stats) {
     host::Grid g(*fwd_def), gi(*inv_def);
     const int64_t n = g.count();
-    // Tables of the (station, phase) pairs in use, ordered by phase then station (TravelTimeTable.cs:319).
-    std::map<std::pair<int, int>, int> table_id;
+    const auto t_begin = std::chrono::steady_clock::now();
+    // Tables of the (station, phase) pairs in use, ordered by phase then station (TravelTimeTable.cs:319):
+    // table_id[phase * n_stations + station], -1 where unused.
+    std::vector<int> table_id(size_t(n_phases) * std::max(1, n_stations), -1);
     for (int a = 0; a < n_arr; a++) {
         if (arr_event[a] < 0 || arr_event[a] >= n_events || arr_station[a] < 0 || arr_station[a] >= n_stations ||
             arr_phase[a] < 0 || arr_phase[a] >= n_phases)
             return ctx->fail(TS_E_ARG, "arrival " + std::to_string(a) + " refers outside the inputs");
-        table_id[{arr_phase[a], arr_station[a]}] = 0;
+        table_id[size_t(arr_phase[a]) * n_stations + arr_station[a]] = 0;
     }
     std::vector<std::pair<int, int>> tables;
-    for (auto& kv : table_id) {
-        kv.second = int(tables.size());
-        tables.push_back(kv.first);
-    }
+    for (int ph = 0; ph < n_phases; ph++)
+        for (int st = 0; st < n_stations; st++) {
+            int& id = table_id[size_t(ph) * n_stations + st];
+            if (id < 0) continue;
+            id = int(tables.size());
+            tables.push_back({ph, st});
+        }
     const int nt = int(tables.size());
     std::vector<double> table_station(3 * std::max(1, nt));
     for (int t = 0; t < nt; t++)
@@ -165,18 +172,33 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
     }
     int rc = solve_tables<Real>(ctx, g, slowness, n_phases, mode, tables, stations, tab, stats);
     if (rc) return rc;
+    const std::string table_stats = ctx->stats;
+    const auto t_tables = std::chrono::steady_clock::now();
     // Arrivals → rays (the engine's field buffers were released for the rows).
     std::vector<int32_t> table_of(std::max(1, n_arr));
     std::vector<double> ev(3 * std::max(1, n_arr));
     for (int a = 0; a < n_arr; a++) {
-        table_of[a] = table_id[{arr_phase[a], arr_station[a]}];
+        table_of[a] = table_id[size_t(arr_phase[a]) * n_stations + arr_station[a]];
         for (int c = 0; c < 3; c++) ev[3 * a + c] = events[3 * arr_event[a] + c];
     }
     if (!(step_km > 0)) step_km = 0.5 * std::min(g.min_spacing_km(), gi.min_spacing_km());  // RayKernels.cs:62
     std::vector<int32_t> table_phase(std::max(1, nt));
     for (int t = 0; t < nt; t++) table_phase[t] = tables[t].first;
-    return rays::trace_on_device(ctx, g, tab, std::max(1, nt), table_station.data(), gi, n_arr, table_of.data(),
-                                 ev.data(), step_km, out, nullptr, table_phase.data());
+    rays::RayStats rs;
+    rc = rays::trace_on_device(ctx, g, tab, std::max(1, nt), table_station.data(), gi, n_arr, table_of.data(),
+                               ev.data(), step_km, out, &rs, table_phase.data());
+    if (rc) return rc;
+    // The step's timing in the context's stats text (ts_last_stats): the tables' call, then the rays'.
+    using ms = std::chrono::duration<double, std::milli>;
+    const auto t_end = std::chrono::steady_clock::now();
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "; tables %.1f ms; rays %.1f ms (host set-up %.1f ms, ray pipeline %.1f ms, on the device %.1f ms, "
+                  "%d chunks)",
+                  ms(t_tables - t_begin).count(), ms(t_end - t_tables).count(), rs.setup_ms, rs.wall_ms, rs.device_ms,
+                  rs.chunks);
+    ctx->stats = table_stats + buf;
+    return TS_OK;
 }
 
 }  // namespace fwd

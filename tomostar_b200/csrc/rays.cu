@@ -17,6 +17,7 @@
 //   emit_kernel   one warp per ray: copies every row from the staging area into the CSR arrays at
 //                 its offset in arrival order, once all chunks are traced.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -457,6 +458,7 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_phase, phases.data(), sizeof(int) * phases.size(), cudaMemcpyHostToDevice, s));
     a.table_phase = d_phase;
 
+    const auto th0 = std::chrono::steady_clock::now();
     // Record room per ray: one record per node per inversion cell crossed, with room for a path
     // three times the straight length; a ray that needs more is traced again with four times the room.
     constexpr int kMaxCap = 16384;  // the larger merge pass sorts up to this many in 128 KB
@@ -471,6 +473,7 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     std::vector<int> order(n_rays);
     for (int q = 0; q < n_rays; q++) order[q] = q;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table_of_host[x] < table_of_host[y]; });
+    const auto th1 = std::chrono::steady_clock::now();
     // Chunk budget: record slots (12 B of record + 8 B of merged output each) within a share of the
     // free device memory, at most 8 GB of records.
     size_t free_b = 0, total_b = 0;
@@ -521,6 +524,7 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
                 maxcap = std::max(maxcap, cap_of[q]);
             }
             c0 = c1;
+            if (st) st->chunks++;
             const int nr = int(ray_of.size());
             TS_BUF(ctx, d_ray_of, int, "rays.ray_of", nr);
             TS_BUF(ctx, d_base, int64_t, "rays.rec_base", nr);
@@ -641,7 +645,11 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     rows->nnz = total;
-    if (st) st->device_ms += ms;
+    if (st) {
+        st->device_ms += ms;
+        st->setup_ms += std::chrono::duration<double, std::milli>(th1 - th0).count();
+        st->wall_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
+    }
     *out = rows_own.release();
     return TS_OK;
 }

@@ -10,7 +10,10 @@ namespace ts {
 namespace rays {
 
 struct RayStats {
-    double device_ms = 0;
+    double device_ms = 0;   // from the first kernel to the row offsets on the stream (events)
+    double setup_ms = 0;    // host: per-ray record rooms and the table order
+    double wall_ms = 0;     // the whole call on the host
+    int chunks = 0;
     int retraced_chunks = 0;
 };
 
