@@ -316,9 +316,10 @@ def _fmm_sample_fields_per_s(grids, slownesses, seed_sets, threads: int):
 
 def inversion_job(device: int, threads: int) -> dict:
     """The forward step of a synthetic inversion (121x121x61 at 0.5 km, 25 stations x P,S = 50 fields,
-    7,500 rays) in FP64 and FP32 (the paired-float scheme): engine fields/s with the model resident,
-    its roofline, the forward step through ts_forward (tables + Jacobian rows), the plain per-plane
-    GPU path on one field and the CPU solver on a sample of fields."""
+    7,500 rays) in FP64 and FP32 (the paired-float scheme): engine fields/s (the 50 fields in one
+    launch, P and S as two slowness models of the grid, the tile shape and scheduler picked by the
+    autotuner on the job), its roofline, the forward step through ts_forward (tables + Jacobian rows),
+    the plain per-plane GPU path on one field and the CPU solver on a sample of fields."""
     from oracle import oracle as O
     from tomostar_b200 import _lib as L
     from tomostar_b200 import synthetic as syn
@@ -333,28 +334,20 @@ def inversion_job(device: int, threads: int) -> dict:
     seeds = {ph: [point_source(g, p.slowness[ph], *p.stations[q]) for q in range(len(p.stations))] for ph in (0, 1)}
     out = {"workload": "inversion_step_121: 121x121x61 at 0.5 km (0.89 M nodes), 25 stations x P,S = 50 fields, "
                        "150 events, 7,500 P+S rays into a CSR Jacobian"}
+    # The P and S fields in one launch: the grid twice, with the P and the S slowness.
+    grids, slows = [g, g], [p.slowness[0], p.slowness[1]]
+    fg = [0] * 25 + [1] * 25
+    sets = seeds[0] + seeds[1]
     with EikonalCuda.create(device, 64) as s:
         for prec in (64, 32):
-            gs = g.struct()
-            mid = C.c_int32()
-            s_all = np.ascontiguousarray(p.slowness)
-            L.check(lib.ts_model_put(s.handle, C.byref(gs), s_all.ctypes.data_as(P(C.c_double)), 2, prec,
-                                     C.byref(mid)), s)
-            stats = L.EikStats()
+            best, sched, _ = s.autotune(grids, slows, fg, sets, mode=L.MODE_FAST, precision=prec)
+            lib.ts_engine_set_tile(s.handle, prec, best)
+            lib.ts_engine_set_scheduler(s.handle, sched)
 
             def step():
-                dev = kern = 0.0
-                upd = 0
-                for ph in (0, 1):
-                    off, idx, t = pack_seeds(seeds[ph])
-                    L.check(lib.ts_eik_solve_model(s.handle, mid.value, ph, len(seeds[ph]),
-                                                   off.ctypes.data_as(P(C.c_int32)), idx.ctypes.data_as(P(C.c_int32)),
-                                                   t.ctypes.data_as(P(C.c_double)), L.MODE_FAST, 1e-7, 0, None,
-                                                   L.OUT_NONE, C.byref(stats)), s)
-                    dev += stats.device_ms
-                    kern += stats.kernel_ms
-                    upd += stats.node_updates
-                return dev, kern, upd
+                s.solve_multi(grids, slows, fg, sets, out_dtype=None, mode=L.MODE_FAST, precision=prec)
+                st = s.last_stats_struct
+                return st.device_ms, st.kernel_ms, st.node_updates
 
             for _ in range(3):
                 step()
@@ -363,6 +356,7 @@ def inversion_job(device: int, threads: int) -> dict:
             kern = sum(r[1] for r in runs) / 5
             upd = runs[-1][2]
             ach = upd * 24 / (kern / 1e3) / 1e9
+            shape = {sid: f"{bx}x{by}x{bz}" for sid, bx, by, bz in L.engine_shapes()}[best]
             rk = RayKernels(p.inv, g, s)
             rk.compute(p.slowness, p.stations, p.events, p.arrivals, precision=prec)  # warm-up
             t0 = time.perf_counter()
@@ -371,6 +365,7 @@ def inversion_job(device: int, threads: int) -> dict:
             tables_s = rk.last_stats.device_ms / 1e3
             out[f"fp{prec}"] = {
                 "fields_per_s": 50 / (dev / 1e3), "ms_per_50_fields": dev, "node_updates": upd,
+                "autotuned": {"shape": shape, "scheduler": ["lockstep", "flow"][sched]},
                 "updates_per_s": upd / (kern / 1e3),
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                              "bytes_per_update": 24},
@@ -379,7 +374,6 @@ def inversion_job(device: int, threads: int) -> dict:
                                  "rows_per_s": rows.n_rows / fwd_s,
                                  "rays_rows_per_s": rows.n_rows / max(1e-9, fwd_s - tables_s)},
             }
-            lib.ts_model_drop(s.handle, mid.value)
         # FP32 against the FP64 fields on two of the fields (the bitwise engine is the FP64 oracle).
         sub_seeds = [seeds[0][0], seeds[1][7]]
         worst = 0.0
@@ -790,7 +784,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--tile", type=int, default=5)
+    ap.add_argument("--tile", type=int, default=6)
     ap.add_argument("--mode", type=int, default=2, help="0 engine (bitwise), 2 fast (wake threshold 1e-13)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")

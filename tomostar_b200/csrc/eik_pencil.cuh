@@ -16,6 +16,8 @@
 // mask, and its y and z neighbours through one ballot of the changed lanes per step.
 #pragma once
 
+#include <type_traits>
+
 #include "eik_kernels.cuh"
 
 namespace ts {
@@ -34,17 +36,23 @@ struct PencilSmem {
 // Halo row of canonical row c (< 0 or >= B on its axis): slot 0..3 for c = −2, −1, B, B+1.
 TS_HDINL int halo_slot(int c, int B) { return c < 0 ? c + 2 : c - B + 2; }
 
+// One bit per node of a row: 64-bit words for 64-wide pencils, 32-bit for 32-wide ones.
 template <int BX>
-TS_DEVINL uint64_t row_reverse(uint64_t m) {
-    if (BX == 64) return __brevll(m);
-    return uint64_t(__brev(uint32_t(m)));
+using RowMask = std::conditional_t<BX == 64, uint64_t, uint32_t>;
+
+template <int BX>
+TS_DEVINL RowMask<BX> row_reverse(RowMask<BX> m) {
+    if constexpr (BX == 64) return __brevll(m);
+    else return __brev(m);
 }
 
 // Variants of the visit (OPT bits): kRing2 — a two-deep prefetch ring instead of four;
 // kLazyW — axis weights read where an update uses them instead of held in registers for the visit.
 // Both only trade registers (the values computed are the same).
 // kSpecAll — the sweep ordering fixed at compile time whatever the width and occupancy (lockstep).
-constexpr int kRing2 = 1, kLazyW = 2, kSpecAll = 4;
+// kReshuffle — the y and z neighbour values are fetched again for the wake tests after an update
+// instead of being held through it (within a step no lane changes the window values it shares).
+constexpr int kRing2 = 1, kLazyW = 2, kSpecAll = 4, kReshuffle = 8;
 
 template <typename Real, int BX, bool VARZ, int SDIR, int OPT = 0>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
@@ -79,11 +87,14 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     static_assert(BX == 32 || BX == 64, "pencil rows are 32 or 64 nodes");
     constexpr int RING = (OPT & kRing2) ? 2 : 4;  // prefetch depth (steps ahead)
     constexpr bool LAZYW = (OPT & kLazyW) != 0;
+    constexpr bool RESHUFFLE = (OPT & kReshuffle) != 0;
     constexpr int BY = kPencilBY, BZ = kPencilBZ, HX = Layout<Real>::HX;
     constexpr int MWR = BX / 32;           // mask words per row
     constexpr int MW = BX * BY * BZ / 32;  // mask words per tile
     constexpr unsigned FULL = 0xffffffffu;
-    constexpr uint64_t kRowBits = BX == 64 ? ~0ull : 0xffffffffull;
+    using Mask = RowMask<BX>;
+    constexpr Mask kOne = 1;
+    constexpr Mask kRowBits = Mask(~Mask(0));
     const Real inf = real_inf<Real>();
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int x0 = tx * BX, y0 = ty * BY, z0 = tz * BZ;
@@ -144,7 +155,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     const Real wz1 = Real(g.wz1), wz2 = Real(g.wz2);
     const Real* zc = VARZ ? static_cast<const Real*>(g.zc) + kZCoef * (row_on ? gz : 0) : nullptr;
     const int r = k * BY + j;
-    uint64_t fixed = 0, due = 0;
+    Mask fixed = 0, due = 0;
     {
         const bool in_range = tid >= fd.seed_tile_lo && tid <= fd.seed_tile_hi;
         int lo = 0, hi = in_range ? fd.seed_count : 0;
@@ -154,14 +165,14 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
             else hi = mid;
         }
         const bool has = in_range && lo < fd.seed_count && __ldg(&a.seed_tile[fd.seed_begin + lo]) == tid;
-        uint64_t fx = 0, dm = 0;
+        Mask fx = 0, dm = 0;
 #pragma unroll
         for (int w = 0; w < MWR; w++) {
-            if (has) fx |= uint64_t(__ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * MW + r * MWR + w])) << (32 * w);
-            dm |= uint64_t(__ldcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w])) << (32 * w);
+            if (has) fx |= Mask(__ldg(&a.seed_mask[int64_t(fd.seed_begin + lo) * MW + r * MWR + w])) << (32 * w);
+            dm |= Mask(__ldcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w])) << (32 * w);
         }
         if (!row_on) fx = kRowBits;
-        else if (x0 + BX > nx) fx |= kRowBits & ~((1ull << (nx - x0)) - 1ull);  // x off the grid
+        else if (x0 + BX > nx) fx |= kRowBits & ~((kOne << (nx - x0)) - kOne);  // x off the grid
         fixed = mx ? row_reverse<BX>(fx) : fx;
         due = (mx ? row_reverse<BX>(dm) : dm) & ~fixed;
     }
@@ -194,10 +205,10 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
 
     const Real tol = a.tol, wake_rel = a.wake_rel;
     const bool causal = a.causal != 0;
-    auto bit = [](int c) -> uint64_t { return (unsigned)c < unsigned(BX) ? (1ull << c) : 0ull; };
+    auto bit = [](int c) -> Mask { return (unsigned)c < unsigned(BX) ? Mask(kOne << c) : Mask(0); };
     // Woken nodes of the neighbour tiles, as row masks in canonical x: the rows one and two beyond
     // the lane's own y and z faces (a lane has at most one such side per axis), and the x halo.
-    uint64_t wky1 = 0, wky2 = 0, wkz1 = 0, wkz2 = 0;
+    Mask wky1 = 0, wky2 = 0, wkz1 = 0, wkz2 = 0;
     unsigned wxh = 0;  // bits 0..3: canonical x = −1, −2, BX, BX+1
     bool big = false;
     int evals = 0;
@@ -206,7 +217,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
 #pragma unroll
         for (int u = 0; u < RING; u++) {
             const int ip = p0 + u + ip0;
-            const bool is_due = (due >> (ip & 63)) & (unsigned(ip) < unsigned(BX));
+            const bool is_due = (due >> (ip & (BX - 1))) & (unsigned(ip) < unsigned(BX));
             if (__any_sync(FULL, is_due)) {
                 // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
                 // ahead has not (offset +1); two rows away likewise at offsets ∓2.
@@ -225,7 +236,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
                     if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
                     if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
-                    due &= ~(1ull << ip);
+                    due &= ~(kOne << ip);
                     evals++;
                     // Canonical → grid orientation (minus = smaller grid index).
                     const Real xm = mx ? W3 : W1, xp = mx ? W1 : W3, xm2 = mx ? W4 : W0, xp2 = mx ? W0 : W4;
@@ -248,12 +259,33 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                 }
                 const unsigned cb = __ballot_sync(FULL, chg);
                 if (cb) {
+                    if constexpr (RESHUFFLE) {
+                        yb1 = shfl_up_r(FULL, W1, 1);
+                        ya1 = shfl_down_r(FULL, W3, 1);
+                        yb2 = shfl_up_r(FULL, W0, 2);
+                        ya2 = shfl_down_r(FULL, W4, 2);
+                        zb1 = shfl_up_r(FULL, W1, 8);
+                        za1 = shfl_down_r(FULL, W3, 8);
+                        zb2 = shfl_up_r(FULL, W0, 16);
+                        za2 = shfl_down_r(FULL, W4, 16);
+                        if (chg) {
+                            const int x = ax(ip);
+                            if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
+                            if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
+                            if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                            if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
+                            if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
+                            if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
+                            if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                            if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
+                        }
+                    }
                     // A changed node wakes its 12 stencil neighbours (with the causal rule, those
                     // holding more than its new value W2). The y and z neighbours are woken through
                     // one ballot per direction: a change one row back wakes x = i'+1 of this row,
                     // one row ahead x = i'−1, and two rows back or ahead x = i'±2.
                     auto wk_if = [&](Real v) { return chg && (!causal || W2 < v); };
-                    uint64_t wk = 0;
+                    Mask wk = 0;
                     if (wk_if(W1)) wk |= bit(ip - 1);
                     if (wk_if(W3)) wk |= bit(ip + 1);
                     if (wk_if(W0)) wk |= bit(ip - 2);
@@ -273,7 +305,7 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     due |= wk & ~fixed;
                     if (chg) {
                         // Neighbours in other tiles (their values are the halo's, fixed in this visit).
-                        const uint64_t b = 1ull << ip;
+                        const Mask b = kOne << ip;
                         if ((hy_m1 >= 0 && wk_if(yb1)) || (hy_p1 >= 0 && wk_if(ya1))) wky1 |= b;
                         if ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2))) wky2 |= b;
                         if ((hz_m1 >= 0 && wk_if(zb1)) || (hz_p1 >= 0 && wk_if(za1))) wkz1 |= b;
@@ -297,12 +329,12 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     }
 
     // Hand the due nodes back; wake the nodes of the neighbour tiles within two nodes of a change.
-    const uint64_t due_g = mx ? row_reverse<BX>(due & ~fixed) : (due & ~fixed);
+    const Mask due_g = mx ? row_reverse<BX>(due & ~fixed) : Mask(due & ~fixed);
 #pragma unroll
     for (int w = 0; w < MWR; w++) __stcg(&fd.dmask[int64_t(tid) * MW + r * MWR + w], uint32_t(due_g >> (32 * w)));
     if (__any_sync(FULL, due_g != 0) && lane == 0) __stcg(&fd.dirty[tid], (uint8_t)1);
-    auto wake_row = [&](int ntid, int nr, uint64_t canon_bits) {
-        const uint64_t bits = mx ? row_reverse<BX>(canon_bits) : canon_bits;
+    auto wake_row = [&](int ntid, int nr, Mask canon_bits) {
+        const Mask bits = mx ? row_reverse<BX>(canon_bits) : canon_bits;
 #pragma unroll
         for (int w = 0; w < MWR; w++) {
             const uint32_t m = uint32_t(bits >> (32 * w));
@@ -311,14 +343,14 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
         __stcg(&fd.dirty[ntid], (uint8_t)1);
     };
     // Rows beyond the y and z faces: canonical row c outside the tile → the neighbour tile and its row.
-    auto wake_y = [&](int c, uint64_t bits) {
+    auto wake_y = [&](int c, Mask bits) {
         if (!bits) return;
         int ay = my ? BY - 1 - c : c;  // tile-local actual row, outside [0, BY)
         int nty = ay < 0 ? ty - 1 : ty + 1;
         if (nty < 0 || nty >= g.ty) return;
         wake_row(tid + (nty - ty) * g.tx, k * BY + (ay < 0 ? ay + BY : ay - BY), bits);
     };
-    auto wake_z = [&](int c, uint64_t bits) {
+    auto wake_z = [&](int c, Mask bits) {
         if (!bits) return;
         int az = mz ? BZ - 1 - c : c;
         int ntz = az < 0 ? tz - 1 : tz + 1;
@@ -332,12 +364,12 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     if (wxh) {
         // Canonical x −1, −2 lie in the tile before along the sweep, BX, BX+1 in the one after.
         const int back = mx ? tx + 1 : tx - 1, ahead = mx ? tx - 1 : tx + 1;
-        const uint64_t top = 1ull << (BX - 1), top2 = 1ull << (BX - 2);
+        const Mask top = kOne << (BX - 1), top2 = kOne << (BX - 2);
         // In the neighbour tile's canonical x, −1 ↦ BX−1, −2 ↦ BX−2, BX ↦ 0, BX+1 ↦ 1.
         if ((wxh & 3u) && back >= 0 && back < g.tx)
-            wake_row(tid + (back - tx), r, ((wxh & 1u) ? top : 0ull) | ((wxh & 2u) ? top2 : 0ull));
+            wake_row(tid + (back - tx), r, Mask(((wxh & 1u) ? top : Mask(0)) | ((wxh & 2u) ? top2 : Mask(0))));
         if ((wxh & 12u) && ahead >= 0 && ahead < g.tx)
-            wake_row(tid + (ahead - tx), r, ((wxh & 4u) ? 1ull : 0ull) | ((wxh & 8u) ? 2ull : 0ull));
+            wake_row(tid + (ahead - tx), r, Mask(((wxh & 4u) ? 1u : 0u) | ((wxh & 8u) ? 2u : 0u)));
     }
     big = __any_sync(FULL, big);
     if (lane == 0 && big) __stcg(&a.fields[f].state->changed, 1);  // every writer writes 1
