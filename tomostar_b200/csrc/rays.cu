@@ -7,7 +7,8 @@
 //   trace_kernel  one thread per ray: steepest descent on the station's float32 table, each new
 //                 polyline segment integrated at once against the trilinear basis of the inversion
 //                 grid. Pieces falling in the same inversion cell are summed before a record
-//                 (node, length) is written, so a ray writes about one record per node per cell.
+//                 (node, length) is written, and a node shared with the next cell (a face
+//                 neighbour) keeps its running sum, so a ray writes about one record per node.
 //                 A step's gradient loads its six evaluations' 48 corners together (one memory
 //                 latency instead of six dependent ones).
 //   merge_kernel  one warp per ray: sorts the ray's records by node (bitonic, shared memory, the
@@ -71,25 +72,49 @@ struct Recorder {
     double outside = 0;           // RayRow.OutsideTime
     const double* bgv = nullptr;  // the background's velocity of the ray's phase
 
+    // The record (node, running sum) of corner n of the current cell.
+    TS_DEVINL void record(const TraceArgs& a, int r, int n) {
+        if (count >= a.rec_cap[r]) {
+            overflow = true;
+            return;
+        }
+        const int di = n & 1, dj = (n >> 1) & 1, dk = n >> 2;
+        const int64_t slot = a.rec_base[r] + count;
+        a.rec_node[slot] = int((ck + dk) * (int64_t(a.inv.nx) * a.inv.ny) + int64_t(cj + dj) * a.inv.nx + (ci + di));
+        a.rec_val[slot] = acc[n];
+        count++;
+    }
+
     TS_DEVINL void flush(const TraceArgs& a, int r) {
         if (ci < 0 || !touched) return;
-        const int nx = a.inv.nx;
-        const int64_t nxy = int64_t(a.inv.nx) * a.inv.ny;
-        const int cap = a.rec_cap[r];
+#pragma unroll
+        for (int n = 0; n < 8; n++)
+            if ((touched >> n) & 1u) record(a, r, n);
+        touched = 0;
+    }
+
+    // Moving into the face neighbour along axis bit B (UP: to the larger index), the four corners the
+    // two cells share keep their running sums, so a node's pieces add up in visit order with no record
+    // in between; the other four are written.
+    template <int B, bool UP>
+    TS_DEVINL void carry(const TraceArgs& a, int r) {
+        double nacc[8];
+        unsigned nt = 0;
+#pragma unroll
+        for (int n = 0; n < 8; n++) nacc[n] = 0.0;
 #pragma unroll
         for (int n = 0; n < 8; n++) {
             if (!((touched >> n) & 1u)) continue;
-            if (count >= cap) {
-                overflow = true;
-                continue;
+            if (UP ? (n & B) != 0 : (n & B) == 0) {
+                nacc[n ^ B] = acc[n];
+                nt |= 1u << (n ^ B);
+            } else {
+                record(a, r, n);
             }
-            int di = n & 1, dj = (n >> 1) & 1, dk = n >> 2;
-            int64_t slot = a.rec_base[r] + count;
-            a.rec_node[slot] = int((ck + dk) * nxy + int64_t(cj + dj) * nx + (ci + di));
-            a.rec_val[slot] = acc[n];
-            count++;
         }
-        touched = 0;
+#pragma unroll
+        for (int n = 0; n < 8; n++) acc[n] = nacc[n];
+        touched = nt;
     }
 
     // RayTracing.Kernel for one polyline segment (RayTracing.cs:133-157).
@@ -115,10 +140,20 @@ struct Recorder {
             double w[8];
             geo::weights(a.inv, fx, fy, fz, i0, j0, k0, w);
             if (i0 != ci || j0 != cj || k0 != ck) {
-                flush(a, r);
-                ci = i0; cj = j0; ck = k0;
+                const int di = i0 - ci, dj = j0 - cj, dk = k0 - ck;
+                if (ci >= 0 && abs(di) + abs(dj) + abs(dk) == 1) {
+                    if (di == 1) carry<1, true>(a, r);
+                    else if (di == -1) carry<1, false>(a, r);
+                    else if (dj == 1) carry<2, true>(a, r);
+                    else if (dj == -1) carry<2, false>(a, r);
+                    else if (dk == 1) carry<4, true>(a, r);
+                    else carry<4, false>(a, r);
+                } else {
+                    flush(a, r);
 #pragma unroll
-                for (int n = 0; n < 8; n++) acc[n] = 0.0;
+                    for (int n = 0; n < 8; n++) acc[n] = 0.0;
+                }
+                ci = i0; cj = j0; ck = k0;
             }
 #pragma unroll
             for (int n = 0; n < 8; n++) {
