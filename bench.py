@@ -802,7 +802,7 @@ def main():
     ap.add_argument("--location-cpu-events", type=int, default=256, help="events the CPU baseline locates")
     ap.add_argument("--serve-scheduler", type=int, default=1)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
-    ap.add_argument("--serve-tile", type=int, default=2)
+    ap.add_argument("--serve-tile", type=int, default=6)
     ap.add_argument("--serve-rounds", type=int, default=2, help="sweep rounds per serving epoch")
     ap.add_argument("--serve-epoch-ms", type=float, default=0.0,
                     help="flow scheduler: fields pause at their next round end after this long (0: off)")

@@ -16,7 +16,7 @@ from .eikonal import point_source
 from .serving import Server
 
 
-def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 2, rounds_per_epoch: int = 1,
+def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 6, rounds_per_epoch: int = 1,
         budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 0,
         epoch_ms: float = 0.0) -> dict:
     models = syn.serving_models()
@@ -97,7 +97,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--seconds", type=float, default=60.0)
     ap.add_argument("--rate", type=float, default=200.0)
-    ap.add_argument("--tile", type=int, default=2)
+    ap.add_argument("--tile", type=int, default=6)
     ap.add_argument("--rounds-per-epoch", type=int, default=1)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--scheduler", type=int, default=0)
