@@ -16,8 +16,8 @@ from .eikonal import point_source
 from .serving import Server
 
 
-def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 6, rounds_per_epoch: int = 1,
-        budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 0,
+def run(seconds: float = 60.0, rate: float = 200.0, tile: int = 6, rounds_per_epoch: int = 2,
+        budget_bytes: float = 120e9, device: int = 0, seed: int = 4, scheduler: int = 1,
         epoch_ms: float = 0.0) -> dict:
     models = syn.serving_models()
     stream = syn.serving_stream(models, rate=rate, duration=seconds, seed=seed)
@@ -98,9 +98,9 @@ def main():
     ap.add_argument("--seconds", type=float, default=60.0)
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--tile", type=int, default=6)
-    ap.add_argument("--rounds-per-epoch", type=int, default=1)
+    ap.add_argument("--rounds-per-epoch", type=int, default=2)
     ap.add_argument("--budget-gb", type=float, default=120.0)
-    ap.add_argument("--scheduler", type=int, default=0)
+    ap.add_argument("--scheduler", type=int, default=1)
     ap.add_argument("--epoch-ms", type=float, default=0.0)
     a = ap.parse_args()
     print(json.dumps(run(a.seconds, a.rate, a.tile, a.rounds_per_epoch, a.budget_gb * 1e9, scheduler=a.scheduler,
