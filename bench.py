@@ -692,6 +692,22 @@ def run_ours(args, problem_fn):
         it_ms = lres.device_ms / max(1, lres.iterations)
         lsqr_gbs = it_bytes / (it_ms / 1e3) / 1e9
         peak, _ = measured_hbm_peak()
+        # Roofline of the ray kernels: per row, one 8-corner float32 gather (32 B) per back-tracing step,
+        # the row's non-zeros (int32 node + float32 length) and 32 B of row scalars, over the ray
+        # pipeline's device time (both from the call's own counters).
+        import re
+
+        m_dev = re.search(r"on the device ([0-9.]+) ms", fwd_stats)
+        m_steps = re.search(r"([0-9]+) steps\)", fwd_stats)
+        ray_roof = None
+        if m_dev and m_steps:
+            ray_dev_s = float(m_dev.group(1)) / 1e3
+            steps = int(m_steps.group(1))
+            ray_bytes = steps * 32 + nnz * 8 + n_rows * 32
+            ach_r = ray_bytes / ray_dev_s / 1e9
+            ray_roof = {"bound": "hbm", "achieved": ach_r, "peak": peak, "unit": "GB/s", "frac": ach_r / peak,
+                        "bytes_per_row": ray_bytes / max(1, n_rows), "steps_per_row": steps / max(1, n_rows),
+                        "device_s": ray_dev_s, "device_rows_per_s": n_rows / ray_dev_s}
         forward = {"arrivals": n_rows, "tables": 2 * len(p.stations), "wall_s": fwd_s + copy_s,
                    "rows_per_s": n_rows / (fwd_s + copy_s), "tables_s": fields_s,
                    "rays_and_copy_s": fwd_s - fields_s + copy_s,
@@ -699,6 +715,7 @@ def run_ours(args, problem_fn):
                    "nnz_per_row": nnz / max(1, kept), "kept_rows": kept,
                    "copy_s": copy_s, "copy_gbs": (nnz * 8 + n_rows * 45) / copy_s / 1e9,
                    "timing": fwd_stats,
+                   "rays_roofline": ray_roof,
                    "mode": ("fast" if args.mode == L.MODE_FAST else "engine (bitwise)") +
                            " tables (FP64 fields as float32), rays FP64",
                    "exact_mode": exact,

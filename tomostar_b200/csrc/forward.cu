@@ -194,9 +194,9 @@ static int forward_impl(ts_ctx* ctx, const ts_grid* fwd_def, const double* slown
     char buf[256];
     std::snprintf(buf, sizeof buf,
                   "; tables %.1f ms; rays %.1f ms (host set-up %.1f ms, ray pipeline %.1f ms, on the device %.1f ms, "
-                  "%d chunks)",
+                  "%d chunks, %llu steps)",
                   ms(t_tables - t_begin).count(), ms(t_end - t_tables).count(), rs.setup_ms, rs.wall_ms, rs.device_ms,
-                  rs.chunks);
+                  rs.chunks, rs.steps);
     ctx->stats = table_stats + buf;
     return TS_OK;
 }

@@ -57,6 +57,7 @@ struct TraceArgs {
     int* rec_count;               // per chunk slot
     double* tcg;                  // 4 per ray (global index)
     double* outside;              // per ray (global index): time outside the inversion grid
+    unsigned long long* steps;    // back-tracing steps of every ray traced (the gathers' unit)
     int bg_n;                     // > 0: the extended domain's background (depths, Vp, Vs at bg)
     const double* bg;
     const int* table_phase;       // per table: 0 P (Vp), 1 S (Vs)
@@ -194,9 +195,16 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     int stalls = 0;
     Recorder rec;
     if (a.bg_n > 0) rec.bgv = a.bg + (a.table_phase[tab] == 0 ? 1 : 2) * a.bg_n;
+    // The steps this ray takes, added to the launch's count on every way out.
+    struct StepCount {
+        unsigned long long* total;
+        unsigned long long n = 0;
+        TS_DEVINL ~StepCount() { atomicAdd(total, n); }
+    } taken{a.steps};
     GeoPt prev = ev;
     for (int s = 0; s < max_steps; s++) {
         if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
+        taken.n++;
         GeoPt gp = geo::from_cartesian(p);
         double ge, gn, gz;
         geo::table_gradient_b(g, tb, gp.lon, gp.lat, gp.dep, ge, gn, gz);
@@ -482,6 +490,9 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     a.piece_km = 0.5 * inv.min_spacing_km();  // RayTracing.cs:130
     a.tcg = rows->tcg;
     a.outside = rows->outside;
+    TS_BUF(ctx, d_steps, unsigned long long, "rays.steps", 1);
+    TS_CUDA_TRY(ctx, cudaMemsetAsync(d_steps, 0, sizeof(unsigned long long), s));
+    a.steps = d_steps;
     // The extended domain's background (ts_set_background) and each table's phase.
     a.bg_n = ctx->bg_n;
     a.bg = a.bg_n > 0 ? static_cast<const double*>(ctx->buf("rays.background", sizeof(double) * 3 * a.bg_n))
@@ -680,7 +691,10 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     rows->nnz = total;
+    unsigned long long h_steps = 0;
+    TS_CUDA_TRY(ctx, cudaMemcpy(&h_steps, d_steps, sizeof h_steps, cudaMemcpyDeviceToHost));
     if (st) {
+        st->steps += h_steps;
         st->device_ms += ms;
         st->setup_ms += std::chrono::duration<double, std::milli>(th1 - th0).count();
         st->wall_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();

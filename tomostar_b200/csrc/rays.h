@@ -15,6 +15,7 @@ struct RayStats {
     double wall_ms = 0;     // the whole call on the host
     int chunks = 0;
     int retraced_chunks = 0;
+    unsigned long long steps = 0;  // back-tracing steps taken (rays traced again count again)
 };
 
 // Traces n_rays rays on device-resident float32 tables (n_tables fields on fwd) and builds their
