@@ -338,3 +338,23 @@ def test_flow_scheduler_inversion_step_121_batch(solver):
     finally:
         lib.ts_engine_set_scheduler(solver.handle, 0)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_many_fields_to_page_locked_memory_equal_pageable(solver, precision, dtype):
+    """With 64 fields or more and a page-locked output the solve copies the first half of the fields
+    to the host while the second half is solved; the result is the same as through pageable memory."""
+    import torch
+
+    g, s, _ = hetero_case(21, 19, 11, seed=8, nsrc=1)
+    rng = np.random.default_rng(8)
+    lon, lat, dep = g.lon(), g.lat(), g.depth()
+    seeds = [point_source(g, s, rng.uniform(lon[0], lon[-1]), rng.uniform(lat[0], lat[-1]),
+                          rng.uniform(dep[0], dep[-1])) for _ in range(70)]
+    pageable = solver.solve(g, s, seeds, precision=precision, mode=L.MODE_FAST,
+                            output=np.empty((70, g.count), dtype))
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    locked = torch.empty((70, g.count), dtype=tdt, pin_memory=True).numpy()
+    solver.solve(g, s, seeds, precision=precision, mode=L.MODE_FAST, output=locked)
+    assert np.array_equal(locked, pageable)

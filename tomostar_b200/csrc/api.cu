@@ -83,6 +83,7 @@ void ts_cuda_destroy(ts_ctx* ctx) {
             if (kv.second.p) cudaFreeHost(kv.second.p);
         ctx->bufs.clear();
         if (ctx->cancel_host) cudaFreeHost(const_cast<int*>(ctx->cancel_host));
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;

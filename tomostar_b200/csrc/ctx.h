@@ -15,6 +15,7 @@
 struct ts_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // device→host copies that overlap the next solve (created on use)
     std::recursive_mutex mu;  // calls on one context are serialised (EikonalOpenCl.cs:64,165)
     std::string err;
     std::string stats;

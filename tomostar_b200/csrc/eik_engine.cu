@@ -642,7 +642,77 @@ int engine_run(ts_ctx* ctx, EngineJob& job, ts_eik_stats* stats) {
     return engine_epoch<Real>(ctx, job.grids, job.metrics, fl, job.tol, job.wake_rel, job.tile, 0, stats, ctx->stream);
 }
 
+// Fields [f0, f1) of a job (after engine_run) converted to dense grid order of out_type into dst, on s.
+template <typename Real>
+static int fields_to_dense_device(ts_ctx* ctx, const EngineJob& job, size_t f0, size_t f1, void* dst, int out_type,
+                                  cudaStream_t s) {
+    char* d = static_cast<char*>(dst);
+    const size_t osz = out_type == TS_OUT_F64 ? 8 : 4;
+    for (size_t f = f0; f < f1; f++) {
+        const host::Grid& g = *job.grids[job.fields[f].grid];
+        const int pitch = job.pitch[job.fields[f].grid];
+        const int64_t rows = int64_t(g.ny) * g.nz, n = rows * g.nx;
+        const int blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
+        const Real* src = static_cast<const Real*>(job.fields[f].T);
+        if (osz == 8)
+            dense_convert_kernel<Real, double><<<dim3(blocks, 1), 256, 0, s>>>(src, 0, pitch, job.xoff, g.nx, rows,
+                                                                               reinterpret_cast<double*>(d));
+        else
+            dense_convert_kernel<Real, float><<<dim3(blocks, 1), 256, 0, s>>>(src, 0, pitch, job.xoff, g.nx, rows,
+                                                                              reinterpret_cast<float*>(d));
+        TS_CUDA_TRY(ctx, cudaGetLastError());
+        d += size_t(n) * osz;
+    }
+    return TS_OK;
+}
+
+template <typename Real>
+int engine_run_to_host(ts_ctx* ctx, EngineJob& job, void* out, int out_type, ts_eik_stats* stats) {
+    const size_t nf = job.fields.size(), half = (nf + 1) / 2;
+    const size_t osz = out_type == TS_OUT_F64 ? 8 : 4;
+    if (!ctx->copy_stream) TS_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    size_t bytes[2] = {0, 0};
+    for (size_t f = 0; f < nf; f++) bytes[f < half ? 0 : 1] += size_t(job.grids[job.fields[f].grid]->count()) * osz;
+    void* stage = ctx->buf("out.pipeline", std::max(bytes[0], bytes[1]));
+    if (!stage) return TS_E_NOMEM;
+    EventPair converted, copied;
+    char* dst = static_cast<char*>(out);
+    int rc = TS_OK;
+    for (int part = 0; part < 2 && rc == TS_OK; part++) {
+        const size_t f0 = part == 0 ? 0 : half, f1 = part == 0 ? half : nf;
+        if (f0 == f1) continue;
+        // The part as a job of its own (its fields move in and back out).
+        EngineJob sub;
+        sub.grids = job.grids;
+        sub.metrics = job.metrics;
+        sub.tol = job.tol;
+        sub.wake_rel = job.wake_rel;
+        sub.tile = job.tile;
+        for (size_t f = f0; f < f1; f++) sub.fields.push_back(std::move(job.fields[f]));
+        rc = engine_run<Real>(ctx, sub, stats);
+        if (rc == TS_OK) {
+            // The stage is free once the previous part's copy has read it.
+            if (part == 1) TS_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, copied.a, 0));
+            rc = fields_to_dense_device<Real>(ctx, sub, 0, sub.fields.size(), stage, out_type, ctx->stream);
+        }
+        if (rc == TS_OK) {
+            TS_CUDA_TRY(ctx, cudaEventRecord(converted.a, ctx->stream));
+            TS_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, converted.a, 0));
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(dst, stage, bytes[part], cudaMemcpyDeviceToHost, ctx->copy_stream));
+            TS_CUDA_TRY(ctx, cudaEventRecord(copied.a, ctx->copy_stream));
+            dst += bytes[part];
+        }
+        job.pitch = sub.pitch;
+        job.xoff = sub.xoff;
+        for (size_t f = f0; f < f1; f++) job.fields[f] = std::move(sub.fields[f - f0]);
+    }
+    TS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->copy_stream));
+    return rc;
+}
+
 template int engine_run<Pair>(ts_ctx*, EngineJob&, ts_eik_stats*);
+template int engine_run_to_host<double>(ts_ctx*, EngineJob&, void*, int, ts_eik_stats*);
+template int engine_run_to_host<Pair>(ts_ctx*, EngineJob&, void*, int, ts_eik_stats*);
 template int engine_run<double>(ts_ctx*, EngineJob&, ts_eik_stats*);
 template int engine_epoch<Pair>(ts_ctx*, const std::vector<const host::Grid*>&, const std::vector<const host::Metric*>&,
                                  const std::vector<EngineField*>&, double, double, int, int, ts_eik_stats*, cudaStream_t);

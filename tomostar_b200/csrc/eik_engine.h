@@ -80,6 +80,12 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
 // Points a field's buffers into one device block of field_layout(...).bytes(precision) bytes.
 void engine_field_place(EngineField& f, const FieldLayout& L, int precision, void* block);
 
+// One-shot with the results to page-locked host memory: the fields are solved in two halves and the
+// first half's fields are converted and copied to the host (on a second stream) while the second
+// half is solved. out: the fields one after another in dense grid order, of out_type.
+template <typename Real>
+int engine_run_to_host(ts_ctx* ctx, EngineJob& job, void* out, int out_type, ts_eik_stats* stats);
+
 // Copies padded engine fields to dense grid order (converting to out_type, TS_OUT_F64 / TS_OUT_F32).
 int fields_to_dense_host(ts_ctx* ctx, const EngineJob& job, int precision, void* out, int out_type);
 int fields_to_dense_f32_device(ts_ctx* ctx, const EngineJob& job, int precision, float* out);

@@ -249,6 +249,14 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
     int rounds_max[2] = {0, 0};
     EngineJob job;
     Real* T = nullptr;
+    // Many fields into page-locked host memory: the copies of the first half overlap the second half's
+    // solve (engine_run_to_host).
+    bool pipelined = false;
+    if (in.mode != TS_MODE_PLAIN && out_type != TS_OUT_NONE && out && nf >= 64 && !ctx->use_graph) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, out) == cudaSuccess) pipelined = at.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+    }
     if (in.mode == TS_MODE_PLAIN) {
         T = static_cast<Real*>(ctx->buf("solve.fields", sizeof(Real) * size_t(nf) * n));
         if (!T) return TS_E_NOMEM;
@@ -273,7 +281,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
             ef.cap = cap;
             job.fields.push_back(ef);
         }
-        rc = engine_run<Real>(ctx, job, stats);
+        rc = pipelined ? engine_run_to_host<Real>(ctx, job, out, out_type, stats) : engine_run<Real>(ctx, job, stats);
         for (auto& ef : job.fields) {
             rounds_max[0] = std::max(rounds_max[0], ef.rounds[0]);
             rounds_max[1] = std::max(rounds_max[1], ef.rounds[1]);
@@ -302,6 +310,7 @@ static int solve_impl(ts_ctx* ctx, const SolveIn& in, void* out, int out_type, t
     const int precision = precision_of<Real>();
     if (out_type == TS_OUT_NONE) return TS_OK;  // the fields stay on the device
     if (in.mode == TS_MODE_PLAIN) return copy_fields_out(ctx, T, precision, int64_t(nf) * n, out, out_type);
+    if (pipelined) return TS_OK;  // already on the host
     return fields_to_dense_host(ctx, job, precision, out, out_type);
 }
 
