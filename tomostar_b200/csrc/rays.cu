@@ -22,6 +22,8 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "ctx.h"
@@ -509,24 +511,41 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     // three times the straight length; a ray that needs more is traced again with four times the room.
     constexpr int kMaxCap = 16384;  // the larger merge pass sorts up to this many in 128 KB
     std::vector<int> cap_of(std::max(1, n_rays));
-    for (int q = 0; q < n_rays; q++) {
-        const double* ev = events_host + 3 * q;
-        const double* stn = table_station_host + 3 * table_of_host[q];
-        const double d = host::dist(host::to_cartesian(ev[0], ev[1], ev[2]), host::to_cartesian(stn[0], stn[1], stn[2]));
-        cap_of[q] = int(std::min(double(kMaxCap), 8.0 * (3.0 * d / a.piece_km + 32)));
+    {
+        // The straight lengths on the host's threads (two trigonometric conversions per ray).
+        auto room = [&](int q0, int q1) {
+            for (int q = q0; q < q1; q++) {
+                const double* ev = events_host + 3 * q;
+                const double* stn = table_station_host + 3 * table_of_host[q];
+                const double d =
+                    host::dist(host::to_cartesian(ev[0], ev[1], ev[2]), host::to_cartesian(stn[0], stn[1], stn[2]));
+                cap_of[q] = int(std::min(double(kMaxCap), 8.0 * (3.0 * d / a.piece_km + 32)));
+            }
+        };
+        const int nt = n_rays < 65536 ? 1 : int(std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; t++)
+            pool.emplace_back(room, int(int64_t(n_rays) * t / nt), int(int64_t(n_rays) * (t + 1) / nt));
+        room(0, int(int64_t(n_rays) / nt));
+        for (auto& th : pool) th.join();
     }
-    // Rays in order of their table: a chunk's rays read few tables, which stay in L2.
+    // Rays in order of their table (a counting sort, stable): a chunk's rays read few tables, which
+    // stay in L2.
     std::vector<int> order(n_rays);
-    for (int q = 0; q < n_rays; q++) order[q] = q;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table_of_host[x] < table_of_host[y]; });
+    {
+        std::vector<int> at(n_tables + 1, 0);
+        for (int q = 0; q < n_rays; q++) at[table_of_host[q] + 1]++;
+        for (int t = 0; t < n_tables; t++) at[t + 1] += at[t];
+        for (int q = 0; q < n_rays; q++) order[at[table_of_host[q]]++] = q;
+    }
     const auto th1 = std::chrono::steady_clock::now();
-    // Chunk budget: record slots (12 B of record + 8 B of merged output each) within a share of the
-    // free device memory, at most 8 GB of records.
+    // Chunk budget: record slots (12 B of record + 8 B of merged output each) of two chunks in
+    // flight within a share of the free device memory, at most 400 M slots per chunk.
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     cudaGetLastError();
     const int64_t budget = std::max<int64_t>(int64_t(kMaxCap) * 64,
-                                             std::min<int64_t>(int64_t(400) << 20, int64_t(free_b / 4 / 20)));
+                                             std::min<int64_t>(int64_t(400) << 20, int64_t(free_b / 8 / 20)));
     TS_BUF(ctx, ray_nnz, int, "rays.ray_nnz", std::max(1, n_rays));
     TS_BUF(ctx, stage_off, long long, "rays.stage_off", std::max(1, n_rays));
     // The staging area (rows in chunk order), freed on every return.
@@ -546,99 +565,152 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     float*& stage_len = stage.len;
     int64_t stage_cap = 0, stage_used = 0;
     auto free_stage = [&]() { stage.free(); };
+    // Two chunks in flight: while the device traces chunk k, the host reads chunk k−1's row total and
+    // queues its staging copy behind it, so the stream never waits on the host.
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        Events() {
+            for (auto& x : e) cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        }
+        ~Events() {
+            for (auto& x : e) cudaEventDestroy(x);
+        }
+    } done;
+    long long* h_sums = static_cast<long long*>(ctx->host_buf("rays.sums_h", sizeof(long long) * 4));
+    if (!h_sums) return bail(TS_E_NOMEM);
     EventPair ev;
     cudaEvent_t e0 = ev.a, e1 = ev.b;
     cudaEventRecord(e0, s);
     std::vector<int> pending = order;
     for (int pass = 0; !pending.empty(); pass++) {
-        std::vector<int> retry;
-        for (size_t c0 = 0; c0 < pending.size();) {
-            // The chunk: rays from c0 while their rooms fit the budget.
-            std::vector<int> ray_of;
-            std::vector<int64_t> base;
-            std::vector<int> caps;
-            int64_t used = 0;
-            int maxcap = 32;
-            size_t c1 = c0;
-            while (c1 < pending.size() && (ray_of.empty() || used + cap_of[pending[c1]] <= budget) &&
-                   ray_of.size() < (size_t(1) << 20)) {
-                const int q = pending[c1++];
-                ray_of.push_back(q);
-                base.push_back(used);
-                caps.push_back(cap_of[q]);
-                used += cap_of[q];
-                maxcap = std::max(maxcap, cap_of[q]);
+        // The pass's chunks: rays in order while their rooms fit the budget; each ray's room and
+        // place, for every chunk, copied to the device at once.
+        struct Chunk {
+            size_t c0, c1;
+            int64_t used;
+            int maxcap;
+        };
+        std::vector<Chunk> chunks;
+        const size_t np = pending.size();
+        int* h_ray = static_cast<int*>(ctx->host_buf("rays.plan_ray", sizeof(int) * np));
+        int64_t* h_base = static_cast<int64_t*>(ctx->host_buf("rays.plan_base", sizeof(int64_t) * np));
+        int* h_cap = static_cast<int*>(ctx->host_buf("rays.plan_cap", sizeof(int) * np));
+        if (!h_ray || !h_base || !h_cap) return bail(TS_E_NOMEM);
+        int64_t max_used = 1;
+        int max_nr = 1, maxcap_all = 32;
+        for (size_t c0 = 0; c0 < np;) {
+            Chunk c{c0, c0, 0, 32};
+            while (c.c1 < np && (c.c1 == c0 || c.used + cap_of[pending[c.c1]] <= budget) &&
+                   c.c1 - c0 < (size_t(1) << 20)) {
+                const int q = pending[c.c1];
+                h_ray[c.c1] = q;
+                h_base[c.c1] = c.used;
+                h_cap[c.c1] = cap_of[q];
+                c.used += cap_of[q];
+                c.maxcap = std::max(c.maxcap, cap_of[q]);
+                c.c1++;
             }
-            c0 = c1;
+            max_used = std::max(max_used, c.used);
+            max_nr = std::max(max_nr, int(c.c1 - c0));
+            maxcap_all = std::max(maxcap_all, c.maxcap);
+            chunks.push_back(c);
+            c0 = c.c1;
+        }
+        TS_BUF(ctx, d_ray_of, int, "rays.ray_of", np);
+        TS_BUF(ctx, d_base, int64_t, "rays.rec_base", np);
+        TS_BUF(ctx, d_cap, int, "rays.rec_cap", np);
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ray_of, h_ray, sizeof(int) * np, cudaMemcpyHostToDevice, s));
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_base, h_base, sizeof(int64_t) * np, cudaMemcpyHostToDevice, s));
+        TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_cap, h_cap, sizeof(int) * np, cudaMemcpyHostToDevice, s));
+        // Per set of a chunk in flight: records, merged rows, row sizes and offsets, the two totals.
+        struct Set {
+            int *rec_node, *rec_count, *out_node, *nnz, *off;
+            double* rec_val;
+            float* out_len;
+            long long* sums;
+        } set[2];
+        for (int b = 0; b < 2; b++) {
+            const std::string k = b ? "1" : "0";
+            set[b].rec_node = static_cast<int*>(ctx->buf("rays.rec_node" + k, sizeof(int) * size_t(max_used)));
+            set[b].rec_val = static_cast<double*>(ctx->buf("rays.rec_val" + k, sizeof(double) * size_t(max_used)));
+            set[b].out_node = static_cast<int*>(ctx->buf("rays.out_node" + k, sizeof(int) * size_t(max_used)));
+            set[b].out_len = static_cast<float*>(ctx->buf("rays.out_len" + k, sizeof(float) * size_t(max_used)));
+            set[b].rec_count = static_cast<int*>(ctx->buf("rays.rec_count" + k, sizeof(int) * max_nr));
+            set[b].nnz = static_cast<int*>(ctx->buf("rays.nnz" + k, sizeof(int) * max_nr));
+            set[b].off = static_cast<int*>(ctx->buf("rays.off" + k, sizeof(int) * max_nr));
+            set[b].sums = static_cast<long long*>(ctx->buf("rays.sums" + k, sizeof(long long) * 2));
+            if (!set[b].rec_node || !set[b].rec_val || !set[b].out_node || !set[b].out_len || !set[b].rec_count ||
+                !set[b].nnz || !set[b].off || !set[b].sums)
+                return bail(TS_E_NOMEM);
+        }
+        // Small sort size for most rays; the rest in a second pass with one warp per block.
+        const int Psmall = 2048, W = 4;
+        int Pbig_all = Psmall;
+        while (Pbig_all < maxcap_all) Pbig_all <<= 1;
+        TS_CUDA_TRY(ctx, cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              std::max(W * Psmall, Pbig_all) * 8));
+        std::vector<int> retry;
+        auto launch = [&](size_t k) -> int {
+            const Chunk& c = chunks[k];
+            const Set& z = set[k & 1];
+            const int nr = int(c.c1 - c.c0);
             if (st) st->chunks++;
-            const int nr = int(ray_of.size());
-            TS_BUF(ctx, d_ray_of, int, "rays.ray_of", nr);
-            TS_BUF(ctx, d_base, int64_t, "rays.rec_base", nr);
-            TS_BUF(ctx, d_cap, int, "rays.rec_cap", nr);
-            TS_BUF(ctx, rec_node, int, "rays.rec_node", size_t(used));
-            TS_BUF(ctx, rec_val, double, "rays.rec_val", size_t(used));
-            TS_BUF(ctx, rec_count, int, "rays.rec_count", nr);
-            TS_BUF(ctx, out_node, int, "rays.out_node", size_t(used));
-            TS_BUF(ctx, out_len, float, "rays.out_len", size_t(used));
-            TS_BUF(ctx, nnz, int, "rays.nnz", nr);
-            TS_BUF(ctx, off, int, "rays.off", nr);
-            TS_BUF(ctx, sums, long long, "rays.sums", 2);
-            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ray_of, ray_of.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
-            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_base, base.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice, s));
-            TS_CUDA_TRY(ctx, cudaMemcpyAsync(d_cap, caps.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
-            a.ray_of = d_ray_of;
+            a.ray_of = d_ray_of + c.c0;
             a.nrays = nr;
-            a.rec_base = d_base;
-            a.rec_cap = d_cap;
-            a.rec_node = rec_node;
-            a.rec_val = rec_val;
-            a.rec_count = rec_count;
+            a.rec_base = d_base + c.c0;
+            a.rec_cap = d_cap + c.c0;
+            a.rec_node = z.rec_node;
+            a.rec_val = z.rec_val;
+            a.rec_count = z.rec_count;
             trace_kernel<<<(nr + 127) / 128, 128, 0, s>>>(a);
             TS_CUDA_TRY(ctx, cudaGetLastError());
-            // Small sort size for most rays; the rest in a second pass with one warp per block.
-            const int Psmall = 2048, W = 4;
             int Pbig = Psmall;
-            while (Pbig < maxcap) Pbig <<= 1;
-            TS_CUDA_TRY(ctx, cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  std::max(W * Psmall, Pbig) * 8));
+            while (Pbig < c.maxcap) Pbig <<= 1;
             merge_kernel<<<std::min((nr + W - 1) / W, ctx->sm_count * 8), W * 32, size_t(W) * Psmall * 8, s>>>(
-                rec_node, rec_val, rec_count, d_base, nr, Psmall, 0, out_node, out_len, nnz);
+                z.rec_node, z.rec_val, z.rec_count, d_base + c.c0, nr, Psmall, 0, z.out_node, z.out_len, z.nnz);
             TS_CUDA_TRY(ctx, cudaGetLastError());
             if (Pbig > Psmall) {
                 merge_kernel<<<std::min(nr, ctx->sm_count * 2), 32, size_t(Pbig) * 8, s>>>(
-                    rec_node, rec_val, rec_count, d_base, nr, Pbig, Psmall, out_node, out_len, nnz);
+                    z.rec_node, z.rec_val, z.rec_count, d_base + c.c0, nr, Pbig, Psmall, z.out_node, z.out_len, z.nnz);
                 TS_CUDA_TRY(ctx, cudaGetLastError());
             }
-            scan_kernel<<<1, 1024, 0, s>>>(nnz, nr, off, sums);
-            long long h_sums[2] = {0, 0};
-            TS_CUDA_TRY(ctx, cudaMemcpyAsync(h_sums, sums, sizeof h_sums, cudaMemcpyDeviceToHost, s));
-            TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-            if (h_sums[1] > 0) {
-                // Rays that ran out of room: traced again later with four times the room.
+            scan_kernel<<<1, 1024, 0, s>>>(z.nnz, nr, z.off, z.sums);
+            TS_CUDA_TRY(ctx, cudaMemcpyAsync(h_sums + 2 * (k & 1), z.sums, sizeof(long long) * 2,
+                                             cudaMemcpyDeviceToHost, s));
+            TS_CUDA_TRY(ctx, cudaEventRecord(done.e[k & 1], s));
+            return TS_OK;
+        };
+        auto finish = [&](size_t k) -> int {
+            const Chunk& c = chunks[k];
+            const Set& z = set[k & 1];
+            const int nr = int(c.c1 - c.c0);
+            TS_CUDA_TRY(ctx, cudaEventSynchronize(done.e[k & 1]));
+            const long long tot = h_sums[2 * (k & 1)], over = h_sums[2 * (k & 1) + 1];
+            if (over > 0) {
+                // Rays that ran out of room: traced again later with four times the room. (The set's
+                // sizes are not overwritten before this chunk's staging copy below.)
                 std::vector<int> hn(nr);
-                TS_CUDA_TRY(ctx, cudaMemcpy(hn.data(), nnz, sizeof(int) * nr, cudaMemcpyDeviceToHost));
+                TS_CUDA_TRY(ctx, cudaMemcpyAsync(hn.data(), z.nnz, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+                TS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
                 for (int r = 0; r < nr; r++) {
                     if (hn[r] != kOverflow) continue;
-                    const int q = ray_of[r];
-                    if (cap_of[q] >= kMaxCap) {
-                        free_stage();
-                        return bail(ctx->fail(TS_E_CAPACITY, "a ray needs more records than supported"));
-                    }
+                    const int q = pending[c.c0 + r];
+                    if (cap_of[q] >= kMaxCap)
+                        return ctx->fail(TS_E_CAPACITY, "a ray needs more records than supported");
                     cap_of[q] = std::min(kMaxCap, cap_of[q] * 4);
                     retry.push_back(q);
                 }
                 if (st) st->retraced_chunks++;
             }
-            if (stage_used + h_sums[0] > stage_cap) {
-                const int64_t want = std::max<int64_t>({stage_used + h_sums[0], stage_cap * 2, 1024});
+            if (stage_used + tot > stage_cap) {
+                const int64_t want = std::max<int64_t>({stage_used + tot, stage_cap * 2, 1024});
                 int* ncol = nullptr;
                 float* nlen = nullptr;
                 if (cudaMallocAsync(reinterpret_cast<void**>(&ncol), sizeof(int) * want, s) != cudaSuccess ||
                     cudaMallocAsync(reinterpret_cast<void**>(&nlen), sizeof(float) * want, s) != cudaSuccess) {
                     cudaGetLastError();
                     if (ncol) cudaFreeAsync(ncol, s);
-                    free_stage();
-                    return bail(ctx->fail(TS_E_NOMEM, "row staging arrays"));
+                    return ctx->fail(TS_E_NOMEM, "row staging arrays");
                 }
                 if (stage_used > 0) {
                     cudaMemcpyAsync(ncol, stage_col, sizeof(int) * stage_used, cudaMemcpyDeviceToDevice, s);
@@ -650,10 +722,20 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
                 stage_cap = want;
             }
             stage_kernel<<<std::min((nr + 7) / 8, ctx->sm_count * 16), 256, 0, s>>>(
-                out_node, out_len, nnz, off, d_base, d_ray_of, nr, stage_used, stage_col, stage_len, stage_off,
-                ray_nnz);
+                z.out_node, z.out_len, z.nnz, z.off, d_base + c.c0, d_ray_of + c.c0, nr, stage_used, stage_col,
+                stage_len, stage_off, ray_nnz);
             TS_CUDA_TRY(ctx, cudaGetLastError());
-            stage_used += h_sums[0];
+            stage_used += tot;
+            return TS_OK;
+        };
+        for (size_t k = 0; k < chunks.size(); k++) {
+            int rc = launch(k);
+            if (rc == TS_OK && k > 0) rc = finish(k - 1);
+            if (rc != TS_OK) return bail(rc);
+        }
+        if (!chunks.empty()) {
+            const int rc = finish(chunks.size() - 1);
+            if (rc != TS_OK) return bail(rc);
         }
         pending.swap(retry);
     }
