@@ -17,8 +17,7 @@ const std::vector<TileShapeInfo>& tile_shapes() {
     // orderings specialised).
     static const std::vector<TileShapeInfo> shapes = {{0, 8, 8, 8}, {1, 16, 8, 4}, {2, 8, 8, 4}, {3, 8, 4, 4},
                                                       {4, 32, 8, 4}, {5, 64, 8, 4}, {6, 32, 8, 4},
-                                                      {7, 32, 8, 4}, {8, 32, 8, 4}, {9, 32, 8, 4}, {10, 32, 8, 4},
-                                                      {11, 32, 8, 4}, {12, 32, 8, 4}};
+                                                      {7, 32, 8, 4}, {8, 32, 8, 4}, {9, 32, 8, 4}, {10, 32, 8, 4}};
     return shapes;
 }
 
@@ -575,10 +574,6 @@ int engine_epoch(ts_ctx* ctx, const std::vector<const host::Grid*>& grids,
         // 10: as 6 (12 warps per SM) with the same register savings.
         case 9: return launch_epoch<Real, 32, 8, 4, 4, 4, true, kRing2 | kLazyW | kSpecAll | kReshuffle>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         case 10: return launch_epoch<Real, 32, 8, 4, 4, F64 ? 3 : 4, true, kRing2 | kLazyW | kReshuffle>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
-        // 11: as 6 with one copy of the step per sweep ordering (a shifting prefetch ring);
-        // 12: as 9 (16 warps per SM) likewise.
-        case 11: return launch_epoch<Real, 32, 8, 4, 4, F64 ? 3 : 4, true, kRoll>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
-        case 12: return launch_epoch<Real, 32, 8, 4, 4, 4, true, kRoll | kLazyW | kSpecAll | kReshuffle>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
         default: return launch_epoch<Real, 8, 8, 8, F64 ? 5 : 8, 1>(ctx, grids, metrics, fields, tol, wake_rel, max_rounds, stats, s);
     }
 }

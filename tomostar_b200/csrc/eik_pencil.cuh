@@ -52,9 +52,7 @@ TS_DEVINL RowMask<BX> row_reverse(RowMask<BX> m) {
 // kSpecAll — the sweep ordering fixed at compile time whatever the width and occupancy (lockstep).
 // kReshuffle — the y and z neighbour values are fetched again for the wake tests after an update
 // instead of being held through it (within a step no lane changes the window values it shares).
-// kRoll — a two-deep prefetch ring that shifts by one value a step, so that the step loop holds one
-// copy of the step instead of one per ring slot (a quarter of the code per sweep ordering).
-constexpr int kRing2 = 1, kLazyW = 2, kSpecAll = 4, kReshuffle = 8, kRoll = 16;
+constexpr int kRing2 = 1, kLazyW = 2, kSpecAll = 4, kReshuffle = 8;
 
 template <typename Real, int BX, bool VARZ, int SDIR, int OPT = 0>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
@@ -87,8 +85,7 @@ template <typename Real, int BX, bool VARZ, int SDIR, int OPT>
 TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const FieldDesc<Real>& fd, int f, int tx, int ty,
                              int tz, int dir, bool second, Real* halo, int lane) {
     static_assert(BX == 32 || BX == 64, "pencil rows are 32 or 64 nodes");
-    constexpr bool ROLL = (OPT & kRoll) != 0;
-    constexpr int RING = (ROLL || (OPT & kRing2)) ? 2 : 4;  // prefetch depth (steps ahead)
+    constexpr int RING = (OPT & kRing2) ? 2 : 4;  // prefetch depth (steps ahead)
     constexpr bool LAZYW = (OPT & kLazyW) != 0;
     constexpr bool RESHUFFLE = (OPT & kReshuffle) != 0;
     constexpr int BY = kPencilBY, BZ = kPencilBZ, HX = Layout<Real>::HX;
@@ -215,142 +212,119 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
     unsigned wxh = 0;  // bits 0..3: canonical x = −1, −2, BX, BX+1
     bool big = false;
     int evals = 0;
-    // One step of the warp: every lane's canonical x = ip, whose slowness is sv.
-    auto step = [&](const int ip, const Real sv) {
-        const bool is_due = (due >> (ip & (BX - 1))) & (unsigned(ip) < unsigned(BX));
-        if (__any_sync(FULL, is_due)) {
-            // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
-            // ahead has not (offset +1); two rows away likewise at offsets ∓2.
-            Real yb1 = shfl_up_r(FULL, W1, 1), ya1 = shfl_down_r(FULL, W3, 1);
-            Real yb2 = shfl_up_r(FULL, W0, 2), ya2 = shfl_down_r(FULL, W4, 2);
-            Real zb1 = shfl_up_r(FULL, W1, 8), za1 = shfl_down_r(FULL, W3, 8);
-            Real zb2 = shfl_up_r(FULL, W0, 16), za2 = shfl_down_r(FULL, W4, 16);
-            bool chg = false;
-            if (is_due) {
-                const int x = ax(ip);
-                if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
-                if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
-                if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
-                if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
-                if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
-                if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
-                if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
-                if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
-                due &= ~(kOne << ip);
-                evals++;
-                // Canonical → grid orientation (minus = smaller grid index).
-                const Real xm = mx ? W3 : W1, xp = mx ? W1 : W3, xm2 = mx ? W4 : W0, xp2 = mx ? W0 : W4;
-                const Real ym = my ? ya1 : yb1, yp = my ? yb1 : ya1, ym2 = my ? ya2 : yb2, yp2 = my ? yb2 : ya2;
-                const Real zm = mz ? za1 : zb1, zp = mz ? zb1 : za1, zm2 = mz ? za2 : zb2, zp2 = mz ? zb2 : za2;
-                if constexpr (LAZYW) {  // due lanes lie on the grid (off-grid rows are fixed)
-                    wx1 = ldg_r(&wxp[2 * rowi]);
-                    wx2 = ldg_r(&wxp[2 * rowi + 1]);
-                    wy1 = ldg_r(&wyp[2 * gz]);
-                    wy2 = ldg_r(&wyp[2 * gz + 1]);
-                }
-                const Real cand = Update<Real, VARZ>::eval(sv, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
-                                                           zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
-                if (cand < W2) {
-                    if (counts_as_change<Real>(W2, cand, tol)) big = true;
-                    chg = wakes<Real>(W2, cand, wake_rel);
-                    W2 = cand;
-                    st_cg(row + x, cand);
-                }
-            }
-            const unsigned cb = __ballot_sync(FULL, chg);
-            if (cb) {
-                if constexpr (RESHUFFLE) {
-                    yb1 = shfl_up_r(FULL, W1, 1);
-                    ya1 = shfl_down_r(FULL, W3, 1);
-                    yb2 = shfl_up_r(FULL, W0, 2);
-                    ya2 = shfl_down_r(FULL, W4, 2);
-                    zb1 = shfl_up_r(FULL, W1, 8);
-                    za1 = shfl_down_r(FULL, W3, 8);
-                    zb2 = shfl_up_r(FULL, W0, 16);
-                    za2 = shfl_down_r(FULL, W4, 16);
-                    if (chg) {
-                        const int x = ax(ip);
-                        if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
-                        if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
-                        if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
-                        if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
-                        if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
-                        if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
-                        if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
-                        if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
+    constexpr int NSTEPS = (BX + BY + BZ - 2 + RING - 1) / RING * RING;
+    for (int p0 = 0; p0 < NSTEPS; p0 += RING) {
+#pragma unroll
+        for (int u = 0; u < RING; u++) {
+            const int ip = p0 + u + ip0;
+            const bool is_due = (due >> (ip & (BX - 1))) & (unsigned(ip) < unsigned(BX));
+            if (__any_sync(FULL, is_due)) {
+                // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
+                // ahead has not (offset +1); two rows away likewise at offsets ∓2.
+                Real yb1 = shfl_up_r(FULL, W1, 1), ya1 = shfl_down_r(FULL, W3, 1);
+                Real yb2 = shfl_up_r(FULL, W0, 2), ya2 = shfl_down_r(FULL, W4, 2);
+                Real zb1 = shfl_up_r(FULL, W1, 8), za1 = shfl_down_r(FULL, W3, 8);
+                Real zb2 = shfl_up_r(FULL, W0, 16), za2 = shfl_down_r(FULL, W4, 16);
+                bool chg = false;
+                if (is_due) {
+                    const int x = ax(ip);
+                    if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
+                    if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
+                    if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                    if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
+                    if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
+                    if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
+                    if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                    if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
+                    due &= ~(kOne << ip);
+                    evals++;
+                    // Canonical → grid orientation (minus = smaller grid index).
+                    const Real xm = mx ? W3 : W1, xp = mx ? W1 : W3, xm2 = mx ? W4 : W0, xp2 = mx ? W0 : W4;
+                    const Real ym = my ? ya1 : yb1, yp = my ? yb1 : ya1, ym2 = my ? ya2 : yb2, yp2 = my ? yb2 : ya2;
+                    const Real zm = mz ? za1 : zb1, zp = mz ? zb1 : za1, zm2 = mz ? za2 : zb2, zp2 = mz ? zb2 : za2;
+                    if constexpr (LAZYW) {  // due lanes lie on the grid (off-grid rows are fixed)
+                        wx1 = ldg_r(&wxp[2 * rowi]);
+                        wx2 = ldg_r(&wxp[2 * rowi + 1]);
+                        wy1 = ldg_r(&wyp[2 * gz]);
+                        wy2 = ldg_r(&wyp[2 * gz + 1]);
+                    }
+                    const Real cand = Update<Real, VARZ>::eval(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
+                                                               zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
+                    if (cand < W2) {
+                        if (counts_as_change<Real>(W2, cand, tol)) big = true;
+                        chg = wakes<Real>(W2, cand, wake_rel);
+                        W2 = cand;
+                        st_cg(row + x, cand);
                     }
                 }
-                // A changed node wakes its 12 stencil neighbours (with the causal rule, those
-                // holding more than its new value W2). The y and z neighbours are woken through
-                // one ballot per direction: a change one row back wakes x = i'+1 of this row,
-                // one row ahead x = i'−1, and two rows back or ahead x = i'±2.
-                auto wk_if = [&](Real v) { return chg && (!causal || W2 < v); };
-                Mask wk = 0;
-                if (wk_if(W1)) wk |= bit(ip - 1);
-                if (wk_if(W3)) wk |= bit(ip + 1);
-                if (wk_if(W0)) wk |= bit(ip - 2);
-                if (wk_if(W4)) wk |= bit(ip + 2);
-                const unsigned Byb1 = __ballot_sync(FULL, wk_if(yb1)), Bya1 = __ballot_sync(FULL, wk_if(ya1));
-                const unsigned Byb2 = __ballot_sync(FULL, wk_if(yb2)), Bya2 = __ballot_sync(FULL, wk_if(ya2));
-                const unsigned Bzb1 = __ballot_sync(FULL, wk_if(zb1)), Bza1 = __ballot_sync(FULL, wk_if(za1));
-                const unsigned Bzb2 = __ballot_sync(FULL, wk_if(zb2)), Bza2 = __ballot_sync(FULL, wk_if(za2));
-                if ((jp >= 1 && ((Bya1 >> (lane - 1)) & 1u)) || (kp >= 1 && ((Bza1 >> (lane - 8)) & 1u)))
-                    wk |= bit(ip + 1);
-                if ((jp <= BY - 2 && ((Byb1 >> (lane + 1)) & 1u)) || (kp <= BZ - 2 && ((Bzb1 >> (lane + 8)) & 1u)))
-                    wk |= bit(ip - 1);
-                if ((jp >= 2 && ((Bya2 >> (lane - 2)) & 1u)) || (kp >= 2 && ((Bza2 >> (lane - 16)) & 1u)))
-                    wk |= bit(ip + 2);
-                if ((jp <= BY - 3 && ((Byb2 >> (lane + 2)) & 1u)) || (kp <= BZ - 3 && ((Bzb2 >> (lane + 16)) & 1u)))
-                    wk |= bit(ip - 2);
-                due |= wk & ~fixed;
-                if (chg) {
-                    // Neighbours in other tiles (their values are the halo's, fixed in this visit).
-                    const Mask b = kOne << ip;
-                    if ((hy_m1 >= 0 && wk_if(yb1)) || (hy_p1 >= 0 && wk_if(ya1))) wky1 |= b;
-                    if ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2))) wky2 |= b;
-                    if ((hz_m1 >= 0 && wk_if(zb1)) || (hz_p1 >= 0 && wk_if(za1))) wkz1 |= b;
-                    if ((hz_m2 >= 0 && wk_if(zb2)) || (hz_p2 >= 0 && wk_if(za2))) wkz2 |= b;
-                    if (ip == 0 && wk_if(W1)) wxh |= 1u;
-                    if (ip <= 1 && wk_if(W0)) wxh |= ip == 0 ? 2u : 1u;
-                    if (ip == BX - 1 && wk_if(W3)) wxh |= 4u;
-                    if (ip >= BX - 2 && wk_if(W4)) wxh |= ip == BX - 1 ? 8u : 4u;
+                const unsigned cb = __ballot_sync(FULL, chg);
+                if (cb) {
+                    if constexpr (RESHUFFLE) {
+                        yb1 = shfl_up_r(FULL, W1, 1);
+                        ya1 = shfl_down_r(FULL, W3, 1);
+                        yb2 = shfl_up_r(FULL, W0, 2);
+                        ya2 = shfl_down_r(FULL, W4, 2);
+                        zb1 = shfl_up_r(FULL, W1, 8);
+                        za1 = shfl_down_r(FULL, W3, 8);
+                        zb2 = shfl_up_r(FULL, W0, 16);
+                        za2 = shfl_down_r(FULL, W4, 16);
+                        if (chg) {
+                            const int x = ax(ip);
+                            if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
+                            if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
+                            if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                            if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
+                            if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
+                            if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
+                            if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                            if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
+                        }
+                    }
+                    // A changed node wakes its 12 stencil neighbours (with the causal rule, those
+                    // holding more than its new value W2). The y and z neighbours are woken through
+                    // one ballot per direction: a change one row back wakes x = i'+1 of this row,
+                    // one row ahead x = i'−1, and two rows back or ahead x = i'±2.
+                    auto wk_if = [&](Real v) { return chg && (!causal || W2 < v); };
+                    Mask wk = 0;
+                    if (wk_if(W1)) wk |= bit(ip - 1);
+                    if (wk_if(W3)) wk |= bit(ip + 1);
+                    if (wk_if(W0)) wk |= bit(ip - 2);
+                    if (wk_if(W4)) wk |= bit(ip + 2);
+                    const unsigned Byb1 = __ballot_sync(FULL, wk_if(yb1)), Bya1 = __ballot_sync(FULL, wk_if(ya1));
+                    const unsigned Byb2 = __ballot_sync(FULL, wk_if(yb2)), Bya2 = __ballot_sync(FULL, wk_if(ya2));
+                    const unsigned Bzb1 = __ballot_sync(FULL, wk_if(zb1)), Bza1 = __ballot_sync(FULL, wk_if(za1));
+                    const unsigned Bzb2 = __ballot_sync(FULL, wk_if(zb2)), Bza2 = __ballot_sync(FULL, wk_if(za2));
+                    if ((jp >= 1 && ((Bya1 >> (lane - 1)) & 1u)) || (kp >= 1 && ((Bza1 >> (lane - 8)) & 1u)))
+                        wk |= bit(ip + 1);
+                    if ((jp <= BY - 2 && ((Byb1 >> (lane + 1)) & 1u)) || (kp <= BZ - 2 && ((Bzb1 >> (lane + 8)) & 1u)))
+                        wk |= bit(ip - 1);
+                    if ((jp >= 2 && ((Bya2 >> (lane - 2)) & 1u)) || (kp >= 2 && ((Bza2 >> (lane - 16)) & 1u)))
+                        wk |= bit(ip + 2);
+                    if ((jp <= BY - 3 && ((Byb2 >> (lane + 2)) & 1u)) || (kp <= BZ - 3 && ((Bzb2 >> (lane + 16)) & 1u)))
+                        wk |= bit(ip - 2);
+                    due |= wk & ~fixed;
+                    if (chg) {
+                        // Neighbours in other tiles (their values are the halo's, fixed in this visit).
+                        const Mask b = kOne << ip;
+                        if ((hy_m1 >= 0 && wk_if(yb1)) || (hy_p1 >= 0 && wk_if(ya1))) wky1 |= b;
+                        if ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2))) wky2 |= b;
+                        if ((hz_m1 >= 0 && wk_if(zb1)) || (hz_p1 >= 0 && wk_if(za1))) wkz1 |= b;
+                        if ((hz_m2 >= 0 && wk_if(zb2)) || (hz_p2 >= 0 && wk_if(za2))) wkz2 |= b;
+                        if (ip == 0 && wk_if(W1)) wxh |= 1u;
+                        if (ip <= 1 && wk_if(W0)) wxh |= ip == 0 ? 2u : 1u;
+                        if (ip == BX - 1 && wk_if(W3)) wxh |= 4u;
+                        if (ip >= BX - 2 && wk_if(W4)) wxh |= ip == BX - 1 ? 8u : 4u;
+                    }
                 }
             }
-        }
-    };
-    if constexpr (ROLL) {
-        // One copy of the step: the prefetch ring shifts by one value a step.
-        constexpr int NSTEPS = BX + BY + BZ - 2;
-#pragma unroll 1
-        for (int p = 0; p < NSTEPS; p++) {
-            const int ip = p + ip0;
-            step(ip, sr[0]);
+            // Slide the window one node and refill the rings four nodes ahead.
             W0 = W1;
             W1 = W2;
             W2 = W3;
             W3 = W4;
-            W4 = tr[0];
-            tr[0] = tr[1];
-            tr[1] = ldT(ip + 5);
-            sr[0] = sr[1];
-            sr[1] = ldS(ip + 2);
-        }
-    } else {
-        constexpr int NSTEPS = (BX + BY + BZ - 2 + RING - 1) / RING * RING;
-        for (int p0 = 0; p0 < NSTEPS; p0 += RING) {
-#pragma unroll
-            for (int u = 0; u < RING; u++) {
-                const int ip = p0 + u + ip0;
-                step(ip, sr[u]);
-                // Slide the window one node and refill the rings RING nodes ahead.
-                W0 = W1;
-                W1 = W2;
-                W2 = W3;
-                W3 = W4;
-                W4 = tr[u];
-                tr[u] = ldT(ip + 3 + RING);
-                sr[u] = ldS(ip + RING);
-            }
+            W4 = tr[u];
+            tr[u] = ldT(ip + 3 + RING);
+            sr[u] = ldS(ip + RING);
         }
     }
 

@@ -87,35 +87,25 @@ TS_DEVINL void sort3(R* t, R* h, R* n) {
     }
 }
 
-// The Godunov root over the first `terms` sorted terms (SphericalEikonal.cs:364-378) is taken for the
-// largest term count first and, when it fails, for one term fewer. The sums of k terms are the running
-// sums after the k-th term (the reference adds the terms in sorted order), so they are formed once;
-// the candidates of the two largest term counts are then evaluated side by side, which keeps the
-// second square root and divide off the critical path of the nodes that need them (about one update
-// in ten needs the second; most steps of a warp hold at least one such node). Each candidate takes
-// the reference's operations in its order, so the result is the same bits.
-struct Sums64 {
-    double sw, swt, swt2;
-};
-
-TS_DEVINL Sums64 add_term(Sums64 q, double w, double t) {
-    q.sw = dadd(q.sw, w);
-    q.swt = dadd(q.swt, dmul(w, t));
-    q.swt2 = dadd(q.swt2, dmul(dmul(w, t), t));
-    return q;
-}
-
-// The candidate of `terms` terms from their sums; false when the discriminant is negative or the root
-// falls below a neighbour it used. A negative discriminant takes the square root of 1 instead (that
-// candidate is discarded), so that no lane enters the special-operand path for it.
-TS_DEVINL bool root_from(const Sums64& q, int terms, const double* n, double s, double& root) {
-    const double disc = dsub(dmul(q.swt, q.swt), dmul(q.sw, dsub(q.swt2, dmul(s, s))));
-    bool ok = !(disc < 0.0);
-    root = ddiv(dadd(q.swt, __dsqrt_rn(ok ? disc : 1.0)), q.sw);
+// The Godunov root over the first `terms` sorted terms; false when the discriminant is negative
+// or the root falls below a neighbour it used (SphericalEikonal.cs:364-378).
+TS_DEVINL bool root64(int terms, const double* t, const double* w, const double* n, double s, double& root) {
+    double sw = 0.0, swt = 0.0, swt2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        if (r < terms) {
+            sw = dadd(sw, w[r]);
+            swt = dadd(swt, dmul(w[r], t[r]));
+            swt2 = dadd(swt2, dmul(dmul(w[r], t[r]), t[r]));
+        }
+    }
+    double disc = dsub(dmul(swt, swt), dmul(sw, dsub(swt2, dmul(s, s))));
+    if (disc < 0.0) return false;
+    root = ddiv(dadd(swt, __dsqrt_rn(disc)), sw);
 #pragma unroll
     for (int r = 0; r < 3; r++)
-        if (r < terms && root < n[r]) ok = false;
-    return ok;
+        if (r < terms && root < n[r]) return false;
+    return true;
 }
 
 // RelaxNode (SphericalEikonal.cs:349-379): the candidate time of a node from its 12 neighbour
@@ -134,17 +124,10 @@ TS_DEVINL double update64(double s, double xm, double xp, double xm2, double xp2
     axis64<VARZ>(zm, zp, zm2, zp2, wz1, wz2, zc, second, t[2], w[2], n[2], used);
     if (used == 0) return inf;
     sort3(t, w, n);
-    const Sums64 q1 = add_term(Sums64{0.0, 0.0, 0.0}, w[0], t[0]);
-    const Sums64 q2 = add_term(q1, w[1], t[1]);
-    const Sums64 q3 = add_term(q2, w[2], t[2]);
-    const Sums64 qa = used == 3 ? q3 : (used == 2 ? q2 : q1);  // `used` terms
-    const Sums64 qb = used == 3 ? q2 : q1;                      // one fewer
-    double ra, rb;
-    const bool oka = root_from(qa, used, n, s, ra);
-    const bool okb = root_from(qb, used - 1, n, s, rb) && used >= 2;
-    if (oka) return ra;
-    if (okb) return rb;
-    if (used == 3 && root_from(q1, 1, n, s, ra)) return ra;
+    double root;
+    if (used >= 3 && root64(3, t, w, n, s, root)) return root;
+    if (used >= 2 && root64(2, t, w, n, s, root)) return root;
+    if (root64(1, t, w, n, s, root)) return root;
     return inf;
 }
 
@@ -211,28 +194,25 @@ TS_DEVINL void termp(const PickP& p, Pair r, float w1, float w2, const Pair* zc,
 }
 
 // The root over the first `terms` sorted terms, as offsets from base = te[0] (EikonalOpenCl.cs:575-597).
-// As in FP64, the sums of k terms are the running sums after the k-th term, and the candidates of the
-// two largest term counts are evaluated side by side.
-struct SumsP {
-    float sw, swd, swd2;
-};
-
-TS_DEVINL SumsP add_termp(SumsP q, float w, float t, float base) {
-    const float d = fsub(t, base);
-    q.sw = fadd(q.sw, w);
-    q.swd = fadd(q.swd, fmul(w, d));
-    q.swd2 = fadd(q.swd2, fmul(fmul(w, d), d));
-    return q;
-}
-
-TS_DEVINL bool rootp_from(const SumsP& q, int terms, const float* n, float s, float base, float& root) {
-    const float disc = fsub(fmul(q.swd, q.swd), fmul(q.sw, fsub(q.swd2, fmul(s, s))));
-    bool ok = !(disc < 0.f);
-    root = fadd(base, fdiv(fadd(q.swd, __fsqrt_rn(ok ? disc : 1.f)), q.sw));
+TS_DEVINL bool rootp(int terms, const float* t, const float* w, const float* n, float s, float& root) {
+    const float base = t[0];
+    float sw = 0.f, swd = 0.f, swd2 = 0.f;
 #pragma unroll
-    for (int r = 0; r < 3; r++)
-        if (r < terms && root < n[r]) ok = false;
-    return ok;
+    for (int q = 0; q < 3; q++) {
+        if (q < terms) {
+            const float d = fsub(t[q], base);
+            sw = fadd(sw, w[q]);
+            swd = fadd(swd, fmul(w[q], d));
+            swd2 = fadd(swd2, fmul(fmul(w[q], d), d));
+        }
+    }
+    const float disc = fsub(fmul(swd, swd), fmul(sw, fsub(swd2, fmul(s, s))));
+    if (disc < 0.f) return false;
+    root = fadd(base, fdiv(fadd(swd, __fsqrt_rn(disc)), sw));
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+        if (q < terms && root < n[q]) return false;
+    return true;
 }
 
 // The paired candidate time of a node (same inputs as update64; slowness and weights in hi).
@@ -259,18 +239,9 @@ TS_DEVINL Pair updatep(Pair sp, Pair xm, Pair xp, Pair xm2, Pair xp2, Pair ym, P
     if (py.ok) { termp<false>(py, r, wy1.hi, wy2.hi, nullptr, second, t[1], w[1], n[1]); used++; }
     if (pz.ok) { termp<VARZ>(pz, r, wz1.hi, wz2.hi, zc, second, t[2], w[2], n[2]); used++; }
     sort3(t, w, n);
-    const float base = t[0];
-    const SumsP q1 = add_termp(SumsP{0.f, 0.f, 0.f}, w[0], t[0], base);
-    const SumsP q2 = add_termp(q1, w[1], t[1], base);
-    const SumsP q3 = add_termp(q2, w[2], t[2], base);
-    const SumsP qa = used == 3 ? q3 : (used == 2 ? q2 : q1);  // `used` terms
-    const SumsP qb = used == 3 ? q2 : q1;                      // one fewer
-    float ra, rb, root;
-    const bool oka = rootp_from(qa, used, n, s, base, ra);
-    const bool okb = rootp_from(qb, used - 1, n, s, base, rb) && used >= 2;
-    const bool found = oka || okb || (used == 3 && rootp_from(q1, 1, n, s, base, root));
-    if (oka) root = ra;
-    else if (okb) root = rb;
+    float root;
+    const bool found = (used >= 3 && rootp(3, t, w, n, s, root)) || (used >= 2 && rootp(2, t, w, n, s, root)) ||
+                       rootp(1, t, w, n, s, root);
     if (!found || !finite_r(root)) return inf;
     return padd(r, root);
 }
