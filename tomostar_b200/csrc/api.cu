@@ -65,6 +65,21 @@ int ts_cuda_create(int32_t device, ts_ctx** out) {
         delete ctx;
         return TS_E_CUDA;
     }
+    {
+        // The context's pool for stream-ordered allocations (without one they come from the device's
+        // default pool, which releases freed memory at every synchronisation).
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+            uint64_t keep = prop.totalGlobalMem / 4;
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            cudaGetLastError();
+            ctx->pool = nullptr;
+        }
+    }
     *out = ctx;
     return TS_OK;
 }
@@ -85,6 +100,8 @@ void ts_cuda_destroy(ts_ctx* ctx) {
         if (ctx->cancel_host) cudaFreeHost(const_cast<int*>(ctx->cancel_host));
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         cudaStreamDestroy(ctx->stream);
+        // Allocations still held (rows not yet freed) keep the pool's memory until they are freed.
+        if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     }
     delete ctx;
 }

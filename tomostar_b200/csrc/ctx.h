@@ -39,6 +39,17 @@ struct ts_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_replays = 0;
 
+    // Stream-ordered allocations (rows, row staging, serving blocks) come from the context's own pool.
+    // It keeps what they free, up to a quarter of the device's memory, for the next call: a pool that
+    // hands freed memory back at every synchronisation maps it again on the next call, which made the
+    // ray pipeline of a 1.5 M-row forward step take 1.3-2.2 s on the device instead of 0.75-0.85 s.
+    cudaMemPool_t pool = nullptr;
+    template <typename T>
+    cudaError_t alloc_async(T** p, size_t bytes, cudaStream_t s) {
+        void** q = reinterpret_cast<void**>(p);
+        return pool ? cudaMallocFromPoolAsync(q, bytes, pool, s) : cudaMallocAsync(q, bytes, s);
+    }
+
     struct Model;
     std::map<int, Model*> models;
     int next_model = 1;

@@ -457,10 +457,10 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     rows->ctx = ctx;
     rows->n_rows = n_rays;
     auto bail = [&](int code) { return code; };
-    if (cudaMallocAsync(reinterpret_cast<void**>(&rows->row_ptr), sizeof(int) * (n_rays + 1), s) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&rows->tcg), sizeof(double) * 4 * std::max(1, n_rays), s) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&rows->ok), std::max(1, n_rays), s) != cudaSuccess ||
-        cudaMallocAsync(reinterpret_cast<void**>(&rows->outside), sizeof(double) * std::max(1, n_rays), s) !=
+    if (ctx->alloc_async(&rows->row_ptr, sizeof(int) * (n_rays + 1), s) != cudaSuccess ||
+        ctx->alloc_async(&rows->tcg, sizeof(double) * 4 * std::max(1, n_rays), s) != cudaSuccess ||
+        ctx->alloc_async(&rows->ok, std::max(1, n_rays), s) != cudaSuccess ||
+        ctx->alloc_async(&rows->outside, sizeof(double) * std::max(1, n_rays), s) !=
             cudaSuccess) {
         cudaGetLastError();
         ctx->fail(TS_E_NOMEM, "row buffers");
@@ -706,8 +706,8 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
                 const int64_t want = std::max<int64_t>({stage_used + tot, stage_cap * 2, 1024});
                 int* ncol = nullptr;
                 float* nlen = nullptr;
-                if (cudaMallocAsync(reinterpret_cast<void**>(&ncol), sizeof(int) * want, s) != cudaSuccess ||
-                    cudaMallocAsync(reinterpret_cast<void**>(&nlen), sizeof(float) * want, s) != cudaSuccess) {
+                if (ctx->alloc_async(&ncol, sizeof(int) * want, s) != cudaSuccess ||
+                    ctx->alloc_async(&nlen, sizeof(float) * want, s) != cudaSuccess) {
                     cudaGetLastError();
                     if (ncol) cudaFreeAsync(ncol, s);
                     return ctx->fail(TS_E_NOMEM, "row staging arrays");
@@ -754,8 +754,8 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
             return bail(ctx->fail(TS_E_CAPACITY, "more than 2^31 non-zeros"));
         }
         const int64_t alloc = std::max<int64_t>(1, total);
-        if (cudaMallocAsync(reinterpret_cast<void**>(&rows->col), sizeof(int) * alloc, s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&rows->len), sizeof(float) * alloc, s) != cudaSuccess) {
+        if (ctx->alloc_async(&rows->col, sizeof(int) * alloc, s) != cudaSuccess ||
+            ctx->alloc_async(&rows->len, sizeof(float) * alloc, s) != cudaSuccess) {
             cudaGetLastError();
             free_stage();
             return bail(ctx->fail(TS_E_NOMEM, "CSR arrays"));
@@ -830,12 +830,12 @@ int split_rows(ts_ctx* ctx, const ts_rows* all, const std::vector<int>& row_begi
             }
             return ctx->fail(TS_E_NOMEM, "row buffers");
         };
-        if (cudaMallocAsync(reinterpret_cast<void**>(&p->row_ptr), sizeof(int) * (n + 1), s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&p->tcg), sizeof(double) * 4 * std::max(1, n), s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&p->ok), std::max(1, n), s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&p->outside), sizeof(double) * std::max(1, n), s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&p->col), sizeof(int) * std::max<int64_t>(1, nnz), s) != cudaSuccess ||
-            cudaMallocAsync(reinterpret_cast<void**>(&p->len), sizeof(float) * std::max<int64_t>(1, nnz), s) != cudaSuccess)
+        if (ctx->alloc_async(&p->row_ptr, sizeof(int) * (n + 1), s) != cudaSuccess ||
+            ctx->alloc_async(&p->tcg, sizeof(double) * 4 * std::max(1, n), s) != cudaSuccess ||
+            ctx->alloc_async(&p->ok, std::max(1, n), s) != cudaSuccess ||
+            ctx->alloc_async(&p->outside, sizeof(double) * std::max(1, n), s) != cudaSuccess ||
+            ctx->alloc_async(&p->col, sizeof(int) * std::max<int64_t>(1, nnz), s) != cudaSuccess ||
+            ctx->alloc_async(&p->len, sizeof(float) * std::max<int64_t>(1, nnz), s) != cudaSuccess)
             return fail();
         // From pageable memory the copy has taken the source when the call returns.
         TS_CUDA_TRY(ctx, cudaMemcpyAsync(p->row_ptr, local.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));

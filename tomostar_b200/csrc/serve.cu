@@ -147,7 +147,7 @@ void admit(ts_server* sv) {
         }
         if (sv->in_use + need > sv->budget) break;  // head of the queue waits for memory
         void* block = nullptr;
-        if (cudaMallocAsync(&block, need, sv->ctx->stream) != cudaSuccess) {
+        if (sv->ctx->alloc_async(&block, need, sv->ctx->stream) != cudaSuccess) {
             cudaGetLastError();
             break;  // the device is short of memory now: retry after the next epoch frees some
         }
