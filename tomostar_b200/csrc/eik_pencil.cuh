@@ -248,12 +248,8 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                         wy1 = ldg_r(&wyp[2 * gz]);
                         wy2 = ldg_r(&wyp[2 * gz + 1]);
                     }
-                    // Fast mode (causal wakes) takes the Newton–Raphson quotient and square root in FP64.
-                    const Real cand =
-                        causal ? Update<Real, VARZ>::eval_fast(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
-                                                               zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second)
-                               : Update<Real, VARZ>::eval(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2,
-                                                          wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
+                    const Real cand = Update<Real, VARZ>::eval(sr[u], xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2,
+                                                               zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
                     if (cand < W2) {
                         if (counts_as_change<Real>(W2, cand, tol)) big = true;
                         chg = wakes<Real>(W2, cand, wake_rel);

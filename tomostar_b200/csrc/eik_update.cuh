@@ -101,43 +101,12 @@ TS_DEVINL Sums64 add_term(Sums64 q, double w, double t) {
     return q;
 }
 
-// Fast mode only (whose bar is 1e-10 relative, not the bits): the quotient and the square root of the
-// root by Newton–Raphson from the hardware's single-precision approximations (PTX rcp.approx and
-// rsqrt.approx, about 2^-22 relative), two iterations in FP64 (each squares the relative error) and
-// one residual correction (Markstein, "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34(1), 1990). Operands outside (1e-30, 1e30), where the single-precision
-// seed could underflow or overflow, take the correctly rounded operations instead.
-TS_DEVINL double nr_div(double a, double b) {
-    if (!(b > 1e-30 && b < 1e30)) return __ddiv_rn(a, b);
-    float y0;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(__double2float_rn(b)));
-    double y = double(y0);
-    y = __fma_rn(y, __fma_rn(-b, y, 1.0), y);
-    y = __fma_rn(y, __fma_rn(-b, y, 1.0), y);
-    const double q = __dmul_rn(a, y);
-    return __fma_rn(__fma_rn(-b, q, a), y, q);
-}
-
-TS_DEVINL double nr_sqrt(double x) {
-    if (!(x > 1e-30 && x < 1e30)) return __dsqrt_rn(x);
-    float r0;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(__double2float_rn(x)));
-    double r = double(r0);
-    const double h = __dmul_rn(0.5, x);
-    r = __dmul_rn(r, __fma_rn(-h, __dmul_rn(r, r), 1.5));
-    r = __dmul_rn(r, __fma_rn(-h, __dmul_rn(r, r), 1.5));
-    const double y = __dmul_rn(x, r);
-    return __fma_rn(__fma_rn(-y, y, x), __dmul_rn(0.5, r), y);
-}
-
 // The candidate of `terms` terms from their sums; false when the discriminant is negative or the root
 // falls below a neighbour it used.
-template <bool FASTM>
 TS_DEVINL bool root_from(const Sums64& q, int terms, const double* n, double s, double& root) {
     const double disc = dsub(dmul(q.swt, q.swt), dmul(q.sw, dsub(q.swt2, dmul(s, s))));
     if (disc < 0.0) return false;
-    if constexpr (FASTM) root = nr_div(dadd(q.swt, nr_sqrt(disc)), q.sw);
-    else root = ddiv(dadd(q.swt, __dsqrt_rn(disc)), q.sw);
+    root = ddiv(dadd(q.swt, __dsqrt_rn(disc)), q.sw);
 #pragma unroll
     for (int r = 0; r < 3; r++)
         if (r < terms && root < n[r]) return false;
@@ -147,7 +116,7 @@ TS_DEVINL bool root_from(const Sums64& q, int terms, const double* n, double s, 
 // RelaxNode (SphericalEikonal.cs:349-379): the candidate time of a node from its 12 neighbour
 // values (+inf off the grid). xm/xp = i∓1, xm2/xp2 = i∓2, likewise y and z; (w1, w2) are each
 // axis's first- and second-order weights.
-template <bool VARZ, bool FASTM = false>
+template <bool VARZ>
 TS_DEVINL double update64(double s, double xm, double xp, double xm2, double xp2, double ym, double yp, double ym2,
                           double yp2, double zm, double zp, double zm2, double zp2, double wx1, double wx2,
                           double wy1, double wy2, double wz1, double wz2, const double* zc, bool second) {
@@ -164,9 +133,9 @@ TS_DEVINL double update64(double s, double xm, double xp, double xm2, double xp2
     const Sums64 q2 = add_term(q1, w[1], t[1]);
     const Sums64 q3 = add_term(q2, w[2], t[2]);
     double root;
-    if (used >= 3 && root_from<FASTM>(q3, 3, n, s, root)) return root;
-    if (used >= 2 && root_from<FASTM>(q2, 2, n, s, root)) return root;
-    if (root_from<FASTM>(q1, 1, n, s, root)) return root;
+    if (used >= 3 && root_from(q3, 3, n, s, root)) return root;
+    if (used >= 2 && root_from(q2, 2, n, s, root)) return root;
+    if (root_from(q1, 1, n, s, root)) return root;
     return inf;
 }
 
@@ -298,14 +267,6 @@ struct Update<double, VARZ> {
         return update64<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
                               zc, second);
     }
-    // Fast mode: the root's quotient and square root by Newton–Raphson (nr_div, nr_sqrt).
-    TS_DEVINL static double eval_fast(double s, double xm, double xp, double xm2, double xp2, double ym, double yp,
-                                      double ym2, double yp2, double zm, double zp, double zm2, double zp2,
-                                      double wx1, double wx2, double wy1, double wy2, double wz1, double wz2,
-                                      const double* zc, bool second) {
-        return update64<VARZ, true>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1,
-                                    wz2, zc, second);
-    }
 };
 
 template <bool VARZ>
@@ -315,12 +276,6 @@ struct Update<Pair, VARZ> {
                                Pair wz2, const Pair* zc, bool second) {
         return updatep<VARZ>(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2,
                              zc, second);
-    }
-    // The paired arithmetic has no faster form: fast mode uses it as it is.
-    TS_DEVINL static Pair eval_fast(Pair s, Pair xm, Pair xp, Pair xm2, Pair xp2, Pair ym, Pair yp, Pair ym2, Pair yp2,
-                                    Pair zm, Pair zp, Pair zm2, Pair zp2, Pair wx1, Pair wx2, Pair wy1, Pair wy2,
-                                    Pair wz1, Pair wz2, const Pair* zc, bool second) {
-        return eval(s, xm, xp, xm2, xp2, ym, yp, ym2, yp2, zm, zp, zm2, zp2, wx1, wx2, wy1, wy2, wz1, wz2, zc, second);
     }
 };
 
