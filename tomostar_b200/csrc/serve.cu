@@ -416,9 +416,9 @@ int ts_serve_create(int32_t device, int32_t precision, int32_t mode, int32_t til
     int rc = ts_cuda_create(device, &ctx);
     if (rc) return rc;
     ctx->scheduler = scheduler;
-    // Memory freed by finished requests stays with the stream-ordered pool for the next ones.
-    cudaMemPool_t pool = nullptr;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    // Memory freed by finished requests stays with the context's stream-ordered pool for the next ones.
+    cudaMemPool_t pool = ctx->pool;
+    if (pool || cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
         uint64_t keep = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
