@@ -120,10 +120,9 @@ struct Recorder {
         touched = nt;
     }
 
-    // RayTracing.Kernel for one polyline segment (RayTracing.cs:133-157).
-    TS_DEVINL void segment(const TraceArgs& a, int r, GeoPt pa, GeoPt pb) {
-        V3 A = geo::to_cartesian(pa.lon, pa.lat, pa.dep);
-        V3 B = geo::to_cartesian(pb.lon, pb.lat, pb.dep);
+    // RayTracing.Kernel for one polyline segment (RayTracing.cs:133-157), from its end points in
+    // Cartesian form (the back-tracing loop has converted both already: the same values).
+    TS_DEVINL void segment(const TraceArgs& a, int r, V3 A, V3 B) {
         V3 d = geo::sub(B, A);
         double len = geo::norm(d);
         if (len <= 0) return;
@@ -203,7 +202,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
         unsigned long long n = 0;
         TS_DEVINL ~StepCount() { atomicAdd(total, n); }
     } taken{a.steps};
-    GeoPt prev = ev;
+    V3 prev = p;  // the polyline's last point (Cartesian of the event, then of each step's point)
     for (int s = 0; s < max_steps; s++) {
         if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
         taken.n++;
@@ -231,8 +230,8 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
         q.lat = fmin(fmax(q.lat, g.min_lat), g.lat_last);
         q.dep = fmin(fmax(q.dep, g.min_dep), g.dep_last);
         p = geo::to_cartesian(q.lon, q.lat, q.dep);
-        rec.segment(a, r, prev, q);
-        prev = q;
+        rec.segment(a, r, prev, p);
+        prev = p;
         double t = geo::table_time_b(g, tb, q.lon, q.lat, q.dep);
         if (!(t < last_t)) {
             if (++stalls > 20) {
@@ -244,7 +243,7 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
         }
         last_t = fmin(last_t, t);
     }
-    rec.segment(a, r, prev, GeoPt{st_lon, st_lat, st_dep});
+    rec.segment(a, r, prev, station);
     rec.flush(a, r);
     a.outside[ray] = rec.outside;
     a.rec_count[r] = rec.overflow ? kOverflow : rec.count;
@@ -540,12 +539,19 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
     }
     const auto th1 = std::chrono::steady_clock::now();
     // Chunk budget: record slots (12 B of record + 8 B of merged output each) of two chunks in
-    // flight within a share of the free device memory, at most 400 M slots per chunk.
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    cudaGetLastError();
-    const int64_t budget = std::max<int64_t>(int64_t(kMaxCap) * 64,
-                                             std::min<int64_t>(int64_t(400) << 20, int64_t(free_b / 8 / 20)));
+    // flight within a share of the free device memory, at most 400 M slots per chunk. A call whose
+    // rooms all fit in 16 M slots (320 MB) is one chunk without asking for the free memory, which
+    // costs milliseconds per query while other work holds the device (small calls, serving).
+    int64_t need = 0;
+    for (int q = 0; q < n_rays; q++) need += cap_of[q];
+    int64_t budget = std::max<int64_t>(need, 1);
+    if (need > (int64_t(16) << 20)) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        cudaGetLastError();
+        budget = std::max<int64_t>(int64_t(kMaxCap) * 64,
+                                   std::min<int64_t>(int64_t(400) << 20, int64_t(free_b / 8 / 20)));
+    }
     TS_BUF(ctx, ray_nnz, int, "rays.ray_nnz", std::max(1, n_rays));
     TS_BUF(ctx, stage_off, long long, "rays.stage_off", std::max(1, n_rays));
     // The staging area (rows in chunk order), freed on every return.
