@@ -259,6 +259,13 @@ int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float
                   const ts_grid* inv, int32_t n_rays, const int32_t* table_of, const double* events, double step_km,
                   ts_rows** out);
 
+/* Which kernel traces a call's rays (no counterpart in the reference, whose Backtrack runs one ray
+ * per CPU thread, RayKernels.cs:67-107): a call of at most max_rays rays is traced with one warp
+ * per ray, whose lanes share each step's corner loads and gradient evaluations (the latency of a
+ * small call, such as a serving completion's, is its longest ray's); a larger call with one thread
+ * per ray. Both give the same rows to the bit. Default 1024; 0 always uses a thread per ray. */
+int ts_rays_set_warp_max(ts_ctx* ctx, int32_t max_rays);
+
 /* RayKernels.Compute for travel times (Tomography/RayKernels.cs:30-115) with the tables built on
  * the device: one field per (station, phase) used, by the engine (precision as ts_eik_solve), each
  * seeded by PointSource at the station and rounded to float32 as TravelTimeTable.Write does, then

@@ -151,3 +151,42 @@ def test_row_time_consistency(solver):
     for row in gpu.rows():
         kt = float(np.sum(row.length * s_inv[row.nodes]))
         assert abs(kt - row.tcalc) / row.tcalc < 0.05
+
+
+def _same_rows(a, b):
+    assert np.array_equal(a.row_ptr, b.row_ptr)
+    assert np.array_equal(a.col, b.col)
+    assert np.array_equal(a.len.view(np.uint32), b.len.view(np.uint32))
+    assert np.array_equal(a.tcalc_grad.view(np.uint64), b.tcalc_grad.view(np.uint64))
+    assert np.array_equal(a.ok, b.ok)
+    assert np.array_equal(a.outside.view(np.uint64), b.outside.view(np.uint64))
+
+
+def test_warp_per_ray_equals_thread_per_ray(solver):
+    """ts_rays_set_warp_max picks the kernel: one warp per ray (small calls) and one thread per ray
+    trace the same 600 P and S rays of the inversion_step_121 sample to the same rows, bit for bit,
+    and both agree with the oracle."""
+    lib = L.load()
+    p = syn.inversion_step_121()
+    og = O.Grid.of(p.grid)
+    tabs, tstations = [], []
+    for ph in (0, 1):
+        for q in (0, 4, 11):
+            si, stt = point_source(p.grid, p.slowness[ph], *p.stations[q])
+            tabs.append(O.to_table(O.relax(og, p.slowness[ph], si, stt)[0]))
+            tstations.append(p.stations[q])
+    tabs, tstations = np.stack(tabs), np.array(tstations)
+    rng = np.random.default_rng(21)
+    table_of = rng.integers(0, len(tabs), 600).astype(np.int32)
+    evs = p.events[rng.integers(0, len(p.events), 600)]
+    try:
+        assert lib.ts_rays_set_warp_max(solver.handle, 100000) == L.TS_OK
+        warp = trace_rows(solver, p.grid, tabs, tstations, p.inv, table_of, evs, p.step_km)
+        assert lib.ts_rays_set_warp_max(solver.handle, 0) == L.TS_OK
+        thread = trace_rows(solver, p.grid, tabs, tstations, p.inv, table_of, evs, p.step_km)
+    finally:
+        lib.ts_rays_set_warp_max(solver.handle, 1024)
+    _same_rows(warp, thread)
+    nnz, nodes, lens, tg = O.ray_rows_many(og, tabs, table_of, tstations[table_of], O.Grid.of(p.inv), evs, p.step_km)
+    compare_rows(warp, nnz, nodes, lens, tg)
+    assert lib.ts_rays_set_warp_max(solver.handle, -1) == L.TS_E_ARG

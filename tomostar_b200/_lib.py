@@ -184,6 +184,7 @@ SIGNATURES = {
     "ts_eik_solve_noalloc": (C.c_int, [_gp, _vp, _i32, _ip, _dp, _vp, _d, _i32, _vp, _ip]),
     "ts_cuda_selftest": (C.c_int, [_vp, _i32, _dp, C.c_char_p, _i32]),
     "ts_rays_trace": (C.c_int, [_vp, _gp, _i32, _fp, _dp, _gp, _i32, _ip, _dp, _d, _P(_vp)]),
+    "ts_rays_set_warp_max": (C.c_int, [_vp, _i32]),
     "ts_forward": (C.c_int, [_vp, _gp, _dp, _i32, _gp, _i32, _dp, _i32, _dp, _i32, _ip, _ip, _ip, _i32, _i32, _d,
                              _P(_vp), _P(EikStats)]),
     "ts_rows_info": (C.c_int, [_vp, _ip, _P(C.c_int64)]),

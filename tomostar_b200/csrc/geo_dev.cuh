@@ -208,6 +208,70 @@ TS_DEVINL void table_gradient_b(const RGrid& g, const float* tb, double lon, dou
     gz = tz / hz;
 }
 
+// ---- the same Time and Gradient computed by one warp for one point ------------------------------
+//
+// For a ray traced by a whole warp: the lanes load the corners (lane l loads corner l & 7 of
+// evaluation l >> 3, and of evaluation 4 + ((l >> 3) & 1) in a second load), each of the six
+// gradient evaluations is summed in its own lane, and every lane then takes the six sums by shuffles
+// and forms the gradient. Every value is computed with the operations and in the order of the forms
+// above, so both give the same bits. All 32 lanes must call these together.
+
+TS_DEVINL int64_t corner_offset(const RGrid& g, int n) {
+    return (n >> 2) * (int64_t(g.nx) * g.ny) + ((n >> 1) & 1) * g.nx + (n & 1);
+}
+
+TS_DEVINL double table_time_w(const RGrid& g, const float* tb, double lon, double lat, double dep, int lane) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    const float mine = __ldg(&tb[corner_base(g, fx, fy, fz) + corner_offset(g, lane & 7)]);
+    float v[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) v[n] = __shfl_sync(0xffffffffu, mine, n);
+    return sum_corners(g, fx, fy, fz, v);
+}
+
+TS_DEVINL void table_gradient_w(const RGrid& g, const float* tb, double lon, double lat, double dep, double& ge,
+                                double& gn, double& gz, int lane) {
+    double fx, fy, fz;
+    fractional(g, lon, lat, dep, fx, fy, fz);
+    const double d = 0.5;
+    auto at = [&](int e, double& ex, double& ey, double& ez) {
+        ex = e == 0 ? fx + d : e == 1 ? fx - d : fx;
+        ey = e == 2 ? fy + d : e == 3 ? fy - d : fy;
+        ez = e == 4 ? fz + d : e == 5 ? fz - d : fz;
+    };
+    const int n = lane & 7;
+    double ax, ay, az, bx, by, bz;
+    at(lane >> 3, ax, ay, az);
+    at(4 + ((lane >> 3) & 1), bx, by, bz);
+    const float va = __ldg(&tb[corner_base(g, ax, ay, az) + corner_offset(g, n)]);
+    const float vb = __ldg(&tb[corner_base(g, bx, by, bz) + corner_offset(g, n)]);
+    const int me = lane < 6 ? lane : 0;  // the evaluation this lane sums
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float x = __shfl_sync(0xffffffffu, va, 8 * (me & 3) + k);
+        const float y = __shfl_sync(0xffffffffu, vb, 8 * (me & 1) + k);
+        v[k] = me < 4 ? x : y;
+    }
+    double ex, ey, ez;
+    at(me, ex, ey, ez);
+    const double te = sum_corners(g, ex, ey, ez, v);
+    double t[6];
+#pragma unroll
+    for (int e = 0; e < 6; e++) t[e] = __shfl_sync(0xffffffffu, te, e);
+    const double tx = (t[0] - t[1]) / (2 * d);
+    const double ty = (t[2] - t[3]) / (2 * d);
+    const double tz = (t[4] - t[5]) / (2 * d);
+    double r = kEarthRadiusKm - dep;
+    double hx = r * cos(lat * kDeg2Rad) * g.dlon_rad;
+    double hy = r * g.dlat_rad;
+    double hz = g.ddep;
+    ge = tx / hx;
+    gn = ty / hy;
+    gz = tz / hz;
+}
+
 // SphericalGrid.Contains (Geo/SphericalGrid.cs:186-192).
 TS_DEVINL bool contains(const RGrid& g, double lon, double lat, double dep, double tol) {
     double fx, fy, fz;

@@ -249,6 +249,101 @@ __global__ void __launch_bounds__(128) trace_kernel(TraceArgs a) {
     a.rec_count[r] = rec.overflow ? kOverflow : rec.count;
 }
 
+// Backtrack + Kernel with one warp per ray, for calls too small to fill the device with a thread per
+// ray (a serving completion traces a few hundred): the lanes share each step's corner loads and sum
+// the six gradient evaluations side by side (table_gradient_w), every lane carries the ray's state
+// through the same arithmetic, and lane 0 integrates the segments and writes the records. The values
+// are those of trace_kernel, so the rows are the same bits.
+__global__ void __launch_bounds__(128) trace_warp_kernel(TraceArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= a.nrays) return;  // the whole warp
+    const bool lead = lane == 0;
+    const int ray = a.ray_of[r];
+    const int tab = a.table_of[ray];
+    const float* tb = a.table_ptr ? a.table_ptr[tab] : a.tables + int64_t(tab) * a.table_n;
+    const RGrid& g = a.fwd;
+    const double st_lon = a.table_station[3 * tab], st_lat = a.table_station[3 * tab + 1];
+    const double st_dep = fmin(fmax(a.table_station[3 * tab + 2], g.min_dep), g.dep_last);
+    const GeoPt ev{a.events[3 * ray], a.events[3 * ray + 1], a.events[3 * ray + 2]};
+    double* tcg = a.tcg + 4 * int64_t(ray);
+    if (lead) a.outside[ray] = 0;
+
+    V3 station = geo::to_cartesian(st_lon, st_lat, st_dep);
+    V3 p = geo::to_cartesian(ev.lon, ev.lat, ev.dep);
+    double t0 = geo::table_time_w(g, tb, ev.lon, ev.lat, ev.dep, lane);
+    if (lead) tcg[0] = t0;
+    if (!isfinite(t0)) {
+        if (lead) a.rec_count[r] = kDropped;
+        return;
+    }
+    double g0e, g0n, g0z;
+    geo::table_gradient_w(g, tb, ev.lon, ev.lat, ev.dep, g0e, g0n, g0z, lane);
+    if (lead) {
+        tcg[1] = g0e;
+        tcg[2] = g0n;
+        tcg[3] = g0z;
+    }
+    const double step = a.step_km;
+    const int max_steps = 20 * int(ceil(geo::norm(geo::sub(p, station)) / step + 10));
+    double last_t = t0;
+    int stalls = 0;
+    Recorder rec;
+    if (a.bg_n > 0) rec.bgv = a.bg + (a.table_phase[tab] == 0 ? 1 : 2) * a.bg_n;
+    unsigned long long taken = 0;
+    V3 prev = p;
+    bool dropped = false;
+    for (int s = 0; s < max_steps; s++) {
+        if (geo::norm(geo::sub(p, station)) <= 1.5 * step) break;
+        taken++;
+        GeoPt gp = geo::from_cartesian(p);
+        double ge, gn, gz;
+        geo::table_gradient_w(g, tb, gp.lon, gp.lat, gp.dep, ge, gn, gz, lane);
+        if (!isfinite(ge) || !isfinite(gn) || !isfinite(gz)) {
+            dropped = true;
+            break;
+        }
+        double sl, cl, so, co;
+        sincos(gp.lat * kDeg2Rad, &sl, &cl);
+        sincos(gp.lon * kDeg2Rad, &so, &co);
+        V3 e{-so, co, 0}, nn{-sl * co, -sl * so, cl}, up{cl * co, cl * so, sl};
+        V3 grad = geo::add(geo::add(geo::scale(e, ge), geo::scale(nn, gn)), geo::scale(up, -gz));
+        double nrm = geo::norm(grad);
+        if (nrm < 1e-12) {
+            dropped = true;
+            break;
+        }
+        p = geo::sub(p, geo::scale(grad, step / nrm));
+        GeoPt q = geo::from_cartesian(p);
+        q.lon = fmin(fmax(geo::unwrap_lon(q.lon, g.centre_lon), g.min_lon), g.lon_last);
+        q.lat = fmin(fmax(q.lat, g.min_lat), g.lat_last);
+        q.dep = fmin(fmax(q.dep, g.min_dep), g.dep_last);
+        p = geo::to_cartesian(q.lon, q.lat, q.dep);
+        if (lead) rec.segment(a, r, prev, p);
+        prev = p;
+        double t = geo::table_time_w(g, tb, q.lon, q.lat, q.dep, lane);
+        if (!(t < last_t)) {
+            if (++stalls > 20) {
+                dropped = true;
+                break;
+            }
+        } else {
+            stalls = 0;
+        }
+        last_t = fmin(last_t, t);
+    }
+    if (!lead) return;
+    atomicAdd(a.steps, taken);
+    if (dropped) {
+        a.rec_count[r] = kDropped;
+        return;
+    }
+    rec.segment(a, r, prev, station);
+    rec.flush(a, r);
+    a.outside[ray] = rec.outside;
+    a.rec_count[r] = rec.overflow ? kOverflow : rec.count;
+}
+
 // One warp per ray: sort records by (node, record index), sum each node in record order, write
 // the unique nodes ascending. P is the power-of-two sort size of one warp's shared memory.
 // A pass handles the rays with lo < records <= P; the first pass (lo = 0) also writes the empty
@@ -668,7 +763,8 @@ static int trace_impl(ts_ctx* ctx, const host::Grid& fwd, const float* tables_de
             a.rec_node = z.rec_node;
             a.rec_val = z.rec_val;
             a.rec_count = z.rec_count;
-            trace_kernel<<<(nr + 127) / 128, 128, 0, s>>>(a);
+            if (n_rays <= ctx->ray_warp_max) trace_warp_kernel<<<(nr + 3) / 4, 128, 0, s>>>(a);
+            else trace_kernel<<<(nr + 127) / 128, 128, 0, s>>>(a);
             TS_CUDA_TRY(ctx, cudaGetLastError());
             int Pbig = Psmall;
             while (Pbig < c.maxcap) Pbig <<= 1;
@@ -875,6 +971,13 @@ void rows_view(const ts_rows* rows, int* n_rows, int64_t* nnz, const int** row_p
 }  // namespace ts
 
 extern "C" {
+
+int ts_rays_set_warp_max(ts_ctx* ctx, int32_t max_rays) {
+    if (!ctx || max_rays < 0) return TS_E_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    ctx->ray_warp_max = max_rays;
+    return TS_OK;
+}
 
 int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float* tables, const double* table_station,
                   const ts_grid* inv, int32_t n_rays, const int32_t* table_of, const double* events, double step_km,
