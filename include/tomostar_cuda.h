@@ -263,7 +263,8 @@ int ts_rays_trace(ts_ctx* ctx, const ts_grid* fwd, int32_t n_tables, const float
  * per CPU thread, RayKernels.cs:67-107): a call of at most max_rays rays is traced with one warp
  * per ray, whose lanes share each step's corner loads and gradient evaluations (the latency of a
  * small call, such as a serving completion's, is its longest ray's); a larger call with one thread
- * per ray. Both give the same rows to the bit. Default 1024; 0 always uses a thread per ray. */
+ * per ray. Both give the same rows to the bit. Default 2048 (one warp per ray is the faster below about
+ * 2,500 rays of a 121×121×61 model, a thread per ray above); 0 always uses a thread per ray. */
 int ts_rays_set_warp_max(ts_ctx* ctx, int32_t max_rays);
 
 /* RayKernels.Compute for travel times (Tomography/RayKernels.cs:30-115) with the tables built on

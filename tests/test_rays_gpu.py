@@ -185,7 +185,7 @@ def test_warp_per_ray_equals_thread_per_ray(solver):
         assert lib.ts_rays_set_warp_max(solver.handle, 0) == L.TS_OK
         thread = trace_rows(solver, p.grid, tabs, tstations, p.inv, table_of, evs, p.step_km)
     finally:
-        lib.ts_rays_set_warp_max(solver.handle, 1024)
+        lib.ts_rays_set_warp_max(solver.handle, 2048)
     _same_rows(warp, thread)
     nnz, nodes, lens, tg = O.ray_rows_many(og, tabs, table_of, tstations[table_of], O.Grid.of(p.inv), evs, p.step_km)
     compare_rows(warp, nnz, nodes, lens, tg)

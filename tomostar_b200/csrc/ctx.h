@@ -30,7 +30,7 @@ struct ts_ctx {
     // The extended domain's 1-D background for the rays' outside time (ts_set_background): node count,
     // the nodes in the "rays.background" buffer (depths, Vp, Vs).
     int bg_n = 0;
-    int ray_warp_max = 1024;  // calls of at most this many rays trace one warp per ray
+    int ray_warp_max = 2048;  // calls of at most this many rays trace one warp per ray
     // LSQR's onIteration (Numerics/Lsqr.cs:43,140): called after every iteration with its ‖r‖.
     void (*lsqr_on_iteration)(int32_t iteration, double rnorm, void* user) = nullptr;
     void* lsqr_user = nullptr;
