@@ -221,31 +221,21 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
             if (__any_sync(FULL, is_due)) {
                 // Canonical neighbours: one row back has evaluated this x (its offset −1), one row
                 // ahead has not (offset +1); two rows away likewise at offsets ∓2.
-                // The first-order phase neither reads nor wakes neighbours two nodes away: its update
-                // never uses them, so waking them could only repeat an evaluation with the same
-                // inputs (no value changes either way; `second` is the same for the whole warp).
                 Real yb1 = shfl_up_r(FULL, W1, 1), ya1 = shfl_down_r(FULL, W3, 1);
+                Real yb2 = shfl_up_r(FULL, W0, 2), ya2 = shfl_down_r(FULL, W4, 2);
                 Real zb1 = shfl_up_r(FULL, W1, 8), za1 = shfl_down_r(FULL, W3, 8);
-                Real yb2 = inf, ya2 = inf, zb2 = inf, za2 = inf;
-                if (second) {
-                    yb2 = shfl_up_r(FULL, W0, 2);
-                    ya2 = shfl_down_r(FULL, W4, 2);
-                    zb2 = shfl_up_r(FULL, W0, 16);
-                    za2 = shfl_down_r(FULL, W4, 16);
-                }
+                Real zb2 = shfl_up_r(FULL, W0, 16), za2 = shfl_down_r(FULL, W4, 16);
                 bool chg = false;
                 if (is_due) {
                     const int x = ax(ip);
                     if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
                     if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
+                    if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                    if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
                     if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
                     if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
-                    if (second) {
-                        if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
-                        if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
-                        if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
-                        if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
-                    }
+                    if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                    if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
                     due &= ~(kOne << ip);
                     evals++;
                     // Canonical → grid orientation (minus = smaller grid index).
@@ -272,26 +262,22 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     if constexpr (RESHUFFLE) {
                         yb1 = shfl_up_r(FULL, W1, 1);
                         ya1 = shfl_down_r(FULL, W3, 1);
-                        if (second) {
-                            yb2 = shfl_up_r(FULL, W0, 2);
-                            ya2 = shfl_down_r(FULL, W4, 2);
-                        }
+                        yb2 = shfl_up_r(FULL, W0, 2);
+                        ya2 = shfl_down_r(FULL, W4, 2);
                         zb1 = shfl_up_r(FULL, W1, 8);
                         za1 = shfl_down_r(FULL, W3, 8);
-                        if (second) {
-                            zb2 = shfl_up_r(FULL, W0, 16);
-                            za2 = shfl_down_r(FULL, W4, 16);
-                        }
+                        zb2 = shfl_up_r(FULL, W0, 16);
+                        za2 = shfl_down_r(FULL, W4, 16);
                         if (chg) {
                             const int x = ax(ip);
                             if (hy_m1 >= 0) yb1 = halo[hy_m1 + x];
                             if (hy_p1 >= 0) ya1 = halo[hy_p1 + x];
-                            if (second && hy_m2 >= 0) yb2 = halo[hy_m2 + x];
-                            if (second && hy_p2 >= 0) ya2 = halo[hy_p2 + x];
+                            if (hy_m2 >= 0) yb2 = halo[hy_m2 + x];
+                            if (hy_p2 >= 0) ya2 = halo[hy_p2 + x];
                             if (hz_m1 >= 0) zb1 = halo[hz_m1 + x];
                             if (hz_p1 >= 0) za1 = halo[hz_p1 + x];
-                            if (second && hz_m2 >= 0) zb2 = halo[hz_m2 + x];
-                            if (second && hz_p2 >= 0) za2 = halo[hz_p2 + x];
+                            if (hz_m2 >= 0) zb2 = halo[hz_m2 + x];
+                            if (hz_p2 >= 0) za2 = halo[hz_p2 + x];
                         }
                     }
                     // A changed node wakes its 12 stencil neighbours (with the causal rule, those
@@ -302,14 +288,12 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     Mask wk = 0;
                     if (wk_if(W1)) wk |= bit(ip - 1);
                     if (wk_if(W3)) wk |= bit(ip + 1);
-                    if (second && wk_if(W0)) wk |= bit(ip - 2);
-                    if (second && wk_if(W4)) wk |= bit(ip + 2);
+                    if (wk_if(W0)) wk |= bit(ip - 2);
+                    if (wk_if(W4)) wk |= bit(ip + 2);
                     const unsigned Byb1 = __ballot_sync(FULL, wk_if(yb1)), Bya1 = __ballot_sync(FULL, wk_if(ya1));
-                    const unsigned Byb2 = second ? __ballot_sync(FULL, wk_if(yb2)) : 0u;
-                    const unsigned Bya2 = second ? __ballot_sync(FULL, wk_if(ya2)) : 0u;
+                    const unsigned Byb2 = __ballot_sync(FULL, wk_if(yb2)), Bya2 = __ballot_sync(FULL, wk_if(ya2));
                     const unsigned Bzb1 = __ballot_sync(FULL, wk_if(zb1)), Bza1 = __ballot_sync(FULL, wk_if(za1));
-                    const unsigned Bzb2 = second ? __ballot_sync(FULL, wk_if(zb2)) : 0u;
-                    const unsigned Bza2 = second ? __ballot_sync(FULL, wk_if(za2)) : 0u;
+                    const unsigned Bzb2 = __ballot_sync(FULL, wk_if(zb2)), Bza2 = __ballot_sync(FULL, wk_if(za2));
                     if ((jp >= 1 && ((Bya1 >> (lane - 1)) & 1u)) || (kp >= 1 && ((Bza1 >> (lane - 8)) & 1u)))
                         wk |= bit(ip + 1);
                     if ((jp <= BY - 2 && ((Byb1 >> (lane + 1)) & 1u)) || (kp <= BZ - 2 && ((Bzb1 >> (lane + 8)) & 1u)))
@@ -323,13 +307,13 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                         // Neighbours in other tiles (their values are the halo's, fixed in this visit).
                         const Mask b = kOne << ip;
                         if ((hy_m1 >= 0 && wk_if(yb1)) || (hy_p1 >= 0 && wk_if(ya1))) wky1 |= b;
-                        if (second && ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2)))) wky2 |= b;
+                        if ((hy_m2 >= 0 && wk_if(yb2)) || (hy_p2 >= 0 && wk_if(ya2))) wky2 |= b;
                         if ((hz_m1 >= 0 && wk_if(zb1)) || (hz_p1 >= 0 && wk_if(za1))) wkz1 |= b;
-                        if (second && ((hz_m2 >= 0 && wk_if(zb2)) || (hz_p2 >= 0 && wk_if(za2)))) wkz2 |= b;
+                        if ((hz_m2 >= 0 && wk_if(zb2)) || (hz_p2 >= 0 && wk_if(za2))) wkz2 |= b;
                         if (ip == 0 && wk_if(W1)) wxh |= 1u;
-                        if (second && ip <= 1 && wk_if(W0)) wxh |= ip == 0 ? 2u : 1u;
+                        if (ip <= 1 && wk_if(W0)) wxh |= ip == 0 ? 2u : 1u;
                         if (ip == BX - 1 && wk_if(W3)) wxh |= 4u;
-                        if (second && ip >= BX - 2 && wk_if(W4)) wxh |= ip == BX - 1 ? 8u : 4u;
+                        if (ip >= BX - 2 && wk_if(W4)) wxh |= ip == BX - 1 ? 8u : 4u;
                     }
                 }
             }
