@@ -290,10 +290,18 @@ TS_DEVINL int process_pencil(const Args<Real>& a, const GridDesc& g, const Field
                     if (wk_if(W3)) wk |= bit(ip + 1);
                     if (wk_if(W0)) wk |= bit(ip - 2);
                     if (wk_if(W4)) wk |= bit(ip + 2);
-                    const unsigned Byb1 = __ballot_sync(FULL, wk_if(yb1)), Bya1 = __ballot_sync(FULL, wk_if(ya1));
-                    const unsigned Byb2 = __ballot_sync(FULL, wk_if(yb2)), Bya2 = __ballot_sync(FULL, wk_if(ya2));
-                    const unsigned Bzb1 = __ballot_sync(FULL, wk_if(zb1)), Bza1 = __ballot_sync(FULL, wk_if(za1));
-                    const unsigned Bzb2 = __ballot_sync(FULL, wk_if(zb2)), Bza2 = __ballot_sync(FULL, wk_if(za2));
+                    // Without the causal rule every direction's ballot is the ballot of the changes.
+                    unsigned Byb1 = cb, Bya1 = cb, Byb2 = cb, Bya2 = cb, Bzb1 = cb, Bza1 = cb, Bzb2 = cb, Bza2 = cb;
+                    if (causal) {  // the same for the whole warp
+                        Byb1 = __ballot_sync(FULL, wk_if(yb1));
+                        Bya1 = __ballot_sync(FULL, wk_if(ya1));
+                        Byb2 = __ballot_sync(FULL, wk_if(yb2));
+                        Bya2 = __ballot_sync(FULL, wk_if(ya2));
+                        Bzb1 = __ballot_sync(FULL, wk_if(zb1));
+                        Bza1 = __ballot_sync(FULL, wk_if(za1));
+                        Bzb2 = __ballot_sync(FULL, wk_if(zb2));
+                        Bza2 = __ballot_sync(FULL, wk_if(za2));
+                    }
                     if ((jp >= 1 && ((Bya1 >> (lane - 1)) & 1u)) || (kp >= 1 && ((Bza1 >> (lane - 8)) & 1u)))
                         wk |= bit(ip + 1);
                     if ((jp <= BY - 2 && ((Byb1 >> (lane + 1)) & 1u)) || (kp <= BZ - 2 && ((Bzb1 >> (lane + 8)) & 1u)))
